@@ -1,0 +1,745 @@
+// D2Q4x6 curved-boundary VLBM time step for sm_100a.
+//
+// Layout: dense SoA, component-major, j fastest: f[(q*6+a)*N + i*ny + j],
+// N = nx*ny.  One thread per node (a warp covers 32 consecutive j, so every
+// population load and store is a coalesced 256-byte segment) and one thread
+// per cut link.
+//
+// Step pipeline (one launch each, all on one stream):
+//   collide  f0 -> fpost, U, u, u*            _collide_masked_kernel
+//   sweep    U, u -> u_next, u* (+ anchors)    _local_displacement_bc/relax
+//   commit   u <- u_next                       _local_displacement_commit
+//   repair   fpost, U <- blend(F, I+grad u)    _local_compatibility_repair
+//   stream   f1[q](x) = fpost[q](x - c_q)      _stream_masked_kernel (pull form)
+//   links    f1[q_in] at cut nodes             _apply_curved_boundary_links
+// Anchors are gathered per node from a CSR of its links in ascending link
+// order, the order in which the reference's serial atomics add them.
+#include <cuda_runtime.h>
+
+#include "cvlbm_common.cuh"
+#include "cvlbm_math.cuh"
+
+using namespace cv;
+
+namespace {
+
+constexpr int kQ2 = 4;
+constexpr int kC2 = 6;
+constexpr int kMaxLsq2 = 24;
+constexpr int kMaxIds2 = 8;
+
+struct Ctx2 {
+  cvlbm2d_problem p;
+  Mat m;
+  int N;
+};
+
+// Boundary time: the step's start time (host value, or the device clock in
+// graph mode) plus `offset`, evaluated as the reference's time + 0.5*dt.
+__device__ __forceinline__ double time_of(const double* clock, double t, double offset) {
+  return (clock ? clock[0] : t) + offset;
+}
+
+// ---------------------------------------------------------------------------
+// Collision, two_d/curved_boundary_warp.py:1691-1843.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_collide2(Ctx2 c, const double* __restrict__ f0,
+                                                  double* __restrict__ fpost,
+                                                  double* __restrict__ U, double* __restrict__ u,
+                                                  double* __restrict__ ustar,
+                                                  int* __restrict__ invalid) {
+  const int N = c.N;
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const cvlbm2d_problem& p = c.p;
+  if (p.active[n] == 0) {
+    for (int k = 0; k < kQ2 * kC2; ++k) fpost[(size_t)k * N + n] = 0.0;
+    for (int a = 0; a < kC2; ++a) U[(size_t)a * N + n] = 0.0;
+    u[n] = 0.0;
+    u[N + n] = 0.0;
+    return;
+  }
+  double f[kQ2 * kC2];
+#pragma unroll
+  for (int k = 0; k < kQ2 * kC2; ++k) f[k] = f0[(size_t)k * N + n];
+  double S[kC2];
+#pragma unroll
+  for (int a = 0; a < kC2; ++a) {
+    double s = 0.0;
+#pragma unroll
+    for (int q = 0; q < kQ2; ++q) s += f[q * kC2 + a];
+    S[a] = s;
+  }
+  const double hdt = 0.5 * p.dt;
+  if (p.source_mode == kSrcConstant) {
+#pragma unroll
+    for (int a = 0; a < kC2; ++a) S[a] += hdt * p.source[a];
+  } else if (p.source_mode == kSrcDamping) {
+    double den = 1.0 + hdt * p.source[0];
+    S[0] = S[0] / den;
+    S[1] = S[1] / den;
+  }
+  double B[kC2];
+#pragma unroll
+  for (int a = 0; a < kC2; ++a) B[a] = source_comp(a, p.source_mode, p.source, S);
+#pragma unroll
+  for (int a = 0; a < kC2; ++a) U[(size_t)a * N + n] = S[a];
+  double ux = ustar[n] + 0.5 * p.dt * S[0];
+  double uy = ustar[N + n] + 0.5 * p.dt * S[1];
+  u[n] = ux;
+  u[N + n] = uy;
+  ustar[n] = ux + 0.5 * p.dt * S[0];
+  ustar[N + n] = uy + 0.5 * p.dt * S[1];
+  double J = S[2] * S[5] - S[3] * S[4];
+  if (J <= c.m.jf) *invalid = 1;
+  P2 P = piola2(S[2], S[3], S[4], S[5], c.m);
+  const double k2c = 2.0 / p.c;
+  const double om = p.omega;
+  const double sw = p.dt * (2.0 - om) * 0.125;
+#pragma unroll
+  for (int q = 0; q < kQ2; ++q) {
+#pragma unroll
+    for (int a = 0; a < kC2; ++a) {
+      double fe = feq2(q, a, S, P, k2c);
+      double old = f[q * kC2 + a];
+      fpost[(size_t)(q * kC2 + a) * N + n] = old + om * (fe - old) + sw * B[a];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Local displacement sweep, two_d/curved_boundary_warp.py:3275-3490, with the
+// link anchors (:3287-3417) gathered per node.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void anchor2(const Ctx2& c, const double* U, int ell, int n, int i, int j,
+                                        double time, double& diag, double& r0, double& r1) {
+  const cvlbm2d_problem& p = c.p;
+  int bid = p.link_bid[ell];
+  if (p.disp_bid >= 0) {
+    if (bid != p.disp_bid) return;
+  } else if (p.bc_kind[bid] != kDirichlet) {
+    return;
+  }
+  const double* pp = p.bc_params + bid * 8;
+  int mode = p.bc_mode[bid];
+  double xb = p.link_xb[ell], yb = p.link_yb[ell];
+  double nxb = p.link_nx[ell], nyb = p.link_ny[ell];
+  double ub0 = 0.0, ub1 = 0.0;
+  if (mode == 1) {
+    ub0 = time * value2(0, mode, pp, xb, yb, nxb, nyb, 0.0);
+    ub1 = time * value2(1, mode, pp, xb, yb, nxb, nyb, 0.0);
+  } else if (mode == 6) {
+    double at = time;
+    if (pp[6] > 0.0 && at > pp[6]) at = pp[6];
+    ub0 = at * value2(0, mode, pp, xb, yb, nxb, nyb, 0.0);
+    ub1 = at * value2(1, mode, pp, xb, yb, nxb, nyb, 0.0);
+  }
+  const int N = c.N;
+  double dbx = xb - ((double)i + 0.5) * p.dx;
+  double dby = yb - ((double)j + 0.5) * p.dy;
+  double tx = ub0 - ((U[2 * N + n] - 1.0) * dbx + U[3 * N + n] * dby);
+  double ty = ub1 - (U[4 * N + n] * dbx + (U[5 * N + n] - 1.0) * dby);
+  double w2 = p.weight * p.weight;
+  diag = diag + w2;
+  r0 = r0 + w2 * tx;
+  r1 = r1 + w2 * ty;
+}
+
+__global__ void __launch_bounds__(256) k_sweep2(Ctx2 c, const double* __restrict__ U,
+                                                const double* __restrict__ u,
+                                                double* __restrict__ unext,
+                                                double* __restrict__ ustar, const double* clock,
+                                                double time_host) {
+  const int N = c.N;
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const cvlbm2d_problem& p = c.p;
+  if (p.active[n] == 0) {
+    unext[n] = 0.0;
+    unext[N + n] = 0.0;
+    return;
+  }
+  const int nx = p.nx, ny = p.ny;
+  const int i = n / ny, j = n - i * ny;
+  double diag = 0.0, rx = 0.0, ry = 0.0;
+  const double time = time_of(clock, time_host, 0.5 * p.dt);
+  for (int k = p.node_link_start[n]; k < p.node_link_start[n + 1]; ++k)
+    anchor2(c, U, p.node_link_list[k], n, i, j, time, diag, rx, ry);
+  const double* U2 = U + 2 * N;
+  const double* U3 = U + 3 * N;
+  const double* U4 = U + 4 * N;
+  const double* U5 = U + 5 * N;
+  const double hx = 0.5 * p.dx, hy = 0.5 * p.dy;
+  if (i + 1 < nx && p.active[n + ny] != 0) {
+    int m = n + ny;
+    double gx = hx * ((U2[n] - 1.0) + (U2[m] - 1.0));
+    double gy = hx * (U4[n] + U4[m]);
+    rx += u[m] - gx;
+    ry += u[N + m] - gy;
+    diag += 1.0;
+  }
+  if (i > 0 && p.active[n - ny] != 0) {
+    int m = n - ny;
+    double gx = hx * ((U2[m] - 1.0) + (U2[n] - 1.0));
+    double gy = hx * (U4[m] + U4[n]);
+    rx += u[m] + gx;
+    ry += u[N + m] + gy;
+    diag += 1.0;
+  }
+  if (j + 1 < ny && p.active[n + 1] != 0) {
+    int m = n + 1;
+    double gx = hy * (U3[n] + U3[m]);
+    double gy = hy * ((U5[n] - 1.0) + (U5[m] - 1.0));
+    rx += u[m] - gx;
+    ry += u[N + m] - gy;
+    diag += 1.0;
+  }
+  if (j > 0 && p.active[n - 1] != 0) {
+    int m = n - 1;
+    double gx = hy * (U3[m] + U3[n]);
+    double gy = hy * ((U5[m] - 1.0) + (U5[n] - 1.0));
+    rx += u[m] + gx;
+    ry += u[N + m] + gy;
+    diag += 1.0;
+  }
+  double u0 = u[n], u1 = u[N + n];
+  double n0 = u0, n1 = u1;
+  if (diag > 0.0) {
+    n0 = u0 + p.relax * (rx / diag - u0);
+    n1 = u1 + p.relax * (ry / diag - u1);
+  }
+  unext[n] = n0;
+  unext[N + n] = n1;
+  // commit (two_d/curved_boundary_warp.py:3493-3518): u* follows the same shift
+  ustar[n] = ustar[n] + (n0 - u0);
+  ustar[N + n] = ustar[N + n] + (n1 - u1);
+}
+
+__global__ void k_commit2(int N2, const double* __restrict__ src, double* __restrict__ dst) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n < N2) dst[n] = src[n];
+}
+
+// ---------------------------------------------------------------------------
+// Local deformation-gradient repair, two_d/curved_boundary_warp.py:3213-3272
+// (_local_dudx/_local_dudy) and :3521-3615.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double dudx2(const double* uc, const int* act, int n, int i, int nx,
+                                        int stride, double h) {
+  // stride = ny for d/dx, 1 for d/dy; i is the index along that axis
+  bool am = i > 0 && act[n - stride] != 0;
+  bool ap = i + 1 < nx && act[n + stride] != 0;
+  if (am && ap) return (uc[n + stride] - uc[n - stride]) / (2.0 * h);
+  if (ap) {
+    if (i + 2 < nx && act[n + 2 * stride] != 0)
+      return (-3.0 * uc[n] + 4.0 * uc[n + stride] - uc[n + 2 * stride]) / (2.0 * h);
+    return (uc[n + stride] - uc[n]) / h;
+  }
+  if (am) {
+    if (i > 1 && act[n - 2 * stride] != 0)
+      return (3.0 * uc[n] - 4.0 * uc[n - stride] + uc[n - 2 * stride]) / (2.0 * h);
+    return (uc[n] - uc[n - stride]) / h;
+  }
+  return 0.0;
+}
+
+__global__ void __launch_bounds__(256) k_repair2(Ctx2 c, double* __restrict__ f,
+                                                 double* __restrict__ U,
+                                                 const double* __restrict__ u) {
+  const int N = c.N;
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const cvlbm2d_problem& p = c.p;
+  const int* act = p.active;
+  if (act[n] == 0) return;
+  const int nx = p.nx, ny = p.ny;
+  const int i = n / ny, j = n - i * ny;
+  if (p.interior_only != 0) {
+    if (i == 0 || i + 1 >= nx || j == 0 || j + 1 >= ny) return;
+    if (act[n - ny] == 0 || act[n + ny] == 0 || act[n - 1] == 0 || act[n + 1] == 0) return;
+  }
+  double o11 = U[2 * N + n], o12 = U[3 * N + n], o21 = U[4 * N + n], o22 = U[5 * N + n];
+  double t11 = 1.0 + dudx2(u, act, n, i, nx, ny, p.dx);
+  double t12 = dudx2(u, act, n, j, ny, 1, p.dy);
+  double t21 = dudx2(u + N, act, n, i, nx, ny, p.dx);
+  double t22 = 1.0 + dudx2(u + N, act, n, j, ny, 1, p.dy);
+  double alpha = fmax(0.0, fmin(1.0, p.blend));
+  double n11 = o11, n12 = o12, n21 = o21, n22 = o22;
+  for (int g = 0; g < 10; ++g) {
+    n11 = o11 + alpha * (t11 - o11);
+    n12 = o12 + alpha * (t12 - o12);
+    n21 = o21 + alpha * (t21 - o21);
+    n22 = o22 + alpha * (t22 - o22);
+    if (n11 * n22 - n12 * n21 > c.m.jf) break;
+    alpha = 0.5 * alpha;
+  }
+  P2 Po = piola2(o11, o12, o21, o22, c.m);
+  P2 Pn = piola2(n11, n12, n21, n22, c.m);
+  double dP11 = Pn.a - Po.a, dP12 = Pn.b - Po.b, dP21 = Pn.c - Po.c, dP22 = Pn.d - Po.d;
+  const double ff = 0.5 / p.c;
+  const double qt = 0.25;
+#pragma unroll
+  for (int q = 0; q < kQ2; ++q) {
+    double cx = (double)cx2(q), cy = (double)cy2(q);
+    size_t b = (size_t)(q * kC2) * N + n;
+    f[b] = f[b] - ff * (cx * dP11 + cy * dP12);
+    f[b + N] = f[b + N] - ff * (cx * dP21 + cy * dP22);
+    f[b + 2 * (size_t)N] = f[b + 2 * (size_t)N] + qt * (n11 - o11);
+    f[b + 3 * (size_t)N] = f[b + 3 * (size_t)N] + qt * (n12 - o12);
+    f[b + 4 * (size_t)N] = f[b + 4 * (size_t)N] + qt * (n21 - o21);
+    f[b + 5 * (size_t)N] = f[b + 5 * (size_t)N] + qt * (n22 - o22);
+  }
+  U[2 * N + n] = n11;
+  U[3 * N + n] = n12;
+  U[4 * N + n] = n21;
+  U[5 * N + n] = n22;
+}
+
+// ---------------------------------------------------------------------------
+// Streaming in pull form, equivalent to the push of
+// two_d/curved_boundary_warp.py:2043-2060 after the clear of f1.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_stream2(Ctx2 c, const double* __restrict__ fpost,
+                                                 double* __restrict__ f1) {
+  const int N = c.N;
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const cvlbm2d_problem& p = c.p;
+  const int nx = p.nx, ny = p.ny;
+  const int i = n / ny, j = n - i * ny;
+  if (p.active[n] == 0) {
+    for (int k = 0; k < kQ2 * kC2; ++k) f1[(size_t)k * N + n] = 0.0;
+    return;
+  }
+#pragma unroll
+  for (int q = 0; q < kQ2; ++q) {
+    int si = i - cx2(q), sj = j - cy2(q);
+    bool ok = si >= 0 && si < nx && sj >= 0 && sj < ny && p.active[si * ny + sj] != 0;
+    int s = si * ny + sj;
+#pragma unroll
+    for (int a = 0; a < kC2; ++a) {
+      size_t k = (size_t)(q * kC2 + a) * N;
+      f1[k + n] = ok ? fpost[k + s] : 0.0;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Cut-link reconstruction, two_d/curved_boundary_warp.py:2063-3098, for the
+// bfl / lsq_bfl / compat_bfl / local_char2 / local_f / local_f_bfl closures.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double interp_link(const double* Uc, const int* act, int i, int j,
+                                              int qo, double s, int nx, int ny) {
+  // two_d/curved_boundary_warp.py:1443-1480 (_interp_U_link)
+  double v0 = Uc[i * ny + j];
+  int i1 = i - cx2(qo), j1 = j - cy2(qo);
+  if (i1 >= 0 && i1 < nx && j1 >= 0 && j1 < ny && act[i1 * ny + j1] != 0) {
+    double v1 = Uc[i1 * ny + j1];
+    int i2 = i - 2 * cx2(qo), j2 = j - 2 * cy2(qo);
+    if (i2 >= 0 && i2 < nx && j2 >= 0 && j2 < ny && act[i2 * ny + j2] != 0) {
+      double v2 = Uc[i2 * ny + j2];
+      double l0 = 0.5 * (s + 1.0) * (s + 2.0);
+      double l1 = -s * (s + 2.0);
+      double l2 = 0.5 * s * (s + 1.0);
+      return l0 * v0 + l1 * v1 + l2 * v2;
+    }
+    return (s + 1.0) * v0 - s * v1;
+  }
+  return v0;
+}
+
+__device__ __forceinline__ double lsq_eval(const cvlbm2d_problem& p, const double* w,
+                                           const double* Uc, int ell) {
+  // two_d/curved_boundary_warp.py:1202-1221 (_lsq_U_at_boundary), valid links only
+  double out = 0.0;
+  const int* li = p.lsq_i + (size_t)ell * kMaxLsq2;
+  const int* lj = p.lsq_j + (size_t)ell * kMaxLsq2;
+  const double* ww = w + (size_t)ell * kMaxLsq2;
+  for (int m = 0; m < kMaxLsq2; ++m) {
+    int ii = li[m], jj = lj[m];
+    if (ii >= 0 && jj >= 0) out += ww[m] * Uc[ii * p.ny + jj];
+  }
+  return out;
+}
+
+__device__ void link2(const Ctx2& c, int ell, const double* __restrict__ fpost,
+                      double* __restrict__ fout, const double* __restrict__ U,
+                      const double* __restrict__ u, double tmid) {
+  const cvlbm2d_problem& p = c.p;
+  const Mat& m = c.m;
+  const int N = c.N, nx = p.nx, ny = p.ny;
+  const int recon = p.recon;
+  const int i = p.link_i[ell], j = p.link_j[ell], qo = p.link_q[ell];
+  int bid = p.link_bid[ell];
+  if (bid < 0 || bid >= kMaxIds2) bid = 0;
+  const int kind = p.bc_kind[bid], mode = p.bc_mode[bid];
+  const double* pp = p.bc_params + bid * 8;
+  int qi = qo + 2;
+  if (qi >= 4) qi -= 4;
+  const double eta = p.link_eta[ell];
+  const double xb = p.link_xb[ell], yb = p.link_yb[ell];
+  const double nxb = p.link_nx[ell], nyb = p.link_ny[ell];
+  const double dxin = (double)cx2(qi), dyin = (double)cy2(qi);
+  const int n = i * ny + j;
+  double bv0 = value2(0, mode, pp, xb, yb, nxb, nyb, tmid);
+  double bv1 = value2(1, mode, pp, xb, yb, nxb, nyb, tmid);
+  if (kind == kNeumann && p.use_dynamic_traction != 0) {
+    bv0 = p.traction_x[ell];
+    bv1 = p.traction_y[ell];
+  }
+  double Fg[4] = {U[2 * N + n], U[3 * N + n], U[4 * N + n], U[5 * N + n]};
+  const int iu = i - cx2(qo), ju = j - cy2(qo);
+  const bool up_ok = iu >= 0 && iu < nx && ju >= 0 && ju < ny && p.active[iu * ny + ju] != 0;
+  const int nu = iu * ny + ju;
+  const bool lsq_ok = p.lsq_valid[ell] != 0;
+  if (recon == 0 || recon == 2 || recon == 13) {
+    if (up_ok) {
+      for (int k = 0; k < 4; ++k) {
+        const double* Uk = U + (size_t)(2 + k) * N;
+        Fg[k] = Uk[n] + eta * (Uk[n] - Uk[nu]);
+      }
+    }
+    if (recon == 2 && lsq_ok)
+      for (int k = 0; k < 4; ++k) Fg[k] = lsq_eval(p, p.lsq_wb, U + (size_t)(2 + k) * N, ell);
+  } else {
+    for (int k = 0; k < 4; ++k)
+      Fg[k] = interp_link(U + (size_t)(2 + k) * N, p.active, i, j, qo, eta, nx, ny);
+  }
+  if ((recon == 11 || recon == 12) && lsq_ok)
+    for (int k = 0; k < 4; ++k) Fg[k] = lsq_eval(p, p.lsq_wb, U + (size_t)(2 + k) * N, ell);
+  if ((recon == 9 || recon == 11) && lsq_ok) {
+    const double tanx = -nyb, tany = nxb;
+    double dut0 = 0.0, dut1 = 0.0, wt_abs = 0.0;
+    if (kind == kNeumann) {
+      const int* li = p.lsq_i + (size_t)ell * kMaxLsq2;
+      const int* lj = p.lsq_j + (size_t)ell * kMaxLsq2;
+      const double* wt = p.lsq_wt + (size_t)ell * kMaxLsq2;
+      for (int mm = 0; mm < kMaxLsq2; ++mm) {
+        int ii = li[mm], jj = lj[mm];
+        if (ii >= 0 && jj >= 0) {
+          double ww = wt[mm];
+          dut0 += ww * u[ii * ny + jj];
+          dut1 += ww * u[N + ii * ny + jj];
+          wt_abs += fabs(ww);
+        }
+      }
+    } else {
+      if (mode == 6) {
+        double at = tmid;
+        if (pp[6] > 0.0 && at > pp[6]) at = pp[6];
+        dut0 = at * (pp[0] * tanx + pp[1] * tany);
+        dut1 = at * (pp[3] * tanx + pp[4] * tany);
+      }
+      wt_abs = 1.0;
+    }
+    if (wt_abs > 0.0) {
+      double hn0 = Fg[0] * nxb + Fg[1] * nyb;
+      double hn1 = Fg[2] * nxb + Fg[3] * nyb;
+      double gt0 = tanx + dut0, gt1 = tany + dut1;
+      Fg[0] = hn0 * nxb + gt0 * tanx;
+      Fg[1] = hn0 * nyb + gt0 * tany;
+      Fg[2] = hn1 * nxb + gt1 * tanx;
+      Fg[3] = hn1 * nyb + gt1 * tany;
+    }
+  }
+  double Fb[4] = {Fg[0], Fg[1], Fg[2], Fg[3]};
+  if (kind == kNeumann) solve_normal_image2(Fg, nxb, nyb, bv0, bv1, m, p.normal_solver, Fb);
+  const P2 Pb = piola2(Fb[0], Fb[1], Fb[2], Fb[3], m);
+
+  const bool use_char = (recon == 11 || recon == 12) && kind == kNeumann && lsq_ok;
+  double cv[6] = {U[n], U[N + n], Fb[0], Fb[1], Fb[2], Fb[3]};
+  if (kind == kDirichlet) {
+    cv[0] = bv0;
+    cv[1] = bv1;
+  }
+  double cw[6] = {0, 0, 0, 0, 0, 0};
+  const double dt = p.dt, cc = p.c, om = p.omega;
+  if (use_char) {
+    double ux[6], uy[6];
+    for (int a = 0; a < 6; ++a) {
+      ux[a] = lsq_eval(p, p.lsq_wx, U + (size_t)a * N, ell);
+      uy[a] = lsq_eval(p, p.lsq_wy, U + (size_t)a * N, ell);
+    }
+    const double sx = -eta * dt * cc * (double)cx2(qo);
+    const double sy = -eta * dt * cc * (double)cy2(qo);
+    double dv[6];
+    for (int a = 0; a < 6; ++a) dv[a] = sx * ux[a] + sy * uy[a];
+    double sc = 1.0;
+    for (int g = 0; g < 10; ++g) {
+      double t11 = cv[2] + sc * dv[2], t12 = cv[3] + sc * dv[3];
+      double t21 = cv[4] + sc * dv[4], t22 = cv[5] + sc * dv[5];
+      if (t11 * t22 - t12 * t21 > 10.0 * m.jf) break;
+      sc = 0.5 * sc;
+    }
+    for (int a = 0; a < 6; ++a) cv[a] = cv[a] + sc * dv[a];
+    double Ax[6], Ay[6], Bx[6], By[6];
+    flux2_jvp(cv, ux, m, Ax, Bx);  // A_x U_x (Bx unused)
+    flux2_jvp(cv, uy, m, By, Ay);  // A_y U_y (By unused)
+    for (int a = 0; a < 6; ++a) {
+      double b = source_comp(a, p.source_mode, p.source, cv);
+      cw[a] = b - Ax[a] - Ay[a] + cc * (dxin * ux[a] + dyin * uy[a]);
+    }
+  }
+  double eqx[6], eqy[6];
+  P2 Pc{0, 0, 0, 0};
+  bool char_ok = false;
+  if (use_char && cv[2] * cv[5] - cv[3] * cv[4] > m.jf) {
+    char_ok = true;
+    flux2_jvp(cv, cw, m, eqx, eqy);
+    Pc = piola2(cv[2], cv[3], cv[4], cv[5], m);
+  }
+  const double k2c = 2.0 / cc;
+  for (int a = 0; a < 6; ++a) {
+    double D = 1.0, S = 0.0;
+    if (kind == kDirichlet) {
+      switch (a) {
+        case 0: D = -1.0; S = 0.5 * bv0; break;
+        case 1: D = -1.0; S = 0.5 * bv1; break;
+        case 2: S = -dxin * bv0 / cc; break;
+        case 3: S = -dyin * bv0 / cc; break;
+        case 4: S = -dxin * bv1 / cc; break;
+        default: S = -dyin * bv1 / cc; break;
+      }
+    } else {
+      switch (a) {
+        case 0: S = -(dxin * Pb.a + dyin * Pb.b) / cc; break;
+        case 1: S = -(dxin * Pb.c + dyin * Pb.d) / cc; break;
+        case 2: D = -1.0; S = 0.5 * Fb[0]; break;
+        case 3: D = -1.0; S = 0.5 * Fb[1]; break;
+        case 4: D = -1.0; S = 0.5 * Fb[2]; break;
+        default: D = -1.0; S = 0.5 * Fb[3]; break;
+      }
+    }
+    double val;
+    if (char_ok) {
+      // characteristic overwrite, two_d/curved_boundary_warp.py:3034-3097
+      double jv = 0.25 * (cw[a] + k2c * (dxin * eqx[a] + dyin * eqy[a]));
+      double ge = feq2(qi, a, cv, Pc, k2c);
+      double sa = source_comp(a, p.source_mode, p.source, cv);
+      val = ge - dt / om * jv + dt * (1.0 / om - 0.5) * 0.25 * sa;
+    } else {
+      double fo = fpost[(size_t)(qo * 6 + a) * N + n];
+      double fi = fpost[(size_t)(qi * 6 + a) * N + n];
+      if (eta >= 0.5) {
+        double al = 1.0 / (2.0 * eta);
+        val = al * (D * fo + S) + (1.0 - al) * fi;
+      } else {
+        double upv = fo;
+        if (up_ok) upv = fpost[(size_t)(qo * 6 + a) * N + nu];
+        val = D * (2.0 * eta * fo + (1.0 - 2.0 * eta) * upv) + S;
+      }
+    }
+    fout[(size_t)(qi * 6 + a) * N + n] = val;
+  }
+}
+
+__global__ void __launch_bounds__(128) k_links2(Ctx2 c, const double* __restrict__ fpost,
+                                                double* __restrict__ fout,
+                                                const double* __restrict__ U,
+                                                const double* __restrict__ u, const double* clock,
+                                                double t_host, double offset) {
+  int ell = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ell >= c.p.n_links) return;
+  link2(c, ell, fpost, fout, U, u, time_of(clock, t_host, offset));
+}
+
+// ---------------------------------------------------------------------------
+// Field refresh, two_d/curved_boundary_warp.py:3127-3210.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_refresh2(Ctx2 c, const double* __restrict__ f0,
+                                                  double* __restrict__ U, double* __restrict__ u,
+                                                  const double* __restrict__ ustar,
+                                                  double* __restrict__ Pf,
+                                                  double* __restrict__ sg,
+                                                  int* __restrict__ invalid) {
+  const int N = c.N;
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const cvlbm2d_problem& p = c.p;
+  if (p.active[n] == 0) {
+    for (int a = 0; a < kC2; ++a) U[(size_t)a * N + n] = 0.0;
+    u[n] = 0.0;
+    u[N + n] = 0.0;
+    for (int a = 0; a < 4; ++a) {
+      Pf[(size_t)a * N + n] = 0.0;
+      sg[(size_t)a * N + n] = 0.0;
+    }
+    return;
+  }
+  double S[kC2];
+  for (int a = 0; a < kC2; ++a) {
+    double s = 0.0;
+    for (int q = 0; q < kQ2; ++q) s += f0[(size_t)(q * kC2 + a) * N + n];
+    S[a] = s;
+  }
+  const double hdt = 0.5 * p.dt;
+  if (p.source_mode == kSrcConstant) {
+    for (int a = 0; a < kC2; ++a) S[a] += hdt * p.source[a];
+  } else if (p.source_mode == kSrcDamping) {
+    double den = 1.0 + hdt * p.source[0];
+    S[0] = S[0] / den;
+    S[1] = S[1] / den;
+  }
+  for (int a = 0; a < kC2; ++a) U[(size_t)a * N + n] = S[a];
+  u[n] = ustar[n] + 0.5 * p.dt * S[0];
+  u[N + n] = ustar[N + n] + 0.5 * p.dt * S[1];
+  double J = S[2] * S[5] - S[3] * S[4];
+  if (J <= c.m.jf) *invalid = 1;
+  double Js = clamp_j(J, c.m.jf);
+  P2 P = piola2(S[2], S[3], S[4], S[5], c.m);
+  Pf[n] = P.a;
+  Pf[(size_t)N + n] = P.b;
+  Pf[2 * (size_t)N + n] = P.c;
+  Pf[3 * (size_t)N + n] = P.d;
+  sg[n] = (P.a * S[2] + P.b * S[3]) / Js;
+  sg[(size_t)N + n] = (P.a * S[4] + P.b * S[5]) / Js;
+  sg[2 * (size_t)N + n] = (P.c * S[2] + P.d * S[3]) / Js;
+  sg[3 * (size_t)N + n] = (P.c * S[4] + P.d * S[5]) / Js;
+}
+
+// P and sigma from U, as stored by the collision (two_d/curved_boundary_warp.py:1791-1803)
+__global__ void __launch_bounds__(256) k_stress2(Ctx2 c, const double* __restrict__ U,
+                                                 double* __restrict__ Pf,
+                                                 double* __restrict__ sg) {
+  const int N = c.N;
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N || c.p.active[n] == 0) return;
+  double F11 = U[2 * (size_t)N + n], F12 = U[3 * (size_t)N + n];
+  double F21 = U[4 * (size_t)N + n], F22 = U[5 * (size_t)N + n];
+  double Js = clamp_j(F11 * F22 - F12 * F21, c.m.jf);
+  P2 P = piola2(F11, F12, F21, F22, c.m);
+  Pf[n] = P.a;
+  Pf[(size_t)N + n] = P.b;
+  Pf[2 * (size_t)N + n] = P.c;
+  Pf[3 * (size_t)N + n] = P.d;
+  sg[n] = (P.a * F11 + P.b * F12) / Js;
+  sg[(size_t)N + n] = (P.a * F21 + P.b * F22) / Js;
+  sg[2 * (size_t)N + n] = (P.c * F11 + P.d * F12) / Js;
+  sg[3 * (size_t)N + n] = (P.c * F21 + P.d * F22) / Js;
+}
+
+__global__ void k_tick(double* clock, double dt) { clock[0] = clock[0] + dt; }
+
+__global__ void k_zero_flag(int* flag) { *flag = 0; }
+
+inline unsigned blocks(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+bool due(int interval, long long step) { return interval > 0 && step % interval == 0; }
+
+int check_problem(const cvlbm2d_problem* p, const cvlbm2d_fields* f) {
+  if (!p || !f) return fail(CVLBM_ERR_INVALID_ARG, "null problem or fields");
+  if (p->nx < 1 || p->ny < 1) return fail(CVLBM_ERR_INVALID_ARG, "empty lattice");
+  if ((long long)p->nx * p->ny > 0x7fffffffLL / 24)
+    return fail(CVLBM_ERR_INVALID_ARG, "lattice too large for 32-bit node indexing");
+  if (!f->f0 || !f->f1 || !f->fpost || !f->U || !f->u || !f->u_next || !f->u_star ||
+      !f->invalid)
+    return fail(CVLBM_ERR_INVALID_ARG, "missing field buffer");
+  if (!p->active || !p->node_link_start || !p->bc_kind || !p->bc_mode || !p->bc_params)
+    return fail(CVLBM_ERR_INVALID_ARG, "missing geometry table");
+  switch (p->recon) {
+    case 0: case 2: case 9: case 11: case 12: case 13: break;
+    default: return fail(CVLBM_ERR_UNSUPPORTED, "unsupported 2-D boundary reconstruction id");
+  }
+  if (p->disp_interval > 0 && (p->disp_sweeps < 1 || p->disp_sweeps > 8))
+    return fail(CVLBM_ERR_INVALID_ARG, "displacement sweeps must be in [1,8]");
+  return CVLBM_OK;
+}
+
+Ctx2 make_ctx(const cvlbm2d_problem* p) {
+  Ctx2 c;
+  c.p = *p;
+  c.m = Mat{p->mat.model, p->mat.lam, p->mat.mu, p->mat.p0, p->mat.p1, p->mat.p2, p->mat.j_floor};
+  c.N = p->nx * p->ny;
+  return c;
+}
+
+void launch_links(const Ctx2& c, const double* src, double* dst, const double* U,
+                  const double* u, const double* clock, double t, double offset,
+                  cudaStream_t s) {
+  if (c.p.n_links <= 0) return;
+  k_links2<<<blocks(c.p.n_links, 128), 128, 0, s>>>(c, src, dst, U, u, clock, t, offset);
+}
+
+}  // namespace
+
+extern "C" int cvlbm2d_run(const cvlbm2d_problem* p, cvlbm2d_fields* f, double time0,
+                           int64_t step0, int32_t nsteps, int32_t graph_mode, void* stream) {
+  int rc = check_problem(p, f);
+  if (rc) return rc;
+  if (nsteps < 0) return fail(CVLBM_ERR_INVALID_ARG, "negative step count");
+  if (graph_mode && !f->clock) return fail(CVLBM_ERR_INVALID_ARG, "graph mode needs a clock");
+  cudaStream_t s = (cudaStream_t)stream;
+  Ctx2 c = make_ctx(p);
+  const int N = c.N;
+  const unsigned nb = blocks(N, 256);
+  const double* clock = graph_mode ? f->clock : nullptr;
+  k_zero_flag<<<1, 1, 0, s>>>(f->invalid);
+  double t = time0;
+  for (int k = 0; k < nsteps; ++k) {
+    const long long step = step0 + k;
+    k_collide2<<<nb, 256, 0, s>>>(c, f->f0, f->fpost, f->U, f->u, f->u_star, f->invalid);
+    if (due(p->disp_interval, step)) {
+      for (int sw = 0; sw < p->disp_sweeps; ++sw) {
+        k_sweep2<<<nb, 256, 0, s>>>(c, f->U, f->u, f->u_next, f->u_star, clock, t);
+        k_commit2<<<blocks(2LL * N, 256), 256, 0, s>>>(2 * N, f->u_next, f->u);
+      }
+    }
+    if (due(p->rep_interval, step)) k_repair2<<<nb, 256, 0, s>>>(c, f->fpost, f->U, f->u);
+    k_stream2<<<nb, 256, 0, s>>>(c, f->fpost, f->f1);
+    launch_links(c, f->fpost, f->f1, f->U, f->u, clock, t, 0.5 * p->dt, s);
+    if (graph_mode) k_tick<<<1, 1, 0, s>>>(f->clock, p->dt);
+    double* tmp = f->f0;
+    f->f0 = f->f1;
+    f->f1 = tmp;
+    t += p->dt;
+  }
+  return check_launch("cvlbm2d_run");
+}
+
+extern "C" int cvlbm2d_apply_boundary(const cvlbm2d_problem* p, cvlbm2d_fields* f, double t,
+                                      int32_t in_place, void* stream) {
+  int rc = check_problem(p, f);
+  if (rc) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  Ctx2 c = make_ctx(p);
+  if (p->n_links == 0) return CVLBM_OK;
+  if (in_place) {
+    // opposing cut links must read one frozen state
+    cudaMemcpyAsync(f->fpost, f->f0, sizeof(double) * 24 * (size_t)c.N, cudaMemcpyDeviceToDevice,
+                    s);
+    launch_links(c, f->fpost, f->f0, f->U, f->u, nullptr, t, 0.0, s);
+  } else {
+    launch_links(c, f->fpost, f->f1, f->U, f->u, nullptr, t, 0.0, s);
+  }
+  return check_launch("cvlbm2d_apply_boundary");
+}
+
+extern "C" int cvlbm2d_refresh(const cvlbm2d_problem* p, cvlbm2d_fields* f, void* stream) {
+  int rc = check_problem(p, f);
+  if (rc) return rc;
+  if (!f->P || !f->sigma) return fail(CVLBM_ERR_INVALID_ARG, "missing stress buffers");
+  cudaStream_t s = (cudaStream_t)stream;
+  Ctx2 c = make_ctx(p);
+  k_zero_flag<<<1, 1, 0, s>>>(f->invalid);
+  k_refresh2<<<blocks(c.N, 256), 256, 0, s>>>(c, f->f0, f->U, f->u, f->u_star, f->P, f->sigma,
+                                               f->invalid);
+  return check_launch("cvlbm2d_refresh");
+}
+
+extern "C" int cvlbm2d_stress(const cvlbm2d_problem* p, cvlbm2d_fields* f, void* stream) {
+  int rc = check_problem(p, f);
+  if (rc) return rc;
+  if (!f->P || !f->sigma) return fail(CVLBM_ERR_INVALID_ARG, "missing stress buffers");
+  Ctx2 c = make_ctx(p);
+  k_stress2<<<blocks(c.N, 256), 256, 0, (cudaStream_t)stream>>>(c, f->U, f->P, f->sigma);
+  return check_launch("cvlbm2d_stress");
+}
+
+extern "C" int cvlbm2d_graph_create(const cvlbm2d_problem* p, const cvlbm2d_fields* f,
+                                    int64_t step0, int32_t nsteps, cvlbm_graph** out) {
+  if (!out) return fail(CVLBM_ERR_INVALID_ARG, "null output");
+  if (nsteps <= 0 || (nsteps & 1)) return fail(CVLBM_ERR_INVALID_ARG, "nsteps must be even");
+  cvlbm2d_fields local = *f;
+  return capture_graph(
+      [&](cudaStream_t s) { return cvlbm2d_run(p, &local, 0.0, step0, nsteps, 1, s); }, out);
+}

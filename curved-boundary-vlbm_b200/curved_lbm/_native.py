@@ -1,0 +1,172 @@
+"""ctypes binding of libcvlbm.so (declared in ``include/cvlbm.h``).
+
+The solver classes keep their state in PyTorch CUDA tensors and hand raw
+device pointers to the library; the library launches the sm_100a kernels on
+PyTorch's current stream.  There is no CPU or fallback path: importing a
+solver on a machine without the built library or without a CUDA device
+raises immediately.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+_LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libcvlbm.so"
+_lib = None
+
+i32 = C.c_int32
+i64 = C.c_int64
+f64 = C.c_double
+pI = C.c_void_p  # device pointers are passed as opaque addresses
+
+
+class Material(C.Structure):
+    _fields_ = [("model", i32), ("reserved", i32), ("lam", f64), ("mu", f64), ("p0", f64),
+                ("p1", f64), ("p2", f64), ("j_floor", f64)]
+
+
+class Problem2D(C.Structure):
+    _fields_ = [
+        ("nx", i32), ("ny", i32), ("n_links", i32), ("recon", i32), ("normal_solver", i32),
+        ("source_mode", i32),
+        ("dx", f64), ("dy", f64), ("dt", f64), ("omega", f64), ("c", f64),
+        ("source", f64 * 6),
+        ("mat", Material),
+        ("disp_interval", i32), ("disp_sweeps", i32), ("disp_bid", i32), ("rep_interval", i32),
+        ("interior_only", i32), ("use_dynamic_traction", i32),
+        ("relax", f64), ("weight", f64), ("blend", f64),
+        ("active", pI),
+        ("link_i", pI), ("link_j", pI), ("link_q", pI), ("link_bid", pI),
+        ("link_eta", pI), ("link_xb", pI), ("link_yb", pI), ("link_nx", pI), ("link_ny", pI),
+        ("lsq_i", pI), ("lsq_j", pI),
+        ("lsq_wb", pI), ("lsq_wt", pI), ("lsq_wx", pI), ("lsq_wy", pI),
+        ("lsq_valid", pI),
+        ("node_link_start", pI), ("node_link_list", pI),
+        ("bc_kind", pI), ("bc_mode", pI), ("bc_params", pI),
+        ("traction_x", pI), ("traction_y", pI),
+    ]
+
+
+class Fields2D(C.Structure):
+    _fields_ = [(name, pI) for name in
+                ("f0", "f1", "fpost", "U", "u", "u_next", "u_star", "P", "sigma", "invalid",
+                 "clock")]
+
+
+class Problem3D(C.Structure):
+    _fields_ = [
+        ("n_active", i32), ("n_links", i32), ("nx", i32), ("ny", i32), ("nz", i32),
+        ("recon", i32), ("normal_solver", i32), ("source_mode", i32), ("has_char", i32),
+        ("has_tangent_lsq", i32),
+        ("disp_interval", i32), ("disp_sweeps", i32), ("disp_bid", i32), ("rep_interval", i32),
+        ("dx", f64), ("dy", f64), ("dz", f64), ("dt", f64), ("omega", f64), ("c", f64),
+        ("source", f64 * 12),
+        ("mat", Material),
+        ("relax", f64), ("weight", f64), ("blend", f64),
+        ("active_i", pI), ("active_j", pI), ("active_k", pI),
+        ("neighbor", pI),
+        ("link_p", pI), ("link_up", pI), ("link_q", pI), ("link_bid", pI),
+        ("link_eta", pI), ("link_xb", pI), ("link_yb", pI), ("link_zb", pI),
+        ("link_nx", pI), ("link_ny", pI), ("link_nz", pI),
+        ("lsq_p", pI), ("lsq_wt1", pI), ("lsq_wt2", pI), ("lsq_valid", pI),
+        ("char_idx", pI), ("char_w", pI),
+        ("node_link_start", pI), ("node_link_list", pI),
+        ("bc_kind", pI), ("bc_mode", pI), ("bc_comp_kind", pI), ("bc_params", pI),
+        ("dyn_enabled", pI), ("dyn_traction", pI),
+    ]
+
+
+class Fields3D(C.Structure):
+    _fields_ = [(name, pI) for name in
+                ("f0", "f1", "U", "u", "u_next", "u_star", "link_kind", "link_comp_kind",
+                 "link_bv", "link_Fb", "link_Pb", "char_state", "invalid", "clock")]
+
+
+EXPORTED = (
+    "cvlbm2d_run",
+    "cvlbm2d_apply_boundary",
+    "cvlbm2d_refresh",
+    "cvlbm2d_stress",
+    "cvlbm3d_run",
+    "cvlbm3d_apply_boundary",
+    "cvlbm3d_refresh",
+    "cvlbm3d_set_ustar",
+    "cvlbm2d_graph_create",
+    "cvlbm3d_graph_create",
+    "cvlbm_graph_launch",
+    "cvlbm_graph_destroy",
+    "cvlbm_version",
+    "cvlbm_last_error",
+)
+
+
+def lib_path() -> Path:
+    return Path(os.environ.get("CVLBM_LIBRARY", str(_LIB_PATH)))
+
+
+def load(require_cuda: bool = True):
+    """Load libcvlbm.so and declare its signatures; raises if unavailable."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = lib_path()
+    if not path.exists():
+        raise RuntimeError(
+            f"libcvlbm.so not found at {path}; build it with "
+            "`python -c 'import __graft_entry__ as g; g.build()'` (nvcc, sm_100a)")
+    lib = C.CDLL(str(path))
+    P2, F2, P3, F3 = C.POINTER(Problem2D), C.POINTER(Fields2D), C.POINTER(Problem3D), C.POINTER(Fields3D)
+    sig = {
+        "cvlbm2d_run": (i32, [P2, F2, f64, i64, i32, i32, pI]),
+        "cvlbm2d_apply_boundary": (i32, [P2, F2, f64, i32, pI]),
+        "cvlbm2d_refresh": (i32, [P2, F2, pI]),
+        "cvlbm2d_stress": (i32, [P2, F2, pI]),
+        "cvlbm3d_run": (i32, [P3, F3, f64, i64, i32, i32, pI]),
+        "cvlbm3d_apply_boundary": (i32, [P3, F3, f64, i32, pI]),
+        "cvlbm3d_refresh": (i32, [P3, F3, pI]),
+        "cvlbm3d_set_ustar": (i32, [P3, F3, pI, pI]),
+        "cvlbm2d_graph_create": (i32, [P2, F2, i64, i32, C.POINTER(pI)]),
+        "cvlbm3d_graph_create": (i32, [P3, F3, i64, i32, C.POINTER(pI)]),
+        "cvlbm_graph_launch": (i32, [pI, pI]),
+        "cvlbm_graph_destroy": (None, [pI]),
+        "cvlbm_version": (i32, []),
+        "cvlbm_last_error": (C.c_char_p, []),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(rc: int, what: str) -> None:
+    if rc != 0:
+        msg = load().cvlbm_last_error()
+        text = msg.decode() if msg else ""
+        raise RuntimeError(f"{what} failed with code {rc}: {text}")
+
+
+def torch_device(device: str | None):
+    """Resolve a device string to a CUDA torch.device; CPU is rejected."""
+    import torch
+
+    name = device or os.environ.get("WARP_DEVICE") or "cuda:0"
+    if not str(name).startswith("cuda"):
+        raise ValueError(
+            f"device {name!r} is not supported: this implementation runs only on CUDA devices")
+    if not torch.cuda.is_available():
+        raise RuntimeError("a CUDA device is required (no CPU fallback)")
+    return torch.device(name)
+
+
+def stream_ptr(device) -> int:
+    import torch
+
+    return int(torch.cuda.current_stream(device).cuda_stream)
+
+
+def ptr(t) -> int:
+    return 0 if t is None else int(t.data_ptr())

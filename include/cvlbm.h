@@ -1,0 +1,229 @@
+/*
+ * cvlbm.h -- C ABI of libcvlbm.so, the sm_100a implementation of the
+ * curved-boundary vectorial lattice Boltzmann (VLBM) time step.
+ *
+ * The reference (JingsenFeng/curved-boundary-vlbm, curved_lbm 1.0.0) exposes
+ * this path only as two Python solver classes whose methods launch Warp
+ * kernels; it has no plugin system and no C interface.  Every entry point
+ * below replaces one of those methods; the citation in front of each names
+ * the reference method (file:line inside the reference project) whose device
+ * work it performs.  The Python drop-in package (curved_lbm.*) binds these
+ * symbols with ctypes; INTEGRATION.md shows the binding a maintainer would
+ * add to the reference.
+ *
+ * Conventions
+ *   - Every pointer inside a *_problem or *_fields struct is a device pointer
+ *     (cudaMalloc / torch CUDA storage) unless stated otherwise.
+ *   - All floating point is IEEE binary64; indices and flags are int32.
+ *   - 2-D node arrays are dense [component][i][j] with j fastest
+ *     (N = nx*ny nodes); 3-D node arrays are compacted active nodes
+ *     [component][p] (N = n_active).
+ *   - Functions return CVLBM_OK (0) or a negative error code; they never
+ *     throw across the ABI.  cvlbm_last_error() returns a thread-local message.
+ *   - `stream` is a cudaStream_t passed as void*; NULL is the legacy stream.
+ *     All work is asynchronous on that stream.
+ *   - Device-side failures (non-positive Jacobian) never trap: kernels set
+ *     fields->invalid[0] to a nonzero value, as the reference's `invalid`
+ *     flag does.
+ */
+#ifndef CVLBM_H
+#define CVLBM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CVLBM_OK 0
+#define CVLBM_ERR_INVALID_ARG (-1)
+#define CVLBM_ERR_CUDA (-2)
+#define CVLBM_ERR_UNSUPPORTED (-3)
+
+/* Material ids (curved_lbm two_d/vector_nonlinear_elastic_warp.py:37-43,
+ * three_d/vector_nonlinear_elastic_warp3d.py:34-40). */
+#define CVLBM_MATERIAL_SVK 0
+#define CVLBM_MATERIAL_NEO_HOOKE 1
+#define CVLBM_MATERIAL_LOG_NEO_HOOKE 2
+#define CVLBM_MATERIAL_MOONEY_RIVLIN 3
+#define CVLBM_MATERIAL_YEOH 4
+#define CVLBM_MATERIAL_GENT 5
+#define CVLBM_MATERIAL_SUGIYAMA_SVK_2D 6 /* 2-D id 6 */
+#define CVLBM_MATERIAL_SPH_NEO_HOOKE_3D 6 /* 3-D id 6 */
+
+typedef struct cvlbm_material {
+  int32_t model;
+  int32_t reserved;
+  double lam, mu, p0, p1, p2;
+  double j_floor;
+} cvlbm_material;
+
+/* ------------------------------------------------------------------------ */
+/* D2Q4x6                                                                    */
+/* ------------------------------------------------------------------------ */
+
+/* Static description of one 2-D problem: lattice, material, boundary tables
+ * and cut-link geometry.  Mirrors the constructor state of
+ * WarpCurvedBoundaryLBM2D (two_d/curved_boundary_warp.py:3621-3843). */
+typedef struct cvlbm2d_problem {
+  int32_t nx, ny;
+  int32_t n_links;
+  int32_t recon;         /* reconstruction id, two_d numbering (0 bfl, 2 lsq_bfl,
+                            9 compat_bfl, 11 local_char2, 12 local_f, 13 local_f_bfl) */
+  int32_t normal_solver; /* 0 finite-difference Newton, 1 acoustic Newton, 2 energy */
+  int32_t source_mode;   /* 0 none, 1 constant, 2 damping */
+  double dx, dy, dt, omega, c;
+  double source[6];
+  cvlbm_material mat;
+  int32_t disp_interval;   /* local displacement sweep every N steps (0 = off) */
+  int32_t disp_sweeps;     /* sweeps per due step, 1..8 */
+  int32_t disp_bid;        /* anchor boundary id, <0: all Dirichlet ids */
+  int32_t rep_interval;    /* local F repair every N steps (0 = off) */
+  int32_t interior_only;   /* repair only nodes with four active neighbours */
+  int32_t use_dynamic_traction;
+  double relax, weight, blend;
+  /* geometry, all device pointers */
+  const int32_t *active;                      /* [nx*ny] 0/1 */
+  const int32_t *link_i, *link_j, *link_q, *link_bid;
+  const double *link_eta, *link_xb, *link_yb, *link_nx, *link_ny;
+  const int32_t *lsq_i, *lsq_j;               /* [n_links*24] */
+  const double *lsq_wb, *lsq_wt, *lsq_wx, *lsq_wy;
+  const int32_t *lsq_valid;                   /* [n_links] */
+  const int32_t *node_link_start;             /* [nx*ny+1] CSR of links per node */
+  const int32_t *node_link_list;              /* [n_links], ascending within a node */
+  const int32_t *bc_kind, *bc_mode;           /* [8] per boundary id */
+  const double *bc_params;                    /* [8*8] */
+  const double *traction_x, *traction_y;      /* [n_links] dynamic traction */
+} cvlbm2d_problem;
+
+/* Mutable state.  f0 is the current population field; a run swaps f0 and f1
+ * once per step and writes the swapped pointers back. */
+typedef struct cvlbm2d_fields {
+  double *f0, *f1, *fpost;  /* [24*N] */
+  double *U;                /* [6*N]  v_x v_y F11 F12 F21 F22 */
+  double *u, *u_next;       /* [2*N]  displacement, sweep scratch */
+  double *u_star;           /* [2*N]  trapezoidal half-step displacement */
+  double *P, *sigma;        /* [4*N]  first Piola and Cauchy stress */
+  int32_t *invalid;         /* [1]    sticky flag, reset at the start of a run */
+  double *clock;            /* [1]    device time; used when graph_mode != 0 */
+} cvlbm2d_fields;
+
+/* Advance `nsteps` time steps starting at host time `time0` and step index
+ * `step0` (used for the displacement/repair interval test).  Replaces
+ * WarpCurvedBoundaryLBM2D.step (two_d/curved_boundary_warp.py:4163-4258)
+ * called nsteps times.  With graph_mode != 0 the kernels read the time from
+ * fields->clock and advance it, so the launch sequence can be captured in a
+ * CUDA graph and replayed; nsteps must then be even. */
+int cvlbm2d_run(const cvlbm2d_problem *p, cvlbm2d_fields *f, double time0, int64_t step0,
+                int32_t nsteps, int32_t graph_mode, void *stream);
+
+/* Cut-link reconstruction at time t, fpost -> f1, or in place on f0 through a
+ * frozen copy in fpost.  Replaces apply_boundary_reconstruction
+ * (two_d/curved_boundary_warp.py:4020-4035). */
+int cvlbm2d_apply_boundary(const cvlbm2d_problem *p, cvlbm2d_fields *f, double t,
+                           int32_t in_place, void *stream);
+
+/* Recompute U, u, P, sigma from f0 and u_star and reset `invalid`.
+ * Replaces refresh_current (two_d/curved_boundary_warp.py:4260-4291). */
+int cvlbm2d_refresh(const cvlbm2d_problem *p, cvlbm2d_fields *f, void *stream);
+
+/* First Piola stress and Cauchy stress of the current U buffer at active
+ * nodes (inactive nodes untouched).  The reference stores P and sigma in its
+ * collision and repair kernels (two_d/curved_boundary_warp.py:1795-1803,
+ * 3603-3615); this library evaluates them on demand from the same U. */
+int cvlbm2d_stress(const cvlbm2d_problem *p, cvlbm2d_fields *f, void *stream);
+
+/* ------------------------------------------------------------------------ */
+/* D3Q6x12 (compacted active nodes)                                          */
+/* ------------------------------------------------------------------------ */
+
+/* Mirrors the constructor state of WarpSparseCurvedBoundaryLBM3D
+ * (three_d/curved_boundary_warp3d.py:3859-4071). */
+typedef struct cvlbm3d_problem {
+  int32_t n_active, n_links;
+  int32_t nx, ny, nz;
+  int32_t recon;         /* three_d numbering: 0 bfl, 1 halfway, 2 compat_bfl,
+                            3 local_f, 4 local_f_bfl */
+  int32_t normal_solver; /* 0 finite-difference Newton, 1 acoustic Newton, 2 energy */
+  int32_t source_mode;
+  int32_t has_char;      /* characteristic stencil present (local_f + Neumann) */
+  int32_t has_tangent_lsq;
+  int32_t disp_interval, disp_sweeps, disp_bid, rep_interval;
+  double dx, dy, dz, dt, omega, c;
+  double source[12];
+  cvlbm_material mat;
+  double relax, weight, blend;
+  const int32_t *active_i, *active_j, *active_k; /* [n_active] */
+  const int32_t *neighbor;                        /* [6*n_active], -1 = none */
+  const int32_t *link_p, *link_up, *link_q, *link_bid;
+  const double *link_eta, *link_xb, *link_yb, *link_zb, *link_nx, *link_ny, *link_nz;
+  const int32_t *lsq_p;                           /* [n_links*32] */
+  const double *lsq_wt1, *lsq_wt2;
+  const int32_t *lsq_valid;
+  const int32_t *char_idx;                        /* [64*n_links] */
+  const double *char_w;                           /* [4*64*n_links] */
+  const int32_t *node_link_start, *node_link_list;/* CSR of links per active node */
+  const int32_t *bc_kind, *bc_mode;               /* [16] */
+  const int32_t *bc_comp_kind;                    /* [3*16] */
+  const double *bc_params;                        /* [16*16] */
+  const int32_t *dyn_enabled;                     /* [n_links] */
+  const double *dyn_traction;                     /* [3*n_links] */
+} cvlbm3d_problem;
+
+typedef struct cvlbm3d_fields {
+  double *f0, *f1;          /* [72*N]; f0 is collided in place */
+  double *U;                /* [12*N] */
+  double *u, *u_next, *u_star; /* [3*N] */
+  int32_t *link_kind, *link_comp_kind; /* [n_links], [3*n_links] */
+  double *link_bv;          /* [3*n_links] */
+  double *link_Fb, *link_Pb;/* [9*n_links] */
+  double *char_state;       /* [4*12*n_links] value, d/dx, d/dy, d/dz */
+  int32_t *invalid;
+  double *clock;
+} cvlbm3d_fields;
+
+/* Replaces WarpSparseCurvedBoundaryLBM3D.step
+ * (three_d/curved_boundary_warp3d.py:4549-4589) called nsteps times. */
+int cvlbm3d_run(const cvlbm3d_problem *p, cvlbm3d_fields *f, double time0, int64_t step0,
+                int32_t nsteps, int32_t graph_mode, void *stream);
+
+/* Replaces apply_boundary_reconstruction (three_d/curved_boundary_warp3d.py:4339-4399):
+ * link preparation (gather, Newton, Piola), BFL rows and characteristic rows. */
+int cvlbm3d_apply_boundary(const cvlbm3d_problem *p, cvlbm3d_fields *f, double t,
+                           int32_t in_place, void *stream);
+
+/* Replaces refresh_current (three_d/curved_boundary_warp3d.py:4401-4424). */
+int cvlbm3d_refresh(const cvlbm3d_problem *p, cvlbm3d_fields *f, void *stream);
+
+/* Replaces the _sparse_set_ustar launch of _initialize_from_active
+ * (three_d/curved_boundary_warp3d.py:2096-2106, 4270-4277):
+ * u_star = displacement - dt/2 * v. */
+int cvlbm3d_set_ustar(const cvlbm3d_problem *p, cvlbm3d_fields *f, const double *displacement,
+                      void *stream);
+
+/* ------------------------------------------------------------------------ */
+/* CUDA graphs of whole step sequences                                       */
+/* ------------------------------------------------------------------------ */
+
+typedef struct cvlbm_graph cvlbm_graph;
+
+/* Capture `nsteps` (even) steps of cvlbm2d_run / cvlbm3d_run in graph mode
+ * into an executable CUDA graph.  The graph keeps the field pointers it was
+ * captured with; it is valid for replays whose starting step index has the
+ * same phase modulo the displacement and repair intervals. */
+int cvlbm2d_graph_create(const cvlbm2d_problem *p, const cvlbm2d_fields *f, int64_t step0,
+                         int32_t nsteps, cvlbm_graph **out);
+int cvlbm3d_graph_create(const cvlbm3d_problem *p, const cvlbm3d_fields *f, int64_t step0,
+                         int32_t nsteps, cvlbm_graph **out);
+int cvlbm_graph_launch(cvlbm_graph *g, void *stream);
+void cvlbm_graph_destroy(cvlbm_graph *g);
+
+/* Library version (major*10000 + minor*100 + patch) and last error text. */
+int cvlbm_version(void);
+const char *cvlbm_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CVLBM_H */

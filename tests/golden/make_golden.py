@@ -418,7 +418,23 @@ def run_2d(c2, v2, name, case, out_dir):
         solver_kw["source_vector"] = tuple(solver_kw["source_vector"])
     solver = c2.WarpCurvedBoundaryLBM2D(geom, material=material, boundary=boundary, **solver_kw)
     U0, disp0 = initial_state_2d(case["init"], geom)
-    solver.initialize_from_numpy(U=U0, displacement=disp0, init_order=case["init"]["init_order"])
+    order = case["init"]["init_order"]
+    # host-side populations exactly as initialize_from_numpy builds them
+    if order == 1:
+        f_host = v2._equilibrium_np(U0, material, solver.lattice_speed)
+        f_host -= (0.5 * solver.dt / float(v2.Q)) * v2._source_np(
+            U0, solver.source_mode, solver.source_params)[None, ...]
+    elif order == 2:
+        f_host = v2._second_order_populations_np(
+            U0, material, solver.lattice_speed, dx=solver.dx, dy=solver.dy, dt=solver.dt,
+            periodic_x=False, periodic_y=False, source_mode=solver.source_mode,
+            source_params=solver.source_params)
+    else:
+        f_host = v2._second_order_populations_masked_np(
+            U0, solver.active_np.astype(bool), material, solver.lattice_speed, dx=solver.dx,
+            dy=solver.dy, dt=solver.dt, periodic_x=False, periodic_y=False,
+            source_mode=solver.source_mode, source_params=solver.source_params)
+    solver.initialize_from_numpy(U=U0, displacement=disp0, init_order=order)
     f0_init = solver.numpy_field("f0").copy()
     ustar_init = solver.numpy_field("u_star").copy()
     for _ in range(case["steps"]):
@@ -432,6 +448,7 @@ def run_2d(c2, v2, name, case, out_dir):
         config=json.dumps(dict(case, dim=2)),
         U0=U0,
         disp0=disp0,
+        f_host=f_host,
         f0_init=f0_init,
         ustar_init=ustar_init,
         f0=f0,
@@ -469,6 +486,10 @@ def run_3d(c3, name, case, out_dir):
     material = c3.WarpHyperelasticMaterial3D.from_poisson(mat["model"], mat["poisson"], mu=mat["mu"])
     boundary = c3.CurvedBoundarySpec3D(**boundary_kwargs(case["boundary"]))
     solver = c3.WarpSparseCurvedBoundaryLBM3D(geom, material=material, boundary=boundary, **case["solver"])
+    U_id = np.zeros((12, solver.n_active))
+    U_id[3] = U_id[7] = U_id[11] = 1.0
+    f_host = c3._equilibrium_np(U_id, material, solver.lattice_speed)
+    f_host -= 0.5 * solver.dt / float(c3.Q) * solver._source_active_np(U_id)[None, ...]
     solver.initialize_identity(init_order=case["init"]["init_order"])
     f0_init = np.asarray(solver.f0.numpy()).copy()
     ustar_init = np.asarray(solver.u_star.numpy()).copy()
@@ -478,6 +499,7 @@ def run_3d(c3, name, case, out_dir):
     ustar = np.asarray(solver.u_star.numpy()).copy()
     out = dict(
         config=json.dumps(dict(case, dim=3)),
+        f_host=f_host.reshape(72, -1),
         f0_init=f0_init,
         ustar_init=ustar_init,
         f0=f0,

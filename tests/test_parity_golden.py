@@ -1,0 +1,98 @@
+"""CUDA time step against the reference, on fixtures the reference produced.
+
+Each case is rebuilt with this package from the fixture's JSON config,
+initialised, stepped, and compared with the reference's own state.  The
+kernels are compiled with --fmad=false and keep the reference's operation
+order, so agreement is at round-off level; the bar asserted here is the
+north-star tolerance, relative 1e-12 on populations, displacement and F
+(absolute floor 1e-15 for entries that are zero).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import cases
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-12
+ATOL = 1e-15
+
+GOLD2 = ["g2_affine_compat", "g2_traction_localf", "g2_bfl_mixed_fd", "g2_energy_intervals"]
+GOLD3 = ["g3_shell_localf", "g3_shell_bfl_fd", "g3_shell_compat"]
+
+
+def close(name, got, ref, rtol=RTOL, atol=ATOL):
+    got, ref = np.asarray(got), np.asarray(ref)
+    assert got.shape == ref.shape, (name, got.shape, ref.shape)
+    err = np.abs(got - ref)
+    tol = atol + rtol * np.abs(ref)
+    bad = err > tol
+    assert not bad.any(), (f"{name}: {int(bad.sum())} entries off, max abs err "
+                           f"{float(err.max()):.3e}, max |ref| {float(np.abs(ref).max()):.3e}")
+
+
+@pytest.mark.parametrize("name", GOLD2)
+def test_2d_steps_match_reference(golden_dir, name):
+    d, cfg = cases.load(golden_dir / f"{name}.npz")
+    s = cases.solver_2d(cfg)
+    U0, disp0 = cases.initial_state_2d(cfg["init"], s.geometry)
+    s.initialize_from_numpy(U=U0, displacement=disp0, init_order=cfg["init"]["init_order"])
+    close("f0_init", s.numpy_field("f0"), d["f0_init"])
+    close("ustar_init", s.numpy_field("u_star"), d["ustar_init"])
+    for _ in range(cfg["steps"]):
+        s.step()
+    close("f0", s.numpy_field("f0"), d["f0"])
+    close("u_star", s.numpy_field("u_star"), d["ustar"])
+    close("U_step", s.numpy_field("U"), d["U_step"])
+    close("u_step", s.numpy_field("u"), d["u_step"])
+    assert s.time == float(d["time"])
+    s.refresh_current()
+    close("U", s.numpy_field("U"), d["U"])
+    close("u", s.numpy_field("u"), d["u"])
+    close("P", s.numpy_field("P"), d["P"])
+    close("sigma", s.numpy_field("sigma"), d["sigma"])
+
+
+@pytest.mark.parametrize("name", GOLD3)
+def test_3d_steps_match_reference(golden_dir, name):
+    d, cfg = cases.load(golden_dir / f"{name}.npz")
+    s = cases.solver_3d(cfg)
+    s.initialize_identity(init_order=cfg["init"]["init_order"])
+    close("f0_init", s.active_populations(), d["f0_init"])
+    close("ustar_init", s.active_ustar(), d["ustar_init"])
+    for _ in range(cfg["steps"]):
+        s.step()
+    close("f0", s.active_populations(), d["f0"])
+    close("u_star", s.active_ustar(), d["ustar"])
+    close("link_Fb", s.link_Fb.cpu().numpy(), d["link_Fb"])
+    close("link_Pb", s.link_Pb.cpu().numpy(), d["link_Pb"])
+    close("link_bv", s.link_bv.cpu().numpy(), d["link_bv"])
+    if s.characteristic_stencil is not None:
+        close("char_state", s.char_state.cpu().numpy(), d["char_state"])
+    s.refresh_current()
+    close("U", s.active_system_state(), d["U"])
+    close("u", s.active_displacement(), d["u"])
+
+
+def test_3d_dirichlet_bfl_regression(golden_dir):
+    """The reference's own Warp-generated regression (tests/test_characteristics.py:43-67)."""
+    from curved_lbm.three_d import curved_boundary_warp3d as cb
+
+    ref = np.load(golden_dir / "dirichlet_bfl_3d_reference.npz")
+    g = cb.CurvedBoundaryGeometry3D.sphere(nx=20, ny=20, nz=20, radius=0.35)
+    material = cb.WarpHyperelasticMaterial3D.from_poisson("neo_hooke", 0.2, mu=1.0)
+    boundary = cb.CurvedBoundarySpec3D(kind="neumann", component_kinds=("dirichlet",) * 3,
+                                       value_mode=cb.CURVED3D_VALUE_CONSTANT_VECTOR,
+                                       params=(0.001, 0.002, -0.001))
+    s = cb.WarpCurvedBoundaryLBM3D(g, material=material, boundary=boundary,
+                                   boundary_reconstruction="local_f", lattice_speed=10.0,
+                                   collision_omega=1.8)
+    s.initialize_from_numpy(U=ref["U"], apply_initial_boundaries=False)
+    for _ in range(25):
+        s.step()
+    np.testing.assert_allclose(s.active_populations(), ref["f25"], rtol=0, atol=1e-13)
+    assert s.characteristic_stencil is None
+    assert s.summary()["characteristic_cut_links"] == 0
