@@ -1,0 +1,441 @@
+#!/usr/bin/env python3
+"""Throughput benchmark of the curved-boundary VLBM time step on B200.
+
+Metric: MLUPS (million active-node updates per second, FP64), reported as
+an absolute figure and as a fraction of the measured HBM roofline.
+
+Workloads (synthetic, seeded geometry; no external data):
+  annulus512  D2Q4x6 traction annulus, 512^2 lattice on [0,1.1]^2, inner
+              r=0.25 clamped, outer r=0.5 radial nominal traction ramped
+              linearly 0 -> 0.05 over 20000 steps (then held); c=10,
+              omega=1.8, alpha_u=0.85, theta_F=0.5, w_D=100, gamma=10,
+              neo-Hooke mu=1, lambda=1; local_f closure, one displacement
+              sweep and one F repair per step.  (Default.)
+  shell192    D3Q6x12 spherical shell, 192^3 lattice on [0,2.2]^3, inner
+              r=0.5 clamped, outer r=1.0 radial traction ramped 0 -> 0.05
+              over 10000 steps; same physical parameters.
+
+One bench step = `--inner` lattice time steps replayed from one CUDA graph.
+L2 (126 MB) is flushed between bench steps, outside the timed events.
+
+Multi-GPU: the single-domain workloads do not shard, so each rank advances
+an independent replica (weak scaling, no collectives on the data path);
+`value` is the sum over ranks divided by the slowest rank's device time.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "curved-boundary-vlbm_b200"))
+sys.path.insert(0, str(ROOT))
+
+BYTES_PER_UPDATE = {"annulus512": 416.0, "shell192": 1200.0}
+HBM_FALLBACK_GBS = 6650.0
+
+
+# ---------------------------------------------------------------------------
+# workloads
+# ---------------------------------------------------------------------------
+def annulus_config(n=512):
+    L = 1.1
+    dx = L / n
+    dt = dx / 10.0
+    ramp = 20000 * dt
+    return dict(
+        geometry=dict(nx=n, ny=n, length_x=L, length_y=L, center_x=0.55, center_y=0.55,
+                      inner_radius=0.25, outer_radius=0.5),
+        boundary=dict(kind="neumann", value_mode=105, params=(0.05, ramp),
+                      id_kinds={1: "neumann", 2: "dirichlet"}, id_value_modes={1: 105, 2: 0},
+                      id_params={1: (0.05, ramp), 2: ()}),
+        solver=dict(lattice_speed=10.0, collision_omega=1.8, boundary_reconstruction="local_f",
+                    source_mode="damping", damping_gamma=10.0, local_displacement_interval=1,
+                    local_displacement_sweeps=1, local_displacement_relax=0.85,
+                    local_displacement_boundary_weight=100.0, local_displacement_boundary_id=2,
+                    local_compatibility_interval=1, local_compatibility_blend=0.5,
+                    local_compatibility_interior_only=False),
+    )
+
+
+def shell_config(n=192):
+    L = 2.2
+    dt = (L / n) / 10.0
+    ramp = 10000 * dt
+    return dict(
+        n=n, L=L, ri=0.5, ro=1.0,
+        boundary=dict(kind="neumann", value_mode=208, params=(0.05, ramp),
+                      id_kinds={1: "neumann", 2: "dirichlet"}, id_value_modes={1: 208, 2: 0},
+                      id_params={1: (0.05, ramp), 2: ()}),
+        solver=dict(lattice_speed=10.0, collision_omega=1.8, boundary_reconstruction="local_f",
+                    source_mode="damping", damping_gamma=10.0, local_displacement_interval=1,
+                    local_displacement_sweeps=1, local_displacement_relax=0.85,
+                    local_displacement_boundary_weight=100.0, local_displacement_boundary_id=2,
+                    local_compatibility_interval=1, local_compatibility_blend=0.5),
+    )
+
+
+def build_annulus(device=None, n=512, oracle=False, threads=1):
+    from curved_lbm.two_d import curved_boundary_warp as c2
+
+    cfg = annulus_config(n)
+    geom = c2.CurvedBoundaryGeometry.annulus(**cfg["geometry"])
+    mat = c2.WarpHyperelasticMaterial(model="neo_hooke", lam=1.0, mu=1.0)
+    spec = c2.CurvedBoundarySpec(**cfg["boundary"])
+    U = np.zeros((6, n, n))
+    U[2] = U[5] = 1.0
+    if oracle:
+        from oracle.oracle import Oracle2D
+
+        s = Oracle2D(geom, material=mat, boundary=spec, threads=threads, **cfg["solver"])
+    else:
+        s = c2.WarpCurvedBoundaryLBM2D(geom, material=mat, boundary=spec, device=device,
+                                       **cfg["solver"])
+    s.initialize_from_numpy(U=U, displacement=np.zeros((2, n, n)), init_order=2)
+    return s, geom.n_active
+
+
+def shell_geometry(n=192):
+    from curved_lbm.three_d import curved_boundary_warp3d as c3
+
+    cfg = shell_config(n)
+    L, ri, ro = cfg["L"], cfg["ri"], cfg["ro"]
+    c = 0.5 * L
+
+    def phiv(X, Y, Z):
+        R = np.sqrt((X - c) ** 2 + (Y - c) ** 2 + (Z - c) ** 2)
+        return np.maximum(R - ro, ri - R)
+
+    def normv(X, Y, Z):
+        X, Y, Z = np.broadcast_arrays(X, Y, Z)
+        dx, dy, dz = X - c, Y - c, Z - c
+        R = np.maximum(np.sqrt(dx * dx + dy * dy + dz * dz), 1e-30)
+        s = np.where(np.abs(R - ri) <= np.abs(R - ro), -1.0, 1.0)
+        return s * dx / R, s * dy / R, s * dz / R
+
+    def bid(x, y, z, *_):
+        r = math.sqrt((x - c) ** 2 + (y - c) ** 2 + (z - c) ** 2)
+        return 2 if abs(r - ri) <= abs(r - ro) else 1
+
+    return c3.CurvedBoundaryGeometry3D.from_level_set(
+        nx=n, ny=n, nz=n, length_x=L, length_y=L, length_z=L,
+        phi=lambda x, y, z: float(phiv(np.asarray(x), np.asarray(y), np.asarray(z))),
+        boundary_id=bid, phi_vectorized=phiv, normal_vectorized=normv, label="shell")
+
+
+def build_shell(device=None, n=192, oracle=False, threads=1):
+    from curved_lbm.three_d import curved_boundary_warp3d as c3
+
+    cfg = shell_config(n)
+    geom = shell_geometry(n)
+    mat = c3.WarpHyperelasticMaterial3D(model="neo_hooke", lam=1.0, mu=1.0)
+    spec = c3.CurvedBoundarySpec3D(**cfg["boundary"])
+    if oracle:
+        from oracle.oracle import Oracle3D
+
+        s = Oracle3D(geom, material=mat, boundary=spec, threads=threads, **cfg["solver"])
+        s.initialize_identity()
+        return s, s.N
+    s = c3.WarpSparseCurvedBoundaryLBM3D(geom, material=mat, boundary=spec, device=device,
+                                         **cfg["solver"])
+    return s, s.n_active
+
+
+BUILDERS = {"annulus512": build_annulus, "shell192": build_shell}
+
+
+# ---------------------------------------------------------------------------
+# measurement helpers
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([v.strip() for v in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows if len(r) >= 9
+                          for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def measured_peaks():
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        try:
+            return json.loads(path.read_text()), "measured"
+        except Exception:
+            pass
+    return {"hbm_gbs": HBM_FALLBACK_GBS}, "fallback"
+
+
+def ncu_traffic(workload: str):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
+    path = ROOT / "profiles" / "traffic.json"
+    if not path.exists():
+        return None
+    try:
+        return json.loads(path.read_text()).get(workload)
+    except Exception:
+        return None
+
+
+def cpu_baseline(workload: str, steps: int, threads: int):
+    """Oracle (C port of the reference kernels) on the host cores, bounded sample."""
+    from oracle import oracle as orc
+
+    orc.load()
+    builder = BUILDERS[workload]
+    s, n_active = builder(oracle=True, threads=threads)
+    s.step()  # warm the page cache and OpenMP pool
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        s.step()
+    dt = time.perf_counter() - t0
+    return {"value": n_active * steps / dt / 1e6, "unit": "MLUPS", "cores": threads,
+            "kind": "port",
+            "sample": f"{steps} lattice time steps of {workload} ({n_active} active nodes), "
+                      f"oracle/cvlbm_oracle.c, OpenMP {threads} threads, {dt:.2f} s"}
+
+
+# ---------------------------------------------------------------------------
+def init_dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        dist.init_process_group(backend, timeout=timedelta(seconds=600))
+    return world, rank, local
+
+
+def reference_arm(args, world, rank):
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    base = cpu_baseline(args.workload, max(1, args.ref_steps), threads)
+    line = {
+        "impl": "reference", "metric": "MLUPS FP64", "value": base["value"], "unit": "MLUPS",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "lbm_steps_per_bench_step": args.inner},
+        "cpu_baseline": base,
+        "e2e": {"value": base["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "note": "reference Warp 1.10.1 is not installable here (no wheel, no network); the "
+                "reference arm times oracle/cvlbm_oracle.c, a C port of its kernels pinned "
+                "to its own outputs",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="annulus512", choices=sorted(BUILDERS))
+    ap.add_argument("--inner", type=int, default=100, help="lattice steps per bench step")
+    ap.add_argument("--ref-steps", type=int, default=4, help="oracle steps for the CPU legs")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    if args.inner % 2:
+        args.inner += 1
+    world, rank, local = init_dist()
+    if args.impl == "reference":
+        rc = reference_arm(args, world, rank)
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+        return rc
+
+    import torch
+
+    from curved_lbm import _native
+
+    dev = torch.device(f"cuda:{local}")
+    torch.cuda.set_device(dev)
+    solver, n_active = BUILDERS[args.workload](device=str(dev))
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 8, dtype=torch.float64, device=dev)
+
+    timer = _native.KernelTimer(args.inner)
+    timer.attach()
+    n0 = _native.launch_count()
+    graph = solver.capture_graph(args.inner)
+    launches_per_graph = _native.launch_count() - n0
+    timer.detach()
+
+    for _ in range(args.warmup):
+        graph.launch()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+    step_ms, kern_ms, kern_n = [], 0.0, 0
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+        for _ in range(args.steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            graph.launch()
+            e1.record(stream)
+            e1.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+            ms, cnt = timer.elapsed()
+            kern_ms += ms
+            kern_n += cnt
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+    total_ms = float(sum(step_ms))
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    updates = float(n_active) * args.inner * args.steps * world
+    value = updates / (total_ms * 1e-3) / 1e6
+
+    # end to end through the public API: pinned host traction -> device,
+    # lattice steps, invalid/finite check read back to the host
+    e2e = None
+    if hasattr(solver, "enable_dynamic_link_traction"):
+        nl = solver.geometry.n_links
+        hx = torch.empty(nl, dtype=torch.float64).pin_memory()
+        hy = torch.empty(nl, dtype=torch.float64).pin_memory()
+        nxv = torch.as_tensor(solver.geometry.link_nx)
+        nyv = torch.as_tensor(solver.geometry.link_ny)
+        out = torch.empty(2, dtype=torch.float64).pin_memory()
+        amp, ramp = solver.boundary_params[0], solver.boundary_params[1]
+        solver.enable_dynamic_link_traction(True)
+        outer = torch.as_tensor(solver.geometry.link_boundary_id == 1)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            sc = min(solver.time / ramp, 1.0) if ramp > 0 else 1.0
+            hx.copy_(torch.where(outer, amp * sc * nxv, torch.zeros_like(nxv)))
+            hy.copy_(torch.where(outer, amp * sc * nyv, torch.zeros_like(nyv)))
+            solver.link_traction_x.copy_(hx, non_blocking=True)
+            solver.link_traction_y.copy_(hy, non_blocking=True)
+            solver.run(args.inner)
+            vmax = torch.stack([solver.invalid.double().max(),
+                                solver.U[:2].abs().max()])
+            out.copy_(vmax, non_blocking=True)
+            torch.cuda.synchronize(dev)
+        e2e_s = time.perf_counter() - t0
+        solver.enable_dynamic_link_traction(False)
+        e2e = {"value": float(n_active) * args.inner * args.steps * world / e2e_s / 1e6,
+               "unit": "MLUPS", "h2d_bytes_per_step": int(2 * nl * 8),
+               "d2h_bytes_per_step": 16,
+               "path": "WarpCurvedBoundaryLBM2D.run() with dynamic link traction uploaded "
+                       "from pinned host memory each bench step; max|v| and the invalid "
+                       "flag read back"}
+
+    peaks, peak_kind = measured_peaks()
+    avg_kern_s = kern_ms * 1e-3 / max(kern_n, 1)
+    algo_bytes = n_active * BYTES_PER_UPDATE[args.workload]
+    achieved = algo_bytes / avg_kern_s / 1e9 if kern_n else None
+    roofline = {"bound": "hbm", "kernel": "bulk node kernel (bracketed per lattice step)",
+                "achieved": achieved, "peak": peaks.get("hbm_gbs", HBM_FALLBACK_GBS),
+                "peak_kind": peak_kind, "unit": "GB/s",
+                "frac": (achieved / peaks.get("hbm_gbs", HBM_FALLBACK_GBS)) if achieved else None,
+                "traffic": ncu_traffic(args.workload),
+                "algorithmic_bytes_per_launch": algo_bytes,
+                "avg_launch_ms": avg_kern_s * 1e3,
+                "step_frac": (kern_ms / total_ms) if total_ms else None,
+                "whole_step_achieved": updates / world * BYTES_PER_UPDATE[args.workload]
+                / (total_ms * 1e-3) / 1e9}
+    base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            base = cpu_baseline(args.workload, args.ref_steps, os.cpu_count() or 1)
+        except Exception as exc:  # the oracle is optional for the GPU number
+            base = {"value": None, "unit": "MLUPS", "cores": 0, "kind": "port",
+                    "sample": f"unavailable: {exc}"}
+    line = {
+        "metric": "MLUPS FP64", "value": value, "unit": "MLUPS", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "n_active": int(n_active),
+                   "lbm_steps_per_bench_step": args.inner,
+                   "l2": "flushed between bench steps (256 MB write)",
+                   "parallelism": f"replicas x{world}"},
+        "e2e": e2e, "roofline": roofline, "cpu_baseline": base,
+        "clocks": clocks.summary(),
+        "gpu_launches": int(launches_per_graph * args.steps),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    del graph
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

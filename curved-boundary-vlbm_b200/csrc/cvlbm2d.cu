@@ -657,7 +657,7 @@ void launch_links(const Ctx2& c, const double* src, double* dst, const double* U
                   const double* u, const double* clock, double t, double offset,
                   cudaStream_t s) {
   if (c.p.n_links <= 0) return;
-  k_links2<<<blocks(c.p.n_links, 128), 128, 0, s>>>(c, src, dst, U, u, clock, t, offset);
+  k_links2<<<blocks(c.p.n_links, 128), 128, 0, s>>>(c, src, dst, U, u, clock, t, offset); cv::count_launches(1);
 }
 
 }  // namespace
@@ -673,21 +673,23 @@ extern "C" int cvlbm2d_run(const cvlbm2d_problem* p, cvlbm2d_fields* f, double t
   const int N = c.N;
   const unsigned nb = blocks(N, 256);
   const double* clock = graph_mode ? f->clock : nullptr;
-  k_zero_flag<<<1, 1, 0, s>>>(f->invalid);
+  k_zero_flag<<<1, 1, 0, s>>>(f->invalid); cv::count_launches(1);
   double t = time0;
   for (int k = 0; k < nsteps; ++k) {
     const long long step = step0 + k;
-    k_collide2<<<nb, 256, 0, s>>>(c, f->f0, f->fpost, f->U, f->u, f->u_star, f->invalid);
+    int tk = timer_begin(s);
+    k_collide2<<<nb, 256, 0, s>>>(c, f->f0, f->fpost, f->U, f->u, f->u_star, f->invalid); cv::count_launches(1);
+    timer_end(tk, s);
     if (due(p->disp_interval, step)) {
       for (int sw = 0; sw < p->disp_sweeps; ++sw) {
-        k_sweep2<<<nb, 256, 0, s>>>(c, f->U, f->u, f->u_next, f->u_star, clock, t);
-        k_commit2<<<blocks(2LL * N, 256), 256, 0, s>>>(2 * N, f->u_next, f->u);
+        k_sweep2<<<nb, 256, 0, s>>>(c, f->U, f->u, f->u_next, f->u_star, clock, t); cv::count_launches(1);
+        k_commit2<<<blocks(2LL * N, 256), 256, 0, s>>>(2 * N, f->u_next, f->u); cv::count_launches(1);
       }
     }
-    if (due(p->rep_interval, step)) k_repair2<<<nb, 256, 0, s>>>(c, f->fpost, f->U, f->u);
-    k_stream2<<<nb, 256, 0, s>>>(c, f->fpost, f->f1);
+    if (due(p->rep_interval, step)) k_repair2<<<nb, 256, 0, s>>>(c, f->fpost, f->U, f->u); cv::count_launches(1);
+    k_stream2<<<nb, 256, 0, s>>>(c, f->fpost, f->f1); cv::count_launches(1);
     launch_links(c, f->fpost, f->f1, f->U, f->u, clock, t, 0.5 * p->dt, s);
-    if (graph_mode) k_tick<<<1, 1, 0, s>>>(f->clock, p->dt);
+    if (graph_mode) k_tick<<<1, 1, 0, s>>>(f->clock, p->dt); cv::count_launches(1);
     double* tmp = f->f0;
     f->f0 = f->f1;
     f->f1 = tmp;
@@ -720,9 +722,9 @@ extern "C" int cvlbm2d_refresh(const cvlbm2d_problem* p, cvlbm2d_fields* f, void
   if (!f->P || !f->sigma) return fail(CVLBM_ERR_INVALID_ARG, "missing stress buffers");
   cudaStream_t s = (cudaStream_t)stream;
   Ctx2 c = make_ctx(p);
-  k_zero_flag<<<1, 1, 0, s>>>(f->invalid);
+  k_zero_flag<<<1, 1, 0, s>>>(f->invalid); cv::count_launches(1);
   k_refresh2<<<blocks(c.N, 256), 256, 0, s>>>(c, f->f0, f->U, f->u, f->u_star, f->P, f->sigma,
-                                               f->invalid);
+                                               f->invalid); cv::count_launches(1);
   return check_launch("cvlbm2d_refresh");
 }
 
@@ -731,7 +733,7 @@ extern "C" int cvlbm2d_stress(const cvlbm2d_problem* p, cvlbm2d_fields* f, void*
   if (rc) return rc;
   if (!f->P || !f->sigma) return fail(CVLBM_ERR_INVALID_ARG, "missing stress buffers");
   Ctx2 c = make_ctx(p);
-  k_stress2<<<blocks(c.N, 256), 256, 0, (cudaStream_t)stream>>>(c, f->U, f->P, f->sigma);
+  k_stress2<<<blocks(c.N, 256), 256, 0, (cudaStream_t)stream>>>(c, f->U, f->P, f->sigma); cv::count_launches(1);
   return check_launch("cvlbm2d_stress");
 }
 

@@ -553,24 +553,26 @@ extern "C" int cvlbm3d_run(const cvlbm3d_problem* p, cvlbm3d_fields* f, double t
   Ctx3 c = make_ctx(p);
   const int N = c.N;
   const double* clock = graph_mode ? f->clock : nullptr;
-  k_zero_flag3<<<1, 1, 0, s>>>(f->invalid);
+  k_zero_flag3<<<1, 1, 0, s>>>(f->invalid); cv::count_launches(1);
   double t = time0;
   for (int k = 0; k < nsteps; ++k) {
     const long long step = step0 + k;
-    if (N > 0) k_collide3<<<blocks(N, 128), 128, 0, s>>>(c, f->f0, f->U, f->u, f->u_star, f->invalid);
+    int tk = timer_begin(s);
+    if (N > 0) k_collide3<<<blocks(N, 128), 128, 0, s>>>(c, f->f0, f->U, f->u, f->u_star, f->invalid); cv::count_launches(1);
+    timer_end(tk, s);
     if (N > 0 && due(p->disp_interval, step)) {
       for (int sw = 0; sw < p->disp_sweeps; ++sw) {
-        k_sweep3<<<blocks(N, 256), 256, 0, s>>>(c, f->U, f->u, f->u_next, f->u_star, clock, t);
-        k_copy3<<<blocks(3LL * N, 256), 256, 0, s>>>(3LL * N, f->u_next, f->u);
+        k_sweep3<<<blocks(N, 256), 256, 0, s>>>(c, f->U, f->u, f->u_next, f->u_star, clock, t); cv::count_launches(1);
+        k_copy3<<<blocks(3LL * N, 256), 256, 0, s>>>(3LL * N, f->u_next, f->u); cv::count_launches(1);
       }
     }
     if (N > 0 && due(p->rep_interval, step))
-      k_repair3<<<blocks(N, 128), 128, 0, s>>>(c, f->f0, f->U, f->u);
-    if (N > 0) k_stream3<<<blocks(N, 256), 256, 0, s>>>(c, f->f0, f->f1);
+      k_repair3<<<blocks(N, 128), 128, 0, s>>>(c, f->f0, f->U, f->u); cv::count_launches(1);
+    if (N > 0) k_stream3<<<blocks(N, 256), 256, 0, s>>>(c, f->f0, f->f1); cv::count_launches(1);
     if (p->n_links > 0)
       k_links3<<<blocks(p->n_links, 64), 64, 0, s>>>(c, f->f0, f->f1, f->U, f->u, *f, clock, t,
-                                                     0.5 * p->dt);
-    if (graph_mode) k_tick3<<<1, 1, 0, s>>>(f->clock, p->dt);
+                                                     0.5 * p->dt); cv::count_launches(1);
+    if (graph_mode) k_tick3<<<1, 1, 0, s>>>(f->clock, p->dt); cv::count_launches(1);
     double* tmp = f->f0;
     f->f0 = f->f1;
     f->f1 = tmp;
@@ -590,10 +592,10 @@ extern "C" int cvlbm3d_apply_boundary(const cvlbm3d_problem* p, cvlbm3d_fields* 
     // f1 is scratch until the next streaming step: links read the copy
     cudaMemcpyAsync(f->f1, f->f0, sizeof(double) * kF3 * (size_t)c.N, cudaMemcpyDeviceToDevice, s);
     k_links3<<<blocks(p->n_links, 64), 64, 0, s>>>(c, f->f1, f->f0, f->U, f->u, *f, nullptr, t,
-                                                   0.0);
+                                                   0.0); cv::count_launches(1);
   } else {
     k_links3<<<blocks(p->n_links, 64), 64, 0, s>>>(c, f->f0, f->f1, f->U, f->u, *f, nullptr, t,
-                                                   0.0);
+                                                   0.0); cv::count_launches(1);
   }
   return check_launch("cvlbm3d_apply_boundary");
 }
@@ -603,9 +605,9 @@ extern "C" int cvlbm3d_refresh(const cvlbm3d_problem* p, cvlbm3d_fields* f, void
   if (rc) return rc;
   cudaStream_t s = (cudaStream_t)stream;
   Ctx3 c = make_ctx(p);
-  k_zero_flag3<<<1, 1, 0, s>>>(f->invalid);
+  k_zero_flag3<<<1, 1, 0, s>>>(f->invalid); cv::count_launches(1);
   if (c.N > 0)
-    k_refresh3<<<blocks(c.N, 256), 256, 0, s>>>(c, f->f0, f->U, f->u, f->u_star, f->invalid);
+    k_refresh3<<<blocks(c.N, 256), 256, 0, s>>>(c, f->f0, f->U, f->u, f->u_star, f->invalid); cv::count_launches(1);
   return check_launch("cvlbm3d_refresh");
 }
 
@@ -617,7 +619,7 @@ extern "C" int cvlbm3d_set_ustar(const cvlbm3d_problem* p, cvlbm3d_fields* f,
   cudaStream_t s = (cudaStream_t)stream;
   if (p->n_active > 0)
     k_set_ustar3<<<blocks(p->n_active, 256), 256, 0, s>>>(p->n_active, displacement, f->U,
-                                                          f->u_star, p->dt);
+                                                          f->u_star, p->dt); cv::count_launches(1);
   return check_launch("cvlbm3d_set_ustar");
 }
 

@@ -9,6 +9,13 @@
 
 #include "cvlbm.h"
 
+struct cvlbm_timer {
+  int capacity;
+  int used;
+  cudaEvent_t* begin;
+  cudaEvent_t* end;
+};
+
 struct cvlbm_graph {
   cudaGraph_t graph;
   cudaGraphExec_t exec;
@@ -17,6 +24,23 @@ struct cvlbm_graph {
 namespace cv {
 
 void set_error(const char* msg);
+
+// Launch accounting and the optional per-thread timer of the dominant kernel.
+void count_launches(int n);
+cvlbm_timer* attached_timer();
+
+// Records the begin event of the next timer pair (if a timer is attached and
+// has room) and returns its index, else -1.
+inline int timer_begin(cudaStream_t s) {
+  cvlbm_timer* t = attached_timer();
+  if (!t || t->used >= t->capacity) return -1;
+  int k = t->used++;
+  cudaEventRecordWithFlags(t->begin[k], s, cudaEventRecordExternal);
+  return k;
+}
+inline void timer_end(int k, cudaStream_t s) {
+  if (k >= 0) cudaEventRecordWithFlags(attached_timer()->end[k], s, cudaEventRecordExternal);
+}
 
 inline int fail(int code, const char* msg) {
   set_error(msg);

@@ -99,6 +99,12 @@ EXPORTED = (
     "cvlbm_graph_destroy",
     "cvlbm_version",
     "cvlbm_last_error",
+    "cvlbm_timer_create",
+    "cvlbm_timer_destroy",
+    "cvlbm_timer_reset",
+    "cvlbm_timer_elapsed",
+    "cvlbm_timer_attach",
+    "cvlbm_launch_count",
 )
 
 
@@ -132,6 +138,12 @@ def load(require_cuda: bool = True):
         "cvlbm_graph_launch": (i32, [pI, pI]),
         "cvlbm_graph_destroy": (None, [pI]),
         "cvlbm_version": (i32, []),
+        "cvlbm_timer_create": (i32, [i32, C.POINTER(pI)]),
+        "cvlbm_timer_destroy": (None, [pI]),
+        "cvlbm_timer_reset": (i32, [pI]),
+        "cvlbm_timer_elapsed": (i32, [pI, C.POINTER(f64), C.POINTER(i32)]),
+        "cvlbm_timer_attach": (i32, [pI]),
+        "cvlbm_launch_count": (i64, []),
         "cvlbm_last_error": (C.c_char_p, []),
     }
     for name, (res, args) in sig.items():
@@ -170,3 +182,36 @@ def stream_ptr(device) -> int:
 
 def ptr(t) -> int:
     return 0 if t is None else int(t.data_ptr())
+
+
+class KernelTimer:
+    """CUDA-event pairs around the dominant kernel of every step (see cvlbm.h)."""
+
+    def __init__(self, capacity: int) -> None:
+        self.lib = load()
+        self.handle = C.c_void_p()
+        check(self.lib.cvlbm_timer_create(int(capacity), C.byref(self.handle)), "cvlbm_timer_create")
+
+    def attach(self) -> None:
+        check(self.lib.cvlbm_timer_attach(self.handle), "cvlbm_timer_attach")
+
+    def detach(self) -> None:
+        check(self.lib.cvlbm_timer_attach(None), "cvlbm_timer_attach")
+
+    def reset(self) -> None:
+        check(self.lib.cvlbm_timer_reset(self.handle), "cvlbm_timer_reset")
+
+    def elapsed(self) -> tuple[float, int]:
+        ms, n = C.c_double(0.0), C.c_int32(0)
+        check(self.lib.cvlbm_timer_elapsed(self.handle, C.byref(ms), C.byref(n)), "cvlbm_timer_elapsed")
+        return float(ms.value), int(n.value)
+
+    def __del__(self) -> None:
+        try:
+            self.lib.cvlbm_timer_destroy(self.handle)
+        except Exception:
+            pass
+
+
+def launch_count() -> int:
+    return int(load().cvlbm_launch_count())

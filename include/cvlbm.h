@@ -202,6 +202,30 @@ int cvlbm3d_set_ustar(const cvlbm3d_problem *p, cvlbm3d_fields *f, const double 
                       void *stream);
 
 /* ------------------------------------------------------------------------ */
+/* Kernel timing                                                             */
+/* ------------------------------------------------------------------------ */
+
+/* A ring of CUDA-event pairs.  A run given a timer brackets the dominant
+ * kernel of every step (the bulk node kernel) with the next free pair, on
+ * the launch stream; inside a captured graph the pairs become event nodes
+ * and are re-recorded by every replay.  No counterpart in the reference,
+ * which has no profiling hooks. */
+typedef struct cvlbm_timer cvlbm_timer;
+int cvlbm_timer_create(int32_t capacity, cvlbm_timer **out);
+void cvlbm_timer_destroy(cvlbm_timer *t);
+/* Forget recorded pairs (next run starts at pair 0). */
+int cvlbm_timer_reset(cvlbm_timer *t);
+/* Wait for the recorded pairs and return their summed duration and count. */
+int cvlbm_timer_elapsed(cvlbm_timer *t, double *total_ms, int32_t *count);
+/* Attach (or detach with NULL) the timer used by subsequent runs/captures
+ * on this thread. */
+int cvlbm_timer_attach(cvlbm_timer *t);
+
+/* Number of kernel launches this library has issued (host-side counter;
+ * launches replayed from a CUDA graph are counted once, at capture). */
+int64_t cvlbm_launch_count(void);
+
+/* ------------------------------------------------------------------------ */
 /* CUDA graphs of whole step sequences                                       */
 /* ------------------------------------------------------------------------ */
 
