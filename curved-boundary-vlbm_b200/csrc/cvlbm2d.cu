@@ -348,200 +348,12 @@ __device__ __forceinline__ double interp_link(const double* Uc, const int* act, 
   return v0;
 }
 
-__device__ __forceinline__ double lsq_eval(const cvlbm2d_problem& p, const double* w,
-                                           const double* Uc, int ell) {
-  // two_d/curved_boundary_warp.py:1202-1221 (_lsq_U_at_boundary), valid links only
-  double out = 0.0;
-  const int* li = p.lsq_i + (size_t)ell * kMaxLsq2;
-  const int* lj = p.lsq_j + (size_t)ell * kMaxLsq2;
-  const double* ww = w + (size_t)ell * kMaxLsq2;
-  for (int m = 0; m < kMaxLsq2; ++m) {
-    int ii = li[m], jj = lj[m];
-    if (ii >= 0 && jj >= 0) out += ww[m] * Uc[ii * p.ny + jj];
-  }
-  return out;
-}
 
-__device__ void link2(const Ctx2& c, int ell, const double* __restrict__ fpost,
-                      double* __restrict__ fout, const double* __restrict__ U,
-                      const double* __restrict__ u, double tmid) {
-  const cvlbm2d_problem& p = c.p;
-  const Mat& m = c.m;
-  const int N = c.N, nx = p.nx, ny = p.ny;
-  const int recon = p.recon;
-  const int i = p.link_i[ell], j = p.link_j[ell], qo = p.link_q[ell];
-  int bid = p.link_bid[ell];
-  if (bid < 0 || bid >= kMaxIds2) bid = 0;
-  const int kind = p.bc_kind[bid], mode = p.bc_mode[bid];
-  const double* pp = p.bc_params + bid * 8;
-  int qi = qo + 2;
-  if (qi >= 4) qi -= 4;
-  const double eta = p.link_eta[ell];
-  const double xb = p.link_xb[ell], yb = p.link_yb[ell];
-  const double nxb = p.link_nx[ell], nyb = p.link_ny[ell];
-  const double dxin = (double)cx2(qi), dyin = (double)cy2(qi);
-  const int n = i * ny + j;
-  double bv0 = value2(0, mode, pp, xb, yb, nxb, nyb, tmid);
-  double bv1 = value2(1, mode, pp, xb, yb, nxb, nyb, tmid);
-  if (kind == kNeumann && p.use_dynamic_traction != 0) {
-    bv0 = p.traction_x[ell];
-    bv1 = p.traction_y[ell];
-  }
-  double Fg[4] = {U[2 * N + n], U[3 * N + n], U[4 * N + n], U[5 * N + n]};
-  const int iu = i - cx2(qo), ju = j - cy2(qo);
-  const bool up_ok = iu >= 0 && iu < nx && ju >= 0 && ju < ny && p.active[iu * ny + ju] != 0;
-  const int nu = iu * ny + ju;
-  const bool lsq_ok = p.lsq_valid[ell] != 0;
-  if (recon == 0 || recon == 2 || recon == 13) {
-    if (up_ok) {
-      for (int k = 0; k < 4; ++k) {
-        const double* Uk = U + (size_t)(2 + k) * N;
-        Fg[k] = Uk[n] + eta * (Uk[n] - Uk[nu]);
-      }
-    }
-    if (recon == 2 && lsq_ok)
-      for (int k = 0; k < 4; ++k) Fg[k] = lsq_eval(p, p.lsq_wb, U + (size_t)(2 + k) * N, ell);
-  } else {
-    for (int k = 0; k < 4; ++k)
-      Fg[k] = interp_link(U + (size_t)(2 + k) * N, p.active, i, j, qo, eta, nx, ny);
-  }
-  if ((recon == 11 || recon == 12) && lsq_ok)
-    for (int k = 0; k < 4; ++k) Fg[k] = lsq_eval(p, p.lsq_wb, U + (size_t)(2 + k) * N, ell);
-  if ((recon == 9 || recon == 11) && lsq_ok) {
-    const double tanx = -nyb, tany = nxb;
-    double dut0 = 0.0, dut1 = 0.0, wt_abs = 0.0;
-    if (kind == kNeumann) {
-      const int* li = p.lsq_i + (size_t)ell * kMaxLsq2;
-      const int* lj = p.lsq_j + (size_t)ell * kMaxLsq2;
-      const double* wt = p.lsq_wt + (size_t)ell * kMaxLsq2;
-      for (int mm = 0; mm < kMaxLsq2; ++mm) {
-        int ii = li[mm], jj = lj[mm];
-        if (ii >= 0 && jj >= 0) {
-          double ww = wt[mm];
-          dut0 += ww * u[ii * ny + jj];
-          dut1 += ww * u[N + ii * ny + jj];
-          wt_abs += fabs(ww);
-        }
-      }
-    } else {
-      if (mode == 6) {
-        double at = tmid;
-        if (pp[6] > 0.0 && at > pp[6]) at = pp[6];
-        dut0 = at * (pp[0] * tanx + pp[1] * tany);
-        dut1 = at * (pp[3] * tanx + pp[4] * tany);
-      }
-      wt_abs = 1.0;
-    }
-    if (wt_abs > 0.0) {
-      double hn0 = Fg[0] * nxb + Fg[1] * nyb;
-      double hn1 = Fg[2] * nxb + Fg[3] * nyb;
-      double gt0 = tanx + dut0, gt1 = tany + dut1;
-      Fg[0] = hn0 * nxb + gt0 * tanx;
-      Fg[1] = hn0 * nyb + gt0 * tany;
-      Fg[2] = hn1 * nxb + gt1 * tanx;
-      Fg[3] = hn1 * nyb + gt1 * tany;
-    }
-  }
-  double Fb[4] = {Fg[0], Fg[1], Fg[2], Fg[3]};
-  if (kind == kNeumann) solve_normal_image2(Fg, nxb, nyb, bv0, bv1, m, p.normal_solver, Fb);
-  const P2 Pb = piola2(Fb[0], Fb[1], Fb[2], Fb[3], m);
+}  // namespace
 
-  const bool use_char = (recon == 11 || recon == 12) && kind == kNeumann && lsq_ok;
-  double cv[6] = {U[n], U[N + n], Fb[0], Fb[1], Fb[2], Fb[3]};
-  if (kind == kDirichlet) {
-    cv[0] = bv0;
-    cv[1] = bv1;
-  }
-  double cw[6] = {0, 0, 0, 0, 0, 0};
-  const double dt = p.dt, cc = p.c, om = p.omega;
-  if (use_char) {
-    double ux[6], uy[6];
-    for (int a = 0; a < 6; ++a) {
-      ux[a] = lsq_eval(p, p.lsq_wx, U + (size_t)a * N, ell);
-      uy[a] = lsq_eval(p, p.lsq_wy, U + (size_t)a * N, ell);
-    }
-    const double sx = -eta * dt * cc * (double)cx2(qo);
-    const double sy = -eta * dt * cc * (double)cy2(qo);
-    double dv[6];
-    for (int a = 0; a < 6; ++a) dv[a] = sx * ux[a] + sy * uy[a];
-    double sc = 1.0;
-    for (int g = 0; g < 10; ++g) {
-      double t11 = cv[2] + sc * dv[2], t12 = cv[3] + sc * dv[3];
-      double t21 = cv[4] + sc * dv[4], t22 = cv[5] + sc * dv[5];
-      if (t11 * t22 - t12 * t21 > 10.0 * m.jf) break;
-      sc = 0.5 * sc;
-    }
-    for (int a = 0; a < 6; ++a) cv[a] = cv[a] + sc * dv[a];
-    double Ax[6], Ay[6], Bx[6], By[6];
-    flux2_jvp(cv, ux, m, Ax, Bx);  // A_x U_x (Bx unused)
-    flux2_jvp(cv, uy, m, By, Ay);  // A_y U_y (By unused)
-    for (int a = 0; a < 6; ++a) {
-      double b = source_comp(a, p.source_mode, p.source, cv);
-      cw[a] = b - Ax[a] - Ay[a] + cc * (dxin * ux[a] + dyin * uy[a]);
-    }
-  }
-  double eqx[6], eqy[6];
-  P2 Pc{0, 0, 0, 0};
-  bool char_ok = false;
-  if (use_char && cv[2] * cv[5] - cv[3] * cv[4] > m.jf) {
-    char_ok = true;
-    flux2_jvp(cv, cw, m, eqx, eqy);
-    Pc = piola2(cv[2], cv[3], cv[4], cv[5], m);
-  }
-  const double k2c = 2.0 / cc;
-  for (int a = 0; a < 6; ++a) {
-    double D = 1.0, S = 0.0;
-    if (kind == kDirichlet) {
-      switch (a) {
-        case 0: D = -1.0; S = 0.5 * bv0; break;
-        case 1: D = -1.0; S = 0.5 * bv1; break;
-        case 2: S = -dxin * bv0 / cc; break;
-        case 3: S = -dyin * bv0 / cc; break;
-        case 4: S = -dxin * bv1 / cc; break;
-        default: S = -dyin * bv1 / cc; break;
-      }
-    } else {
-      switch (a) {
-        case 0: S = -(dxin * Pb.a + dyin * Pb.b) / cc; break;
-        case 1: S = -(dxin * Pb.c + dyin * Pb.d) / cc; break;
-        case 2: D = -1.0; S = 0.5 * Fb[0]; break;
-        case 3: D = -1.0; S = 0.5 * Fb[1]; break;
-        case 4: D = -1.0; S = 0.5 * Fb[2]; break;
-        default: D = -1.0; S = 0.5 * Fb[3]; break;
-      }
-    }
-    double val;
-    if (char_ok) {
-      // characteristic overwrite, two_d/curved_boundary_warp.py:3034-3097
-      double jv = 0.25 * (cw[a] + k2c * (dxin * eqx[a] + dyin * eqy[a]));
-      double ge = feq2(qi, a, cv, Pc, k2c);
-      double sa = source_comp(a, p.source_mode, p.source, cv);
-      val = ge - dt / om * jv + dt * (1.0 / om - 0.5) * 0.25 * sa;
-    } else {
-      double fo = fpost[(size_t)(qo * 6 + a) * N + n];
-      double fi = fpost[(size_t)(qi * 6 + a) * N + n];
-      if (eta >= 0.5) {
-        double al = 1.0 / (2.0 * eta);
-        val = al * (D * fo + S) + (1.0 - al) * fi;
-      } else {
-        double upv = fo;
-        if (up_ok) upv = fpost[(size_t)(qo * 6 + a) * N + nu];
-        val = D * (2.0 * eta * fo + (1.0 - 2.0 * eta) * upv) + S;
-      }
-    }
-    fout[(size_t)(qi * 6 + a) * N + n] = val;
-  }
-}
+#include "cvlbm2d_fused.cuh"
 
-__global__ void __launch_bounds__(128) k_links2(Ctx2 c, const double* __restrict__ fpost,
-                                                double* __restrict__ fout,
-                                                const double* __restrict__ U,
-                                                const double* __restrict__ u, const double* clock,
-                                                double t_host, double offset) {
-  int ell = blockIdx.x * blockDim.x + threadIdx.x;
-  if (ell >= c.p.n_links) return;
-  link2(c, ell, fpost, fout, U, u, time_of(clock, t_host, offset));
-}
+namespace {
 
 // ---------------------------------------------------------------------------
 // Field refresh, two_d/curved_boundary_warp.py:3127-3210.
@@ -618,7 +430,7 @@ __global__ void __launch_bounds__(256) k_stress2(Ctx2 c, const double* __restric
   sg[3 * (size_t)N + n] = (P.c * F21 + P.d * F22) / Js;
 }
 
-__global__ void k_tick(double* clock, double dt) { clock[0] = clock[0] + dt; }
+__global__ void k_tick(const double* clock, double* next, double dt) { next[0] = clock[0] + dt; }
 
 __global__ void k_zero_flag(int* flag) { *flag = 0; }
 
@@ -655,9 +467,18 @@ Ctx2 make_ctx(const cvlbm2d_problem* p) {
 
 void launch_links(const Ctx2& c, const double* src, double* dst, const double* U,
                   const double* u, const double* clock, double t, double offset,
-                  cudaStream_t s) {
+                  cudaStream_t s, int fused = 0, const double* scratch = nullptr,
+                  const int32_t* partner = nullptr, double* clock_next = nullptr) {
   if (c.p.n_links <= 0) return;
-  k_links2<<<blocks(c.p.n_links, 128), 128, 0, s>>>(c, src, dst, U, u, clock, t, offset); cv::count_launches(1);
+  const int per = 128 / kLG;
+  k_links2g<<<blocks(c.p.n_links, per), 128, 0, s>>>(c, src, dst, U, u, clock, t, offset, fused,
+                                                      scratch, partner, clock_next);
+  cv::count_launches(1);
+}
+
+bool fused_ok(const cvlbm2d_problem* p, const cvlbm2d_fields* f) {
+  return p->tiles && p->need_fields && p->link_partner && f->link_scratch && p->lsq_node &&
+         p->disp_sweeps <= 1;
 }
 
 }  // namespace
@@ -672,24 +493,57 @@ extern "C" int cvlbm2d_run(const cvlbm2d_problem* p, cvlbm2d_fields* f, double t
   Ctx2 c = make_ctx(p);
   const int N = c.N;
   const unsigned nb = blocks(N, 256);
-  const double* clock = graph_mode ? f->clock : nullptr;
   k_zero_flag<<<1, 1, 0, s>>>(f->invalid); cv::count_launches(1);
   double t = time0;
+  const bool fused = fused_ok(p, f);
+  if (fused)
+    cudaFuncSetAttribute(k_fused2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFusedSmem2);
   for (int k = 0; k < nsteps; ++k) {
     const long long step = step0 + k;
-    int tk = timer_begin(s);
-    k_collide2<<<nb, 256, 0, s>>>(c, f->f0, f->fpost, f->U, f->u, f->u_star, f->invalid); cv::count_launches(1);
-    timer_end(tk, s);
-    if (due(p->disp_interval, step)) {
-      for (int sw = 0; sw < p->disp_sweeps; ++sw) {
-        k_sweep2<<<nb, 256, 0, s>>>(c, f->U, f->u, f->u_next, f->u_star, clock, t); cv::count_launches(1);
-        k_commit2<<<blocks(2LL * N, 256), 256, 0, s>>>(2 * N, f->u_next, f->u); cv::count_launches(1);
+    const int sweep = due(p->disp_interval, step), repair = due(p->rep_interval, step);
+    // graph mode: step k reads the device time from clock[k&1] and the link
+    // kernel writes clock[(k+1)&1] (no separate tick launch)
+    const double* clock = graph_mode ? f->clock + (k & 1) : nullptr;
+    double* clock_next = graph_mode ? f->clock + ((k + 1) & 1) : nullptr;
+    if (fused) {
+      Fused2 fz{p->tiles, p->n_tiles, p->tiles_j, p->need_fields, p->link_partner,
+                f->link_scratch, k == nsteps - 1};
+      int tk = timer_begin(s);
+      if (p->n_tiles > 0) {
+        k_fused2<<<p->n_tiles, kTX * kTY, kFusedSmem2, s>>>(c, fz, f->f0, f->f1, f->U, f->u,
+                                                            f->u_star, f->invalid, clock, t,
+                                                            sweep, repair);
+        cv::count_launches(1);
       }
+      timer_end(tk, s);
+      launch_links(c, f->f1, f->f1, f->U, f->u, clock, t, 0.5 * p->dt, s, 1, f->link_scratch,
+                   p->link_partner, clock_next);
+    } else {
+      int tk = timer_begin(s);
+      k_collide2<<<nb, 256, 0, s>>>(c, f->f0, f->fpost, f->U, f->u, f->u_star, f->invalid);
+      cv::count_launches(1);
+      timer_end(tk, s);
+      if (sweep) {
+        for (int sw = 0; sw < p->disp_sweeps; ++sw) {
+          k_sweep2<<<nb, 256, 0, s>>>(c, f->U, f->u, f->u_next, f->u_star, clock, t);
+          cv::count_launches(1);
+          k_commit2<<<blocks(2LL * N, 256), 256, 0, s>>>(2 * N, f->u_next, f->u);
+          cv::count_launches(1);
+        }
+      }
+      if (repair) {
+        k_repair2<<<nb, 256, 0, s>>>(c, f->fpost, f->U, f->u);
+        cv::count_launches(1);
+      }
+      k_stream2<<<nb, 256, 0, s>>>(c, f->fpost, f->f1);
+      cv::count_launches(1);
+      launch_links(c, f->fpost, f->f1, f->U, f->u, clock, t, 0.5 * p->dt, s, 0, nullptr, nullptr,
+                   clock_next);
     }
-    if (due(p->rep_interval, step)) k_repair2<<<nb, 256, 0, s>>>(c, f->fpost, f->U, f->u); cv::count_launches(1);
-    k_stream2<<<nb, 256, 0, s>>>(c, f->fpost, f->f1); cv::count_launches(1);
-    launch_links(c, f->fpost, f->f1, f->U, f->u, clock, t, 0.5 * p->dt, s);
-    if (graph_mode) k_tick<<<1, 1, 0, s>>>(f->clock, p->dt); cv::count_launches(1);
+    if (graph_mode && p->n_links <= 0) {
+      k_tick<<<1, 1, 0, s>>>(f->clock + (k & 1), f->clock + ((k + 1) & 1), p->dt);
+      cv::count_launches(1);
+    }
     double* tmp = f->f0;
     f->f0 = f->f1;
     f->f1 = tmp;

@@ -1,0 +1,603 @@
+// D2Q4x6 step, fused form: one tiled node kernel plus one cooperative link
+// kernel per time step.  Included by cvlbm2d.cu (shares Ctx2 and helpers).
+//
+// Node kernel (k_fused2): a 32x16 tile of nodes per 512-thread block.
+//   A  every node of the tile plus a 3-node halo: moments and collide-time
+//      displacement u from f0, u* into shared memory (halo moments are
+//      recomputed from f0 through L2 instead of being exchanged);
+//   B  displacement sweep with cut-point anchors on tile+2;
+//   C  owner nodes: F repair (needs swept u at +-2), BGK collision, repair
+//      delta, push-streaming of f_post to active neighbours.  A population
+//      whose neighbour is not active leaves through a cut link: it is stored
+//      per link (link_scratch) for the link kernel.
+// Per active node and step the node kernel reads f0 and u* once and writes
+// f1 and u* once (416 bytes), plus the fields the link stencils read.
+//
+// Link kernel (k_links2g): 16 lanes cooperate on one cut link: component-wise
+// stencil gathers in parallel, Newton on one lane, flux tangents split over
+// two lanes, one population row per lane.  With `fused` set the link reads
+// the populations it needs from link_scratch and f1 (post-stream) instead of
+// fpost.
+#pragma once
+
+namespace {
+
+constexpr int kTX = 32, kTY = 16, kH = 3;
+constexpr int kRX = kTX + 2 * kH, kRY = kTY + 2 * kH, kRN = kRX * kRY;  // 38 x 22
+constexpr int kSX = kTX + 4, kSY = kTY + 4, kSN = kSX * kSY;            // sweep region
+
+struct Fused2 {
+  const int32_t* tiles;        // [n_tiles] tile ids with at least one active node
+  int32_t n_tiles, tiles_j;    // tiles along j
+  const uint8_t* need;         // [N] node fields read by some link stencil
+  const int32_t* partner;      // [n_links] link at the same node in direction q_in, or -1
+  double* scratch;             // [6*n_links] f_post leaving through each link
+  int32_t store_all;           // write U and u for every active node
+};
+
+// Moments of node n (reference order: for q: for a) with the collision's
+// source / damping half step (two_d/curved_boundary_warp.py:1735-1756).
+__device__ __forceinline__ void moments2(const cvlbm2d_problem& p, const double* __restrict__ f0,
+                                         int N, int n, double* S) {
+#pragma unroll
+  for (int a = 0; a < 6; ++a) S[a] = 0.0;
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int a = 0; a < 6; ++a) S[a] += f0[(size_t)(q * 6 + a) * N + n];
+  const double hdt = 0.5 * p.dt;
+  if (p.source_mode == kSrcConstant) {
+#pragma unroll
+    for (int a = 0; a < 6; ++a) S[a] += hdt * p.source[a];
+  } else if (p.source_mode == kSrcDamping) {
+    double den = 1.0 + hdt * p.source[0];
+    S[0] = S[0] / den;
+    S[1] = S[1] / den;
+  }
+}
+
+constexpr size_t kFusedSmem2 =
+    sizeof(double) * (4 * kRN + 2 * kRN + 2 * kSN) + sizeof(int) * kRN;
+
+__global__ void __launch_bounds__(512, 1)
+    k_fused2(Ctx2 c, Fused2 fz, const double* __restrict__ f0, double* __restrict__ f1,
+             double* __restrict__ Ug, double* __restrict__ ug, double* __restrict__ ustar,
+             int* __restrict__ invalid, const double* clock, double t_host, int do_sweep,
+             int do_repair) {
+  extern __shared__ double smem2[];
+  double(*sF)[kRN] = reinterpret_cast<double(*)[kRN]>(smem2);            // collide-time F
+  double(*sU)[kRN] = reinterpret_cast<double(*)[kRN]>(smem2 + 4 * kRN);  // collide-time u
+  double(*sN)[kSN] = reinterpret_cast<double(*)[kSN]>(smem2 + 6 * kRN);  // swept u, tile+2
+  int* sA = reinterpret_cast<int*>(smem2 + 6 * kRN + 2 * kSN);           // active flags
+
+  const cvlbm2d_problem& p = c.p;
+  const int N = c.N, nx = p.nx, ny = p.ny;
+  const int tile = fz.tiles[blockIdx.x];
+  const int i0 = (tile / fz.tiles_j) * kTY, j0 = (tile % fz.tiles_j) * kTX;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int i = i0 + ty, j = j0 + tx;
+  const bool own = i < nx && j < ny;
+  const int n = i * ny + j;
+  const bool own_act = own && p.active[n] != 0;
+  const int r_own = (ty + kH) * kRX + tx + kH;
+  const double hdt = 0.5 * p.dt;
+
+  // -- A: region moments -----------------------------------------------------
+  double S[6];
+  double ucol0 = 0.0, ucol1 = 0.0;
+  if (own_act) {
+    moments2(p, f0, N, n, S);
+    ucol0 = ustar[n] + 0.5 * p.dt * S[0];
+    ucol1 = ustar[N + n] + 0.5 * p.dt * S[1];
+  }
+  for (int r = threadIdx.x; r < kRN; r += blockDim.x) {
+    const int ri = r / kRX, rj = r - ri * kRX;
+    const bool interior = ri >= kH && ri < kH + kTY && rj >= kH && rj < kH + kTX;
+    if (interior) continue;
+    const int gi = i0 - kH + ri, gj = j0 - kH + rj;
+    const bool inb = gi >= 0 && gi < nx && gj >= 0 && gj < ny;
+    const int m = gi * ny + gj;
+    const int act = inb ? p.active[m] : 0;
+    sA[r] = act;
+    if (act) {
+      double Sh[6];
+      moments2(p, f0, N, m, Sh);
+      sF[0][r] = Sh[2];
+      sF[1][r] = Sh[3];
+      sF[2][r] = Sh[4];
+      sF[3][r] = Sh[5];
+      sU[0][r] = ustar[m] + 0.5 * p.dt * Sh[0];
+      sU[1][r] = ustar[N + m] + 0.5 * p.dt * Sh[1];
+    } else {
+      sF[0][r] = sF[1][r] = sF[2][r] = sF[3][r] = 0.0;
+      sU[0][r] = sU[1][r] = 0.0;
+    }
+  }
+  sA[r_own] = own_act ? 1 : 0;
+  if (own_act) {
+    sF[0][r_own] = S[2];
+    sF[1][r_own] = S[3];
+    sF[2][r_own] = S[4];
+    sF[3][r_own] = S[5];
+    sU[0][r_own] = ucol0;
+    sU[1][r_own] = ucol1;
+  } else {
+    sF[0][r_own] = sF[1][r_own] = sF[2][r_own] = sF[3][r_own] = 0.0;
+    sU[0][r_own] = sU[1][r_own] = 0.0;
+  }
+  __syncthreads();
+
+  // -- B: displacement sweep on tile+2 (two_d/curved_boundary_warp.py:3275-3518)
+  const double time_mid = time_of(clock, t_host, 0.5 * p.dt);
+  for (int s = threadIdx.x; s < kSN; s += blockDim.x) {
+    const int si = s / kSX, sj = s - si * kSX;
+    const int r = (si + 1) * kRX + sj + 1;
+    if (!sA[r]) {
+      sN[0][s] = 0.0;
+      sN[1][s] = 0.0;
+      continue;
+    }
+    if (!do_sweep) {
+      sN[0][s] = sU[0][r];
+      sN[1][s] = sU[1][r];
+      continue;
+    }
+    const int gi = i0 - 2 + si, gj = j0 - 2 + sj;
+    const int m = gi * ny + gj;
+    double diag = 0.0, rx = 0.0, ry = 0.0;
+    const int k0 = p.node_link_start[m], k1 = p.node_link_start[m + 1];
+    for (int k = k0; k < k1; ++k) {
+      const int ell = p.node_link_list[k];
+      const int bid = p.link_bid[ell];
+      if (p.disp_bid >= 0) {
+        if (bid != p.disp_bid) continue;
+      } else if (p.bc_kind[bid] != kDirichlet) {
+        continue;
+      }
+      const double* pp = p.bc_params + bid * 8;
+      const int mode = p.bc_mode[bid];
+      const double xb = p.link_xb[ell], yb = p.link_yb[ell];
+      const double nxb = p.link_nx[ell], nyb = p.link_ny[ell];
+      double ub0 = 0.0, ub1 = 0.0;
+      if (mode == 1) {
+        ub0 = time_mid * value2(0, mode, pp, xb, yb, nxb, nyb, 0.0);
+        ub1 = time_mid * value2(1, mode, pp, xb, yb, nxb, nyb, 0.0);
+      } else if (mode == 6) {
+        double at = time_mid;
+        if (pp[6] > 0.0 && at > pp[6]) at = pp[6];
+        ub0 = at * value2(0, mode, pp, xb, yb, nxb, nyb, 0.0);
+        ub1 = at * value2(1, mode, pp, xb, yb, nxb, nyb, 0.0);
+      }
+      const double dbx = xb - ((double)gi + 0.5) * p.dx;
+      const double dby = yb - ((double)gj + 0.5) * p.dy;
+      const double tx_ = ub0 - ((sF[0][r] - 1.0) * dbx + sF[1][r] * dby);
+      const double ty_ = ub1 - (sF[2][r] * dbx + (sF[3][r] - 1.0) * dby);
+      const double w2 = p.weight * p.weight;
+      diag = diag + w2;
+      rx = rx + w2 * tx_;
+      ry = ry + w2 * ty_;
+    }
+    const double hx = 0.5 * p.dx, hy = 0.5 * p.dy;
+    if (sA[r + kRX]) {  // +x (i+1)
+      const int o = r + kRX;
+      rx += sU[0][o] - hx * ((sF[0][r] - 1.0) + (sF[0][o] - 1.0));
+      ry += sU[1][o] - hx * (sF[2][r] + sF[2][o]);
+      diag += 1.0;
+    }
+    if (sA[r - kRX]) {  // -x
+      const int o = r - kRX;
+      rx += sU[0][o] + hx * ((sF[0][o] - 1.0) + (sF[0][r] - 1.0));
+      ry += sU[1][o] + hx * (sF[2][o] + sF[2][r]);
+      diag += 1.0;
+    }
+    if (sA[r + 1]) {  // +y
+      const int o = r + 1;
+      rx += sU[0][o] - hy * (sF[1][r] + sF[1][o]);
+      ry += sU[1][o] - hy * ((sF[3][r] - 1.0) + (sF[3][o] - 1.0));
+      diag += 1.0;
+    }
+    if (sA[r - 1]) {  // -y
+      const int o = r - 1;
+      rx += sU[0][o] + hy * (sF[1][o] + sF[1][r]);
+      ry += sU[1][o] + hy * ((sF[3][o] - 1.0) + (sF[3][r] - 1.0));
+      diag += 1.0;
+    }
+    double u0 = sU[0][r], u1 = sU[1][r];
+    if (diag > 0.0) {
+      u0 = u0 + p.relax * (rx / diag - u0);
+      u1 = u1 + p.relax * (ry / diag - u1);
+    }
+    sN[0][s] = u0;
+    sN[1][s] = u1;
+  }
+  __syncthreads();
+  if (!own_act) return;
+
+  // -- C: repair, collision, streaming (owner) -------------------------------
+  const int s_own = (ty + 2) * kSX + tx + 2;
+  const double un0 = sN[0][s_own], un1 = sN[1][s_own];
+  const Mat& m = c.m;
+  double Fn[4] = {S[2], S[3], S[4], S[5]};
+  bool repaired = false;
+  if (do_repair) {
+    bool ok = true;
+    if (p.interior_only) {
+      ok = i > 0 && i + 1 < nx && j > 0 && j + 1 < ny && sA[r_own - kRX] && sA[r_own + kRX] &&
+           sA[r_own - 1] && sA[r_own + 1];
+    }
+    if (ok) {
+      // one-sided / centred derivatives of the swept displacement
+      // (two_d/curved_boundary_warp.py:3213-3272) on the shared tile+2 window
+      double g[2][2];
+#pragma unroll
+      for (int ax = 0; ax < 2; ++ax) {
+        const int rs = ax == 0 ? kRX : 1, ss = ax == 0 ? kSX : 1;
+        const int ii = ax == 0 ? i : j, nn = ax == 0 ? nx : ny;
+        const double h = ax == 0 ? p.dx : p.dy;
+        const bool am = ii > 0 && sA[r_own - rs], ap = ii + 1 < nn && sA[r_own + rs];
+#pragma unroll
+        for (int comp = 0; comp < 2; ++comp) {
+          const double* w = sN[comp];
+          double d;
+          if (am && ap) {
+            d = (w[s_own + ss] - w[s_own - ss]) / (2.0 * h);
+          } else if (ap) {
+            if (ii + 2 < nn && sA[r_own + 2 * rs])
+              d = (-3.0 * w[s_own] + 4.0 * w[s_own + ss] - w[s_own + 2 * ss]) / (2.0 * h);
+            else
+              d = (w[s_own + ss] - w[s_own]) / h;
+          } else if (am) {
+            if (ii > 1 && sA[r_own - 2 * rs])
+              d = (3.0 * w[s_own] - 4.0 * w[s_own - ss] + w[s_own - 2 * ss]) / (2.0 * h);
+            else
+              d = (w[s_own] - w[s_own - ss]) / h;
+          } else {
+            d = 0.0;
+          }
+          g[comp][ax] = d;
+        }
+      }
+      const double t11 = 1.0 + g[0][0], t12 = g[0][1], t21 = g[1][0], t22 = 1.0 + g[1][1];
+      double alpha = fmax(0.0, fmin(1.0, p.blend));
+      for (int it = 0; it < 10; ++it) {
+        Fn[0] = S[2] + alpha * (t11 - S[2]);
+        Fn[1] = S[3] + alpha * (t12 - S[3]);
+        Fn[2] = S[4] + alpha * (t21 - S[4]);
+        Fn[3] = S[5] + alpha * (t22 - S[5]);
+        if (Fn[0] * Fn[3] - Fn[1] * Fn[2] > m.jf) break;
+        alpha = 0.5 * alpha;
+      }
+      repaired = true;
+    }
+  }
+  const double J = S[2] * S[5] - S[3] * S[4];
+  if (J <= m.jf) *invalid = 1;
+  const P2 Po = piola2(S[2], S[3], S[4], S[5], m);
+  const double k2c = 2.0 / p.c, om = p.omega, sw = p.dt * (2.0 - om) * 0.125;
+  double d11 = 0.0, d12 = 0.0, d21 = 0.0, d22 = 0.0;
+  if (repaired) {
+    const P2 Pn = piola2(Fn[0], Fn[1], Fn[2], Fn[3], m);
+    d11 = Pn.a - Po.a;
+    d12 = Pn.b - Po.b;
+    d21 = Pn.c - Po.c;
+    d22 = Pn.d - Po.d;
+  }
+  const double ff = 0.5 / p.c, qt = 0.25;
+  // collision, repair delta and push-streaming, one population at a time
+  // (f0 of the owner is re-read from L1: the tile loaded it in phase A)
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int cq = cx2(q), cy = cy2(q);
+    const double cxd = (double)cq, cyd = (double)cy;
+    const bool to_node = sA[r_own + cq * kRX + cy] != 0;
+    const int d = n + cq * ny + cy;
+    int ell_out = -1;
+    if (!to_node) {
+      for (int k = p.node_link_start[n]; k < p.node_link_start[n + 1]; ++k) {
+        const int e = p.node_link_list[k];
+        if (p.link_q[e] == q) ell_out = e;
+      }
+    }
+#pragma unroll
+    for (int a = 0; a < 6; ++a) {
+      const double old = f0[(size_t)(q * 6 + a) * N + n];
+      const double fe = feq2(q, a, S, Po, k2c);
+      double v = old + om * (fe - old) + sw * source_comp(a, p.source_mode, p.source, S);
+      if (repaired) {
+        switch (a) {
+          case 0: v = v - ff * (cxd * d11 + cyd * d12); break;
+          case 1: v = v - ff * (cxd * d21 + cyd * d22); break;
+          default: v = v + qt * (Fn[a - 2] - S[a]); break;
+        }
+      }
+      if (to_node)
+        f1[(size_t)(q * 6 + a) * N + d] = v;
+      else if (ell_out >= 0)
+        fz.scratch[(size_t)ell_out * 6 + a] = v;
+    }
+  }
+  const double dt = p.dt;
+  ustar[n] = (ucol0 + 0.5 * dt * S[0]) + (un0 - ucol0);
+  ustar[N + n] = (ucol1 + 0.5 * dt * S[1]) + (un1 - ucol1);
+  if (fz.store_all || fz.need[n]) {
+    Ug[n] = S[0];
+    Ug[(size_t)N + n] = S[1];
+    Ug[2 * (size_t)N + n] = Fn[0];
+    Ug[3 * (size_t)N + n] = Fn[1];
+    Ug[4 * (size_t)N + n] = Fn[2];
+    Ug[5 * (size_t)N + n] = Fn[3];
+    ug[n] = un0;
+    ug[N + n] = un1;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Cooperative cut-link kernel: 16 lanes per link, 8 links per 128-thread block.
+// Lanes 0-5 gather d/dx of component `lane`, lanes 6-11 d/dy, lanes 12-15 the
+// F predictor; lane 0 runs the Newton solve; lanes 0/1 the two flux tangents;
+// lanes 0-5 write one population row each.  Links are visited in `order`
+// (traction links first) so a warp's links take the same branches.
+// ---------------------------------------------------------------------------
+constexpr int kLG = 16;
+
+struct LinkShared2 {
+  double Fg[4], ux[6], uy[6], dut[2], wt_abs;
+  double Fb[4], cv[6], cw[6], Ax[6], Ay[6], eqx[6], eqy[6], Pb[4], Pc[4];
+};
+
+// sum_m w[m] * Uc[node[m]] over the 24 stencil slots in slot order (as
+// _lsq_U_at_boundary, two_d/curved_boundary_warp.py:1213-1221), with all
+// loads issued before the sequential sum.
+__device__ __forceinline__ double lsq_sum(const int* __restrict__ node, const double* __restrict__ w,
+                                          const double* __restrict__ Uc) {
+  int nd[kMaxLsq2];
+  double wv[kMaxLsq2], uv[kMaxLsq2];
+#pragma unroll
+  for (int m = 0; m < kMaxLsq2; ++m) {
+    nd[m] = node[m];
+    wv[m] = w[m];
+  }
+#pragma unroll
+  for (int m = 0; m < kMaxLsq2; ++m) uv[m] = nd[m] >= 0 ? Uc[nd[m]] : 0.0;
+  double out = 0.0;
+#pragma unroll
+  for (int m = 0; m < kMaxLsq2; ++m)
+    if (nd[m] >= 0) out += wv[m] * uv[m];
+  return out;
+}
+
+__global__ void __launch_bounds__(128)
+    k_links2g(Ctx2 c, const double* __restrict__ fpost, double* __restrict__ fout,
+              const double* __restrict__ U, const double* __restrict__ u, const double* clock,
+              double t_host, double offset, int fused, const double* __restrict__ scratch,
+              const int32_t* __restrict__ partner, double* clock_next) {
+  __shared__ LinkShared2 sh[128 / kLG];
+  const cvlbm2d_problem& p = c.p;
+  const Mat& m = c.m;
+  const int lane = threadIdx.x & (kLG - 1);
+  const int grp = threadIdx.x / kLG;
+  const int slot = blockIdx.x * (128 / kLG) + grp;
+  const bool live = slot < p.n_links;
+  const int ell = live ? (p.link_order ? p.link_order[slot] : slot) : 0;
+  LinkShared2& S = sh[grp];
+  const int N = c.N, nx = p.nx, ny = p.ny, recon = p.recon;
+  const double tmid = time_of(clock, t_host, offset);
+  if (clock_next && blockIdx.x == 0 && threadIdx.x == 0) *clock_next = clock[0] + p.dt;
+
+  int i = 0, j = 0, qo = 0, qi = 2, kind = kDirichlet, mode = 0, n = 0, nu = 0;
+  double eta = 0.5, xb = 0, yb = 0, nxb = 1, nyb = 0, bv0 = 0, bv1 = 0;
+  bool up_ok = false, lsq_ok = false;
+  const double* pp = p.bc_params;
+  if (live) {
+    i = p.link_i[ell];
+    j = p.link_j[ell];
+    qo = p.link_q[ell];
+    int bid = p.link_bid[ell];
+    if (bid < 0 || bid >= kMaxIds2) bid = 0;
+    kind = p.bc_kind[bid];
+    mode = p.bc_mode[bid];
+    pp = p.bc_params + bid * 8;
+    qi = qo + 2;
+    if (qi >= 4) qi -= 4;
+    eta = p.link_eta[ell];
+    xb = p.link_xb[ell];
+    yb = p.link_yb[ell];
+    nxb = p.link_nx[ell];
+    nyb = p.link_ny[ell];
+    n = i * ny + j;
+    bv0 = value2(0, mode, pp, xb, yb, nxb, nyb, tmid);
+    bv1 = value2(1, mode, pp, xb, yb, nxb, nyb, tmid);
+    if (kind == kNeumann && p.use_dynamic_traction != 0) {
+      bv0 = p.traction_x[ell];
+      bv1 = p.traction_y[ell];
+    }
+    const int iu = i - cx2(qo), ju = j - cy2(qo);
+    up_ok = iu >= 0 && iu < nx && ju >= 0 && ju < ny && p.active[iu * ny + ju] != 0;
+    nu = up_ok ? iu * ny + ju : n;
+    lsq_ok = p.lsq_valid[ell] != 0;
+  }
+  const bool use_char = live && (recon == 11 || recon == 12) && kind == kNeumann && lsq_ok;
+  const bool compat = live && (recon == 9 || recon == 11) && lsq_ok;
+  const int* lnode = p.lsq_node + (size_t)ell * kMaxLsq2;
+
+  // -- gathers ----------------------------------------------------------------
+  if (live) {
+    if (lane < 12) {
+      const int a = lane < 6 ? lane : lane - 6;
+      if (use_char) {
+        const double* w = (lane < 6 ? p.lsq_wx : p.lsq_wy) + (size_t)ell * kMaxLsq2;
+        const double g = lsq_sum(lnode, w, U + (size_t)a * N);
+        if (lane < 6)
+          S.ux[a] = g;
+        else
+          S.uy[a] = g;
+      } else if (compat && kind == kNeumann && lane < 2) {
+        const double* wt = p.lsq_wt + (size_t)ell * kMaxLsq2;
+        double d = 0.0, wa = 0.0;
+        for (int mm = 0; mm < kMaxLsq2; ++mm) {
+          const int nd = lnode[mm];
+          if (nd >= 0) {
+            d += wt[mm] * u[(size_t)lane * N + nd];
+            wa += fabs(wt[mm]);
+          }
+        }
+        S.dut[lane] = d;
+        if (lane == 0) S.wt_abs = wa;
+      }
+    } else {
+      const int k = lane - 12;
+      const double* Uk = U + (size_t)(2 + k) * N;
+      double fg;
+      if (recon == 0 || recon == 2 || recon == 13) {
+        fg = up_ok ? Uk[n] + eta * (Uk[n] - Uk[nu]) : Uk[n];
+        if (recon == 2 && lsq_ok) fg = lsq_sum(lnode, p.lsq_wb + (size_t)ell * kMaxLsq2, Uk);
+      } else {
+        fg = interp_link(Uk, p.active, i, j, qo, eta, nx, ny);
+      }
+      if ((recon == 11 || recon == 12) && lsq_ok)
+        fg = lsq_sum(lnode, p.lsq_wb + (size_t)ell * kMaxLsq2, Uk);
+      S.Fg[k] = fg;
+    }
+  }
+  __syncwarp();
+
+  // -- predictor finalisation, Newton, characteristic state (lane 0) ---------
+  const double dt = p.dt, cc = p.c, om = p.omega;
+  const double dxin = (double)cx2(qi), dyin = (double)cy2(qi);
+  if (live && lane == 0) {
+    double Fg[4] = {S.Fg[0], S.Fg[1], S.Fg[2], S.Fg[3]};
+    if (compat) {
+      const double tanx = -nyb, tany = nxb;
+      double dut0 = 0.0, dut1 = 0.0, wt_abs = 0.0;
+      if (kind == kNeumann) {
+        dut0 = S.dut[0];
+        dut1 = S.dut[1];
+        wt_abs = S.wt_abs;
+      } else {
+        if (mode == 6) {
+          double at = tmid;
+          if (pp[6] > 0.0 && at > pp[6]) at = pp[6];
+          dut0 = at * (pp[0] * tanx + pp[1] * tany);
+          dut1 = at * (pp[3] * tanx + pp[4] * tany);
+        }
+        wt_abs = 1.0;
+      }
+      if (wt_abs > 0.0) {
+        const double hn0 = Fg[0] * nxb + Fg[1] * nyb, hn1 = Fg[2] * nxb + Fg[3] * nyb;
+        const double gt0 = tanx + dut0, gt1 = tany + dut1;
+        Fg[0] = hn0 * nxb + gt0 * tanx;
+        Fg[1] = hn0 * nyb + gt0 * tany;
+        Fg[2] = hn1 * nxb + gt1 * tanx;
+        Fg[3] = hn1 * nyb + gt1 * tany;
+      }
+    }
+    double Fb[4] = {Fg[0], Fg[1], Fg[2], Fg[3]};
+    if (kind == kNeumann) solve_normal_image2(Fg, nxb, nyb, bv0, bv1, m, p.normal_solver, Fb);
+    const P2 Pb = piola2(Fb[0], Fb[1], Fb[2], Fb[3], m);
+    S.Pb[0] = Pb.a;
+    S.Pb[1] = Pb.b;
+    S.Pb[2] = Pb.c;
+    S.Pb[3] = Pb.d;
+    for (int k = 0; k < 4; ++k) S.Fb[k] = Fb[k];
+    double cv[6] = {U[n], U[(size_t)N + n], Fb[0], Fb[1], Fb[2], Fb[3]};
+    if (kind == kDirichlet) {
+      cv[0] = bv0;
+      cv[1] = bv1;
+    }
+    if (use_char) {
+      const double sx = -eta * dt * cc * (double)cx2(qo);
+      const double sy = -eta * dt * cc * (double)cy2(qo);
+      double dv[6];
+      for (int a = 0; a < 6; ++a) dv[a] = sx * S.ux[a] + sy * S.uy[a];
+      double sc = 1.0;
+      for (int g = 0; g < 10; ++g) {
+        const double t11 = cv[2] + sc * dv[2], t12 = cv[3] + sc * dv[3];
+        const double t21 = cv[4] + sc * dv[4], t22 = cv[5] + sc * dv[5];
+        if (t11 * t22 - t12 * t21 > 10.0 * m.jf) break;
+        sc = 0.5 * sc;
+      }
+      for (int a = 0; a < 6; ++a) cv[a] = cv[a] + sc * dv[a];
+    }
+    for (int a = 0; a < 6; ++a) S.cv[a] = cv[a];
+  }
+  __syncwarp();
+
+  // -- flux tangents of the characteristic closure --------------------------
+  if (use_char && lane < 2) {
+    double tmp[6];
+    if (lane == 0)
+      flux2_jvp(S.cv, S.ux, m, S.Ax, tmp);  // A_x U_x
+    else
+      flux2_jvp(S.cv, S.uy, m, tmp, S.Ay);  // A_y U_y
+  }
+  __syncwarp();
+  if (use_char && lane < 6) {
+    const int a = lane;
+    const double b = source_comp(a, p.source_mode, p.source, S.cv);
+    S.cw[a] = b - S.Ax[a] - S.Ay[a] + cc * (dxin * S.ux[a] + dyin * S.uy[a]);
+  }
+  __syncwarp();
+  const bool char_ok = use_char && S.cv[2] * S.cv[5] - S.cv[3] * S.cv[4] > m.jf;
+  if (char_ok && lane < 2) {
+    if (lane == 0) {
+      flux2_jvp(S.cv, S.cw, m, S.eqx, S.eqy);
+    } else {
+      const P2 Pc = piola2(S.cv[2], S.cv[3], S.cv[4], S.cv[5], m);
+      S.Pc[0] = Pc.a;
+      S.Pc[1] = Pc.b;
+      S.Pc[2] = Pc.c;
+      S.Pc[3] = Pc.d;
+    }
+  }
+  __syncwarp();
+
+  // -- one population row per lane -----------------------------------------
+  if (live && lane < 6) {
+    const int a = lane;
+    double D = 1.0, Sv = 0.0;
+    if (kind == kDirichlet) {
+      switch (a) {
+        case 0: D = -1.0; Sv = 0.5 * bv0; break;
+        case 1: D = -1.0; Sv = 0.5 * bv1; break;
+        case 2: Sv = -dxin * bv0 / cc; break;
+        case 3: Sv = -dyin * bv0 / cc; break;
+        case 4: Sv = -dxin * bv1 / cc; break;
+        default: Sv = -dyin * bv1 / cc; break;
+      }
+    } else {
+      switch (a) {
+        case 0: Sv = -(dxin * S.Pb[0] + dyin * S.Pb[1]) / cc; break;
+        case 1: Sv = -(dxin * S.Pb[2] + dyin * S.Pb[3]) / cc; break;
+        default: D = -1.0; Sv = 0.5 * S.Fb[a - 2]; break;
+      }
+    }
+    double val;
+    if (char_ok) {
+      const P2 Pc{S.Pc[0], S.Pc[1], S.Pc[2], S.Pc[3]};
+      const double jv = 0.25 * (S.cw[a] + (2.0 / cc) * (dxin * S.eqx[a] + dyin * S.eqy[a]));
+      const double ge = feq2(qi, a, S.cv, Pc, 2.0 / cc);
+      const double sa = source_comp(a, p.source_mode, p.source, S.cv);
+      val = ge - dt / om * jv + dt * (1.0 / om - 0.5) * 0.25 * sa;
+    } else {
+      double fo, fi, upv;
+      if (fused) {
+        fo = scratch[(size_t)ell * 6 + a];
+        fi = up_ok ? fpost[(size_t)(qi * 6 + a) * N + nu] : scratch[(size_t)partner[ell] * 6 + a];
+        upv = up_ok ? fpost[(size_t)(qo * 6 + a) * N + n] : fo;
+      } else {
+        fo = fpost[(size_t)(qo * 6 + a) * N + n];
+        fi = fpost[(size_t)(qi * 6 + a) * N + n];
+        upv = up_ok ? fpost[(size_t)(qo * 6 + a) * N + nu] : fo;
+      }
+      if (eta >= 0.5) {
+        const double al = 1.0 / (2.0 * eta);
+        val = al * (D * fo + Sv) + (1.0 - al) * fi;
+      } else {
+        val = D * (2.0 * eta * fo + (1.0 - 2.0 * eta) * upv) + Sv;
+      }
+    }
+    fout[(size_t)(qi * 6 + a) * N + n] = val;
+  }
+}
+
+}  // namespace

@@ -46,13 +46,15 @@ class Problem2D(C.Structure):
         ("node_link_start", pI), ("node_link_list", pI),
         ("bc_kind", pI), ("bc_mode", pI), ("bc_params", pI),
         ("traction_x", pI), ("traction_y", pI),
+        ("tiles", pI), ("n_tiles", i32), ("tiles_j", i32), ("need_fields", pI),
+        ("link_partner", pI), ("lsq_node", pI), ("link_order", pI),
     ]
 
 
 class Fields2D(C.Structure):
     _fields_ = [(name, pI) for name in
                 ("f0", "f1", "fpost", "U", "u", "u_next", "u_star", "P", "sigma", "invalid",
-                 "clock")]
+                 "clock", "link_scratch")]
 
 
 class Problem3D(C.Structure):

@@ -215,6 +215,49 @@ class CurvedBoundarySpec:
         return kind, mode, np.ascontiguousarray(params)
 
 
+TILE_I, TILE_J = 8, 32
+
+
+def _fused_tables(geometry, lsq_i, lsq_j, lsq_valid):
+    """Tables of the fused step: active tiles, link-stencil nodes, link partners.
+
+    * tiles: ids (ti * tiles_j + tj) of the 8x32 node tiles that hold at least
+      one active node;
+    * need: nodes whose post-step U and u some cut link reads (the cut node,
+      two upstream nodes along the link, and the probe/LSQ stencil);
+    * partner: for link (x, q_out), the link (x, q_in) at the same node, whose
+      stored outgoing population is this link's f_post[q_in](x) when the
+      upstream neighbour is not active; -1 if that neighbour is active.
+    """
+    nx, ny = geometry.nx, geometry.ny
+    act = geometry.active.astype(bool)
+    ti, tj = -(-nx // TILE_I), -(-ny // TILE_J)
+    pad = np.zeros((ti * TILE_I, tj * TILE_J), dtype=bool)
+    pad[:nx, :ny] = act
+    occupied = pad.reshape(ti, TILE_I, tj, TILE_J).any(axis=(1, 3))
+    tiles = np.flatnonzero(occupied.reshape(-1)).astype(np.int32)
+    need = np.zeros((nx, ny), dtype=np.uint8)
+    li, lj, lq = geometry.link_i, geometry.link_j, geometry.link_q
+    cx, cy = _CX[lq], _CY[lq]
+    for k in range(3):
+        ii, jj = li - k * cx, lj - k * cy
+        ok = (ii >= 0) & (ii < nx) & (jj >= 0) & (jj < ny)
+        need[ii[ok], jj[ok]] = 1
+    if lsq_i is not None and len(lsq_i):
+        sel = (lsq_i >= 0) & (lsq_j >= 0)
+        need[lsq_i[sel], lsq_j[sel]] = 1
+    key = {(int(a), int(b), int(q)): e for e, (a, b, q) in enumerate(zip(li, lj, lq))}
+    partner = np.full(li.size, -1, dtype=np.int32)
+    for e, (a, b, q) in enumerate(zip(li, lj, lq)):
+        qi = (int(q) + 2) % 4
+        ui, uj = int(a) - int(_CX[q]), int(b) - int(_CY[q])
+        if not (0 <= ui < nx and 0 <= uj < ny and act[ui, uj]):
+            partner[e] = key.get((int(a), int(b), qi), -1)
+            if partner[e] < 0:
+                return None  # link tables without the opposite link: no fused step
+    return tiles, tj, np.ascontiguousarray(need.reshape(-1)), partner
+
+
 def _node_link_csr(link_node: np.ndarray, n_nodes: int):
     """CSR of link ids per node, ascending link id within a node."""
     order = np.argsort(link_node, kind="stable").astype(np.int32)
@@ -394,6 +437,20 @@ class WarpCurvedBoundaryLBM2D:
         t["lsq_valid"] = dev_i(lsq_valid)
         t["node_link_start"], t["node_link_list"] = dev_i(start), dev_i(order)
         t["bc_kind"], t["bc_mode"], t["bc_params"] = dev_i(kind), dev_i(mode), dev_f(params)
+        fused = _fused_tables(geometry, np.asarray(lsq_i), np.asarray(lsq_j), lsq_valid)
+        self._n_tiles, self._tiles_j = 0, 0
+        if fused is not None:
+            tiles, tiles_j, need, partner = fused
+            t["tiles"] = dev_i(tiles)
+            t["need_fields"] = torch.as_tensor(need, device=dev)
+            t["link_partner"] = dev_i(partner)
+            self._n_tiles, self._tiles_j = int(tiles.size), int(tiles_j)
+        li_np, lj_np = np.asarray(lsq_i), np.asarray(lsq_j)
+        t["lsq_node"] = dev_i(np.where((li_np >= 0) & (lj_np >= 0), li_np * self.ny + lj_np, -1))
+        # traction (Neumann) links first, then by node: a warp's links share branches
+        link_kind = kind[np.clip(geometry.link_boundary_id, 0, MAX_BOUNDARY_IDS - 1)]
+        t["link_order"] = dev_i(np.lexsort((np.arange(nl), link_kind != BC_NEUMANN)))
+        self.link_scratch = torch.zeros(max(6 * nl, 1), dtype=f64, device=dev)
         self.link_traction_x = torch.zeros(nl, dtype=f64, device=dev)
         self.link_traction_y = torch.zeros(nl, dtype=f64, device=dev)
         self.use_dynamic_link_traction = False
@@ -410,7 +467,7 @@ class WarpCurvedBoundaryLBM2D:
         self.P = torch.zeros((4,) + shp, dtype=f64, device=dev)
         self.sigma = torch.zeros_like(self.P)
         self.invalid = torch.zeros(1, dtype=i32, device=dev)
-        self._clock = torch.zeros(1, dtype=f64, device=dev)
+        self._clock = torch.zeros(2, dtype=f64, device=dev)
         self._stress_current = True
         self._graphs: dict = {}
         self._problem = self._make_problem()
@@ -442,16 +499,23 @@ class WarpCurvedBoundaryLBM2D:
         p.blend = self.local_compatibility_blend
         for name, tensor in t.items():
             setattr(p, name, _native.ptr(tensor))
+        p.n_tiles, p.tiles_j = self._n_tiles, self._tiles_j
         p.traction_x = _native.ptr(self.link_traction_x)
         p.traction_y = _native.ptr(self.link_traction_y)
         return p
+
+    def _set_fused(self, enabled: bool) -> None:
+        """Select the fused node kernel (default) or the per-phase kernels."""
+        t = self._tables.get("tiles")
+        self._problem.tiles = _native.ptr(t) if (enabled and t is not None) else None
 
     def _fields(self) -> _native.Fields2D:
         fl = _native.Fields2D()
         for name, tensor in (("f0", self.f0), ("f1", self.f1), ("fpost", self.fpost),
                              ("U", self.U), ("u", self.u), ("u_next", self.u_local_next),
                              ("u_star", self.u_star), ("P", self.P), ("sigma", self.sigma),
-                             ("invalid", self.invalid), ("clock", self._clock)):
+                             ("invalid", self.invalid), ("clock", self._clock),
+                             ("link_scratch", self.link_scratch)):
             setattr(fl, name, _native.ptr(tensor))
         return fl
 

@@ -94,6 +94,14 @@ typedef struct cvlbm2d_problem {
   const int32_t *bc_kind, *bc_mode;           /* [8] per boundary id */
   const double *bc_params;                    /* [8*8] */
   const double *traction_x, *traction_y;      /* [n_links] dynamic traction */
+  /* fused step (optional; all four set enables it when disp_sweeps <= 1) */
+  const int32_t *tiles;                       /* [n_tiles] ids of 8x32 tiles with active nodes */
+  int32_t n_tiles, tiles_j;                   /* tile count, tiles along j */
+  const uint8_t *need_fields;                 /* [nx*ny] node read by some link stencil */
+  const int32_t *link_partner;                /* [n_links] link at the same node in the
+                                                 incoming direction, or -1 */
+  const int32_t *lsq_node;                    /* [n_links*24] lsq_i*ny+lsq_j, -1 unused */
+  const int32_t *link_order;                  /* [n_links] processing order (optional) */
 } cvlbm2d_problem;
 
 /* Mutable state.  f0 is the current population field; a run swaps f0 and f1
@@ -105,7 +113,9 @@ typedef struct cvlbm2d_fields {
   double *u_star;           /* [2*N]  trapezoidal half-step displacement */
   double *P, *sigma;        /* [4*N]  first Piola and Cauchy stress */
   int32_t *invalid;         /* [1]    sticky flag, reset at the start of a run */
-  double *clock;            /* [1]    device time; used when graph_mode != 0 */
+  double *clock;            /* [2]    device time (ping-pong); graph_mode != 0 */
+  double *link_scratch;     /* [6*n_links] fused step: post-collision populations
+                               leaving through each cut link */
 } cvlbm2d_fields;
 
 /* Advance `nsteps` time steps starting at host time `time0` and step index

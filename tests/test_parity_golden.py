@@ -96,3 +96,51 @@ def test_3d_dirichlet_bfl_regression(golden_dir):
     np.testing.assert_allclose(s.active_populations(), ref["f25"], rtol=0, atol=1e-13)
     assert s.characteristic_stencil is None
     assert s.summary()["characteristic_cut_links"] == 0
+
+
+@pytest.mark.parametrize("name", ["g2_traction_localf", "g2_affine_compat", "g2_bfl_mixed_fd"])
+def test_2d_fused_step_equals_per_phase_kernels(golden_dir, name):
+    """The fused node kernel and the per-phase kernels give identical states."""
+    d, cfg = cases.load(golden_dir / f"{name}.npz")
+    out = []
+    for fused in (True, False):
+        s = cases.solver_2d(cfg)
+        s._set_fused(fused)
+        U0, disp0 = cases.initial_state_2d(cfg["init"], s.geometry)
+        s.initialize_from_numpy(U=U0, displacement=disp0, init_order=cfg["init"]["init_order"])
+        s.run(cfg["steps"])
+        out.append((s.numpy_field("f0"), s.numpy_field("u_star"), s.numpy_field("U"),
+                    s.numpy_field("u")))
+    for a, b in zip(*out):
+        np.testing.assert_array_equal(a, b)
+
+
+def test_2d_run_equals_repeated_step(golden_dir):
+    d, cfg = cases.load(golden_dir / "g2_traction_localf.npz")
+    s1 = cases.solver_2d(cfg)
+    s2 = cases.solver_2d(cfg)
+    for s in (s1, s2):
+        U0, disp0 = cases.initial_state_2d(cfg["init"], s.geometry)
+        s.initialize_from_numpy(U=U0, displacement=disp0, init_order=2)
+    s1.run(9)
+    for _ in range(9):
+        s2.step()
+    assert s1.time == s2.time and s1.steps == s2.steps
+    for name in ("f0", "u_star", "U", "u"):
+        np.testing.assert_array_equal(s1.numpy_field(name), s2.numpy_field(name))
+
+
+def test_graph_replay_equals_run(golden_dir):
+    d, cfg = cases.load(golden_dir / "g2_traction_localf.npz")
+    s1 = cases.solver_2d(cfg)
+    s2 = cases.solver_2d(cfg)
+    for s in (s1, s2):
+        U0, disp0 = cases.initial_state_2d(cfg["init"], s.geometry)
+        s.initialize_from_numpy(U=U0, displacement=disp0, init_order=2)
+    g = s1.capture_graph(4)
+    g.launch()
+    g.launch()
+    s2.run(8)
+    assert s1.time == s2.time
+    for name in ("f0", "u_star", "U", "u"):
+        np.testing.assert_array_equal(s1.numpy_field(name), s2.numpy_field(name))
