@@ -51,106 +51,36 @@ HBM_FALLBACK_GBS = 6650.0
 # ---------------------------------------------------------------------------
 # workloads
 # ---------------------------------------------------------------------------
-def annulus_config(n=512):
-    L = 1.1
-    dx = L / n
-    dt = dx / 10.0
-    ramp = 20000 * dt
-    return dict(
-        geometry=dict(nx=n, ny=n, length_x=L, length_y=L, center_x=0.55, center_y=0.55,
-                      inner_radius=0.25, outer_radius=0.5),
-        boundary=dict(kind="neumann", value_mode=105, params=(0.05, ramp),
-                      id_kinds={1: "neumann", 2: "dirichlet"}, id_value_modes={1: 105, 2: 0},
-                      id_params={1: (0.05, ramp), 2: ()}),
-        solver=dict(lattice_speed=10.0, collision_omega=1.8, boundary_reconstruction="local_f",
-                    source_mode="damping", damping_gamma=10.0, local_displacement_interval=1,
-                    local_displacement_sweeps=1, local_displacement_relax=0.85,
-                    local_displacement_boundary_weight=100.0, local_displacement_boundary_id=2,
-                    local_compatibility_interval=1, local_compatibility_blend=0.5,
-                    local_compatibility_interior_only=False),
-    )
-
-
-def shell_config(n=192):
-    L = 2.2
-    dt = (L / n) / 10.0
-    ramp = 10000 * dt
-    return dict(
-        n=n, L=L, ri=0.5, ro=1.0,
-        boundary=dict(kind="neumann", value_mode=208, params=(0.05, ramp),
-                      id_kinds={1: "neumann", 2: "dirichlet"}, id_value_modes={1: 208, 2: 0},
-                      id_params={1: (0.05, ramp), 2: ()}),
-        solver=dict(lattice_speed=10.0, collision_omega=1.8, boundary_reconstruction="local_f",
-                    source_mode="damping", damping_gamma=10.0, local_displacement_interval=1,
-                    local_displacement_sweeps=1, local_displacement_relax=0.85,
-                    local_displacement_boundary_weight=100.0, local_displacement_boundary_id=2,
-                    local_compatibility_interval=1, local_compatibility_blend=0.5),
-    )
-
-
 def build_annulus(device=None, n=512, oracle=False, threads=1):
-    from curved_lbm.two_d import curved_boundary_warp as c2
+    from curved_lbm import workloads
 
-    cfg = annulus_config(n)
-    geom = c2.CurvedBoundaryGeometry.annulus(**cfg["geometry"])
-    mat = c2.WarpHyperelasticMaterial(model="neo_hooke", lam=1.0, mu=1.0)
-    spec = c2.CurvedBoundarySpec(**cfg["boundary"])
-    U = np.zeros((6, n, n))
-    U[2] = U[5] = 1.0
+    geom, mat, spec, kw = workloads.annulus(n)
     if oracle:
         from oracle.oracle import Oracle2D
 
-        s = Oracle2D(geom, material=mat, boundary=spec, threads=threads, **cfg["solver"])
+        s = Oracle2D(geom, material=mat, boundary=spec, threads=threads, **kw)
     else:
-        s = c2.WarpCurvedBoundaryLBM2D(geom, material=mat, boundary=spec, device=device,
-                                       **cfg["solver"])
-    s.initialize_from_numpy(U=U, displacement=np.zeros((2, n, n)), init_order=2)
+        from curved_lbm.two_d import curved_boundary_warp as c2
+
+        s = c2.WarpCurvedBoundaryLBM2D(geom, material=mat, boundary=spec, device=device, **kw)
+    U, disp = workloads.annulus_initial_state(n)
+    s.initialize_from_numpy(U=U, displacement=disp, init_order=2)
     return s, geom.n_active
 
 
-def shell_geometry(n=192):
-    from curved_lbm.three_d import curved_boundary_warp3d as c3
-
-    cfg = shell_config(n)
-    L, ri, ro = cfg["L"], cfg["ri"], cfg["ro"]
-    c = 0.5 * L
-
-    def phiv(X, Y, Z):
-        R = np.sqrt((X - c) ** 2 + (Y - c) ** 2 + (Z - c) ** 2)
-        return np.maximum(R - ro, ri - R)
-
-    def normv(X, Y, Z):
-        X, Y, Z = np.broadcast_arrays(X, Y, Z)
-        dx, dy, dz = X - c, Y - c, Z - c
-        R = np.maximum(np.sqrt(dx * dx + dy * dy + dz * dz), 1e-30)
-        s = np.where(np.abs(R - ri) <= np.abs(R - ro), -1.0, 1.0)
-        return s * dx / R, s * dy / R, s * dz / R
-
-    def bid(x, y, z, *_):
-        r = math.sqrt((x - c) ** 2 + (y - c) ** 2 + (z - c) ** 2)
-        return 2 if abs(r - ri) <= abs(r - ro) else 1
-
-    return c3.CurvedBoundaryGeometry3D.from_level_set(
-        nx=n, ny=n, nz=n, length_x=L, length_y=L, length_z=L,
-        phi=lambda x, y, z: float(phiv(np.asarray(x), np.asarray(y), np.asarray(z))),
-        boundary_id=bid, phi_vectorized=phiv, normal_vectorized=normv, label="shell")
-
-
 def build_shell(device=None, n=192, oracle=False, threads=1):
-    from curved_lbm.three_d import curved_boundary_warp3d as c3
+    from curved_lbm import workloads
 
-    cfg = shell_config(n)
-    geom = shell_geometry(n)
-    mat = c3.WarpHyperelasticMaterial3D(model="neo_hooke", lam=1.0, mu=1.0)
-    spec = c3.CurvedBoundarySpec3D(**cfg["boundary"])
+    geom, mat, spec, kw = workloads.shell(n)
     if oracle:
         from oracle.oracle import Oracle3D
 
-        s = Oracle3D(geom, material=mat, boundary=spec, threads=threads, **cfg["solver"])
+        s = Oracle3D(geom, material=mat, boundary=spec, threads=threads, **kw)
         s.initialize_identity()
         return s, s.N
-    s = c3.WarpSparseCurvedBoundaryLBM3D(geom, material=mat, boundary=spec, device=device,
-                                         **cfg["solver"])
+    from curved_lbm.three_d import curved_boundary_warp3d as c3
+
+    s = c3.WarpSparseCurvedBoundaryLBM3D(geom, material=mat, boundary=spec, device=device, **kw)
     return s, s.n_active
 
 
@@ -295,6 +225,8 @@ def main():
     ap.add_argument("--inner", type=int, default=100, help="lattice steps per bench step")
     ap.add_argument("--ref-steps", type=int, default=4, help="oracle steps for the CPU legs")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tile-variant", type=int, default=-1,
+                    help="fused 2-D tile shape; -1 = autotune on the workload")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.inner % 2:
@@ -315,6 +247,12 @@ def main():
     dev = torch.device(f"cuda:{local}")
     torch.cuda.set_device(dev)
     solver, n_active = BUILDERS[args.workload](device=str(dev))
+    tuned = {}
+    if hasattr(solver, "autotune"):
+        if args.tile_variant >= 0:
+            solver._select_variant(args.tile_variant)
+        else:
+            tuned = solver.autotune()
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(256 * 1024 * 1024 // 8, dtype=torch.float64, device=dev)
 
@@ -424,7 +362,9 @@ def main():
         "config": {"workload": args.workload, "n_active": int(n_active),
                    "lbm_steps_per_bench_step": args.inner,
                    "l2": "flushed between bench steps (256 MB write)",
-                   "parallelism": f"replicas x{world}"},
+                   "parallelism": f"replicas x{world}",
+                   "tile_variant": getattr(solver, "tile_variant", None),
+                   "autotune_us_per_step": {str(k): round(v, 2) for k, v in tuned.items()}},
         "e2e": e2e, "roofline": roofline, "cpu_baseline": base,
         "clocks": clocks.summary(),
         "gpu_launches": int(launches_per_graph * args.steps),

@@ -476,9 +476,30 @@ void launch_links(const Ctx2& c, const double* src, double* dst, const double* U
   cv::count_launches(1);
 }
 
+using FusedFn2 = void (*)(Ctx2, Fused2, const double*, double*, double*, double*, const double*,
+                          double*, int*, const double*, double, int, int);
+struct FusedLaunch2 {
+  FusedFn2 fn;
+  int threads;
+  size_t smem;
+  int tile_i;
+};
+
+// Compiled tile variants: (tile rows, resident blocks per SM).  The tile list
+// in the problem must have been built for the variant's tile height.
+FusedLaunch2 fused_variant(int v) {
+  switch (v) {
+    case 1: return {k_fused2<8, 2>, kTX * 8, fused_smem2<8>(), 8};
+    case 2: return {k_fused2<8, 3>, kTX * 8, fused_smem2<8>(), 8};
+    case 3: return {k_fused2<16, 2>, kTX * 16, fused_smem2<16>(), 16};
+    case 4: return {k_fused2<4, 4>, kTX * 4, fused_smem2<4>(), 4};
+    default: return {k_fused2<16, 1>, kTX * 16, fused_smem2<16>(), 16};
+  }
+}
+
 bool fused_ok(const cvlbm2d_problem* p, const cvlbm2d_fields* f) {
   return p->tiles && p->need_fields && p->link_partner && f->link_scratch && p->lsq_node &&
-         p->disp_sweeps <= 1;
+         p->disp_sweeps <= 1 && fused_variant(p->tile_variant).tile_i == p->tile_i;
 }
 
 }  // namespace
@@ -496,8 +517,12 @@ extern "C" int cvlbm2d_run(const cvlbm2d_problem* p, cvlbm2d_fields* f, double t
   k_zero_flag<<<1, 1, 0, s>>>(f->invalid); cv::count_launches(1);
   double t = time0;
   const bool fused = fused_ok(p, f);
-  if (fused)
-    cudaFuncSetAttribute(k_fused2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFusedSmem2);
+  FusedLaunch2 fl = fused_variant(p->tile_variant);
+  if (fused) cudaFuncSetAttribute(fl.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fl.smem);
+  // the fused kernel reads u* in the halo of its tile, so it ping-pongs
+  // between u_star and u_next; an odd count ends with one copy back
+  double* us_cur = f->u_star;
+  double* us_nxt = f->u_next;
   for (int k = 0; k < nsteps; ++k) {
     const long long step = step0 + k;
     const int sweep = due(p->disp_interval, step), repair = due(p->rep_interval, step);
@@ -510,11 +535,13 @@ extern "C" int cvlbm2d_run(const cvlbm2d_problem* p, cvlbm2d_fields* f, double t
                 f->link_scratch, k == nsteps - 1};
       int tk = timer_begin(s);
       if (p->n_tiles > 0) {
-        k_fused2<<<p->n_tiles, kTX * kTY, kFusedSmem2, s>>>(c, fz, f->f0, f->f1, f->U, f->u,
-                                                            f->u_star, f->invalid, clock, t,
-                                                            sweep, repair);
+        fl.fn<<<p->n_tiles, fl.threads, fl.smem, s>>>(c, fz, f->f0, f->f1, f->U, f->u, us_cur,
+                                                      us_nxt, f->invalid, clock, t, sweep, repair);
         cv::count_launches(1);
       }
+      double* us = us_cur;
+      us_cur = us_nxt;
+      us_nxt = us;
       timer_end(tk, s);
       launch_links(c, f->f1, f->f1, f->U, f->u, clock, t, 0.5 * p->dt, s, 1, f->link_scratch,
                    p->link_partner, clock_next);
@@ -549,6 +576,8 @@ extern "C" int cvlbm2d_run(const cvlbm2d_problem* p, cvlbm2d_fields* f, double t
     f->f1 = tmp;
     t += p->dt;
   }
+  if (us_cur != f->u_star)
+    cudaMemcpyAsync(f->u_star, us_cur, sizeof(double) * 2 * (size_t)N, cudaMemcpyDeviceToDevice, s);
   return check_launch("cvlbm2d_run");
 }
 
@@ -580,6 +609,11 @@ extern "C" int cvlbm2d_refresh(const cvlbm2d_problem* p, cvlbm2d_fields* f, void
   k_refresh2<<<blocks(c.N, 256), 256, 0, s>>>(c, f->f0, f->U, f->u, f->u_star, f->P, f->sigma,
                                                f->invalid); cv::count_launches(1);
   return check_launch("cvlbm2d_refresh");
+}
+
+extern "C" int cvlbm2d_tile_variant(int32_t v) {
+  if (v < 0 || v > 4) return 0;
+  return fused_variant(v).tile_i;
 }
 
 extern "C" int cvlbm2d_stress(const cvlbm2d_problem* p, cvlbm2d_fields* f, void* stream) {

@@ -22,9 +22,9 @@
 
 namespace {
 
-constexpr int kTX = 32, kTY = 16, kH = 3;
-constexpr int kRX = kTX + 2 * kH, kRY = kTY + 2 * kH, kRN = kRX * kRY;  // 38 x 22
-constexpr int kSX = kTX + 4, kSY = kTY + 4, kSN = kSX * kSY;            // sweep region
+constexpr int kTX = 32, kH = 3;
+constexpr int kRX = kTX + 2 * kH;  // region row length (tile + halo 3)
+constexpr int kSX = kTX + 4;       // sweep-region row length (tile + 2)
 
 struct Fused2 {
   const int32_t* tiles;        // [n_tiles] tile ids with at least one active node
@@ -56,14 +56,24 @@ __device__ __forceinline__ void moments2(const cvlbm2d_problem& p, const double*
   }
 }
 
-constexpr size_t kFusedSmem2 =
-    sizeof(double) * (4 * kRN + 2 * kRN + 2 * kSN) + sizeof(int) * kRN;
+template <int TY>
+constexpr size_t fused_smem2() {
+  return sizeof(double) * (6 * kRX * (TY + 2 * kH) + 2 * kSX * (TY + 4)) +
+         sizeof(int) * kRX * (TY + 2 * kH);
+}
 
-__global__ void __launch_bounds__(512, 1)
+// Tile kTX x TY, one node per thread; MINB resident blocks per SM bounds the
+// registers per thread (tuned per problem, see curved_lbm autotune).
+template <int TY, int MINB>
+__global__ void __launch_bounds__(kTX * TY, MINB)
     k_fused2(Ctx2 c, Fused2 fz, const double* __restrict__ f0, double* __restrict__ f1,
-             double* __restrict__ Ug, double* __restrict__ ug, double* __restrict__ ustar,
+             double* __restrict__ Ug, double* __restrict__ ug,
+             const double* __restrict__ ustar, double* __restrict__ ustar_out,
              int* __restrict__ invalid, const double* clock, double t_host, int do_sweep,
              int do_repair) {
+  constexpr int kTY = TY;
+  constexpr int kRN = kRX * (TY + 2 * kH);
+  constexpr int kSN = kSX * (TY + 4);
   extern __shared__ double smem2[];
   double(*sF)[kRN] = reinterpret_cast<double(*)[kRN]>(smem2);            // collide-time F
   double(*sU)[kRN] = reinterpret_cast<double(*)[kRN]>(smem2 + 4 * kRN);  // collide-time u
@@ -317,8 +327,10 @@ __global__ void __launch_bounds__(512, 1)
     }
   }
   const double dt = p.dt;
-  ustar[n] = (ucol0 + 0.5 * dt * S[0]) + (un0 - ucol0);
-  ustar[N + n] = (ucol1 + 0.5 * dt * S[1]) + (un1 - ucol1);
+  // u* goes to the other buffer: neighbouring tiles read this node's old u*
+  // in their halo during the same launch
+  ustar_out[n] = (ucol0 + 0.5 * dt * S[0]) + (un0 - ucol0);
+  ustar_out[N + n] = (ucol1 + 0.5 * dt * S[1]) + (un1 - ucol1);
   if (fz.store_all || fz.need[n]) {
     Ug[n] = S[0];
     Ug[(size_t)N + n] = S[1];

@@ -48,6 +48,7 @@ class Problem2D(C.Structure):
         ("traction_x", pI), ("traction_y", pI),
         ("tiles", pI), ("n_tiles", i32), ("tiles_j", i32), ("need_fields", pI),
         ("link_partner", pI), ("lsq_node", pI), ("link_order", pI),
+        ("tile_variant", i32), ("tile_i", i32),
     ]
 
 
@@ -107,6 +108,7 @@ EXPORTED = (
     "cvlbm_timer_elapsed",
     "cvlbm_timer_attach",
     "cvlbm_launch_count",
+    "cvlbm2d_tile_variant",
 )
 
 
@@ -146,6 +148,7 @@ def load(require_cuda: bool = True):
         "cvlbm_timer_elapsed": (i32, [pI, C.POINTER(f64), C.POINTER(i32)]),
         "cvlbm_timer_attach": (i32, [pI]),
         "cvlbm_launch_count": (i64, []),
+        "cvlbm2d_tile_variant": (i32, [i32]),
         "cvlbm_last_error": (C.c_char_p, []),
     }
     for name, (res, args) in sig.items():

@@ -215,14 +215,25 @@ class CurvedBoundarySpec:
         return kind, mode, np.ascontiguousarray(params)
 
 
-TILE_I, TILE_J = 8, 32
+TILE_J = 32
+DEFAULT_TILE_VARIANT = 0
+
+
+def _tile_list(active: np.ndarray, tile_i: int):
+    """Ids (ti * tiles_j + tj) of the tile_i x 32 node tiles holding an active node."""
+    nx, ny = active.shape
+    ti, tj = -(-nx // tile_i), -(-ny // TILE_J)
+    pad = np.zeros((ti * tile_i, tj * TILE_J), dtype=bool)
+    pad[:nx, :ny] = active
+    occupied = pad.reshape(ti, tile_i, tj, TILE_J).any(axis=(1, 3))
+    return np.flatnonzero(occupied.reshape(-1)).astype(np.int32), tj
 
 
 def _fused_tables(geometry, lsq_i, lsq_j, lsq_valid):
-    """Tables of the fused step: active tiles, link-stencil nodes, link partners.
+    """Tables of the fused step: link-stencil nodes and link partners.
 
-    * tiles: ids (ti * tiles_j + tj) of the 8x32 node tiles that hold at least
-      one active node;
+    (The tile list depends on the fused-kernel variant; see `_tile_list`.)
+
     * need: nodes whose post-step U and u some cut link reads (the cut node,
       two upstream nodes along the link, and the probe/LSQ stencil);
     * partner: for link (x, q_out), the link (x, q_in) at the same node, whose
@@ -231,11 +242,6 @@ def _fused_tables(geometry, lsq_i, lsq_j, lsq_valid):
     """
     nx, ny = geometry.nx, geometry.ny
     act = geometry.active.astype(bool)
-    ti, tj = -(-nx // TILE_I), -(-ny // TILE_J)
-    pad = np.zeros((ti * TILE_I, tj * TILE_J), dtype=bool)
-    pad[:nx, :ny] = act
-    occupied = pad.reshape(ti, TILE_I, tj, TILE_J).any(axis=(1, 3))
-    tiles = np.flatnonzero(occupied.reshape(-1)).astype(np.int32)
     need = np.zeros((nx, ny), dtype=np.uint8)
     li, lj, lq = geometry.link_i, geometry.link_j, geometry.link_q
     cx, cy = _CX[lq], _CY[lq]
@@ -255,7 +261,7 @@ def _fused_tables(geometry, lsq_i, lsq_j, lsq_valid):
             partner[e] = key.get((int(a), int(b), qi), -1)
             if partner[e] < 0:
                 return None  # link tables without the opposite link: no fused step
-    return tiles, tj, np.ascontiguousarray(need.reshape(-1)), partner
+    return np.ascontiguousarray(need.reshape(-1)), partner
 
 
 def _node_link_csr(link_node: np.ndarray, n_nodes: int):
@@ -438,13 +444,13 @@ class WarpCurvedBoundaryLBM2D:
         t["node_link_start"], t["node_link_list"] = dev_i(start), dev_i(order)
         t["bc_kind"], t["bc_mode"], t["bc_params"] = dev_i(kind), dev_i(mode), dev_f(params)
         fused = _fused_tables(geometry, np.asarray(lsq_i), np.asarray(lsq_j), lsq_valid)
-        self._n_tiles, self._tiles_j = 0, 0
         if fused is not None:
-            tiles, tiles_j, need, partner = fused
-            t["tiles"] = dev_i(tiles)
+            need, partner = fused
             t["need_fields"] = torch.as_tensor(need, device=dev)
             t["link_partner"] = dev_i(partner)
-            self._n_tiles, self._tiles_j = int(tiles.size), int(tiles_j)
+        self._tile_lists: dict = {}
+        self._fused_possible = fused is not None
+        self.tile_variant = DEFAULT_TILE_VARIANT
         li_np, lj_np = np.asarray(lsq_i), np.asarray(lsq_j)
         t["lsq_node"] = dev_i(np.where((li_np >= 0) & (lj_np >= 0), li_np * self.ny + lj_np, -1))
         # traction (Neumann) links first, then by node: a warp's links share branches
@@ -471,9 +477,59 @@ class WarpCurvedBoundaryLBM2D:
         self._stress_current = True
         self._graphs: dict = {}
         self._problem = self._make_problem()
+        self._select_variant(self.tile_variant)
         self.initialize_identity(init_order=1)
 
     # -- native plumbing ---------------------------------------------------
+    def _select_variant(self, variant: int) -> None:
+        """Point the problem at the tile list of fused-kernel variant `variant`."""
+        import torch
+
+        tile_i = int(self._lib.cvlbm2d_tile_variant(int(variant)))
+        if tile_i <= 0:
+            raise ValueError(f"fused-kernel variant {variant} is not compiled")
+        if tile_i not in self._tile_lists:
+            tiles, tj = _tile_list(self.active_np.astype(bool), tile_i)
+            self._tile_lists[tile_i] = (torch.as_tensor(tiles, device=self._tdev), tj)
+        tiles, tj = self._tile_lists[tile_i]
+        self._tables["tiles"] = tiles
+        self.tile_variant = int(variant)
+        p = self._problem
+        p.tile_variant, p.tile_i = int(variant), tile_i
+        p.n_tiles, p.tiles_j = int(tiles.numel()), int(tj)
+        p.tiles = _native.ptr(tiles) if self._fused_possible else None
+
+    def autotune(self, steps: int = 40, variants=None) -> dict:
+        """Time every compiled fused-kernel variant on this problem; keep the fastest.
+
+        Runs on a copy of the state (populations, u*, time) that is restored
+        afterwards, so the solution is unchanged.  Returns {variant: us/step}.
+        """
+        import torch
+
+        if not self._fused_possible:
+            return {}
+        saved = (self.f0.clone(), self.f1.clone(), self.u_star.clone(), self.U.clone(),
+                 self.u.clone(), self.time, self.steps)
+        cand = [v for v in (variants if variants is not None else range(8))
+                if int(self._lib.cvlbm2d_tile_variant(int(v))) > 0]
+        times = {}
+        for v in cand:
+            self._select_variant(v)
+            self.run(4)
+            torch.cuda.synchronize(self._tdev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            self.run(steps)
+            e1.record()
+            e1.synchronize()
+            times[v] = e0.elapsed_time(e1) * 1e3 / steps
+            self.f0.copy_(saved[0]); self.f1.copy_(saved[1]); self.u_star.copy_(saved[2])
+            self.U.copy_(saved[3]); self.u.copy_(saved[4])
+            self.time, self.steps = saved[5], saved[6]
+        best = min(times, key=times.get)
+        self._select_variant(best)
+        return times
     def _make_problem(self) -> _native.Problem2D:
         t = self._tables
         m = self.material
@@ -499,7 +555,6 @@ class WarpCurvedBoundaryLBM2D:
         p.blend = self.local_compatibility_blend
         for name, tensor in t.items():
             setattr(p, name, _native.ptr(tensor))
-        p.n_tiles, p.tiles_j = self._n_tiles, self._tiles_j
         p.traction_x = _native.ptr(self.link_traction_x)
         p.traction_y = _native.ptr(self.link_traction_y)
         return p
@@ -507,7 +562,8 @@ class WarpCurvedBoundaryLBM2D:
     def _set_fused(self, enabled: bool) -> None:
         """Select the fused node kernel (default) or the per-phase kernels."""
         t = self._tables.get("tiles")
-        self._problem.tiles = _native.ptr(t) if (enabled and t is not None) else None
+        ok = enabled and t is not None and self._fused_possible
+        self._problem.tiles = _native.ptr(t) if ok else None
 
     def _fields(self) -> _native.Fields2D:
         fl = _native.Fields2D()

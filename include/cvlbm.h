@@ -95,14 +95,21 @@ typedef struct cvlbm2d_problem {
   const double *bc_params;                    /* [8*8] */
   const double *traction_x, *traction_y;      /* [n_links] dynamic traction */
   /* fused step (optional; all four set enables it when disp_sweeps <= 1) */
-  const int32_t *tiles;                       /* [n_tiles] ids of 8x32 tiles with active nodes */
+  const int32_t *tiles;                       /* [n_tiles] ids of tile_i x 32 tiles with active nodes */
   int32_t n_tiles, tiles_j;                   /* tile count, tiles along j */
   const uint8_t *need_fields;                 /* [nx*ny] node read by some link stencil */
   const int32_t *link_partner;                /* [n_links] link at the same node in the
                                                  incoming direction, or -1 */
   const int32_t *lsq_node;                    /* [n_links*24] lsq_i*ny+lsq_j, -1 unused */
   const int32_t *link_order;                  /* [n_links] processing order (optional) */
+  int32_t tile_variant;                       /* compiled fused-kernel variant, see
+                                                 cvlbm2d_tile_variant() */
+  int32_t tile_i;                             /* tile rows the tile list was built for */
 } cvlbm2d_problem;
+
+/* Tile rows (i extent, tiles are 32 nodes wide in j) of fused-kernel variant
+ * v, or 0 if v is not compiled.  Used by autotuners to enumerate variants. */
+int cvlbm2d_tile_variant(int32_t v);
 
 /* Mutable state.  f0 is the current population field; a run swaps f0 and f1
  * once per step and writes the swapped pointers back. */

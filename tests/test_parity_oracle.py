@@ -1,0 +1,134 @@
+"""CUDA time step against the CPU oracle on the benchmark workloads.
+
+The golden fixtures are small (tens of nodes across); these cases run the
+benchmark physics (traction annulus, spherical shell) on grids with many
+tiles in both directions and sizes that are not multiples of the tile, for
+1000 steps (2-D) and 200 steps (3-D), and compare with the oracle — the C
+restatement of the reference kernels, itself pinned to every fixture.
+Tolerance: relative 1e-12 of the field's largest magnitude, on populations,
+u*, U (velocity and F) and u.
+
+At the full benchmark size (512^2), where the oracle is too slow to replay
+1000 steps inside a test, size-independent properties are checked instead:
+every fused tile shape and the per-phase kernels give bitwise-identical
+states, and a CUDA-graph replay equals the plain run.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-12
+
+
+def close_rel(name, got, ref, rtol=RTOL):
+    got, ref = np.asarray(got), np.asarray(ref)
+    assert got.shape == ref.shape, (name, got.shape, ref.shape)
+    scale = float(np.max(np.abs(ref))) or 1.0
+    err = float(np.max(np.abs(got - ref)))
+    assert err <= rtol * scale, f"{name}: max abs err {err:.3e} > {rtol:g} x {scale:.3e}"
+
+
+_cache: dict = {}
+
+
+def _oracle_annulus(n, steps):
+    key = ("annulus", n, steps)
+    if key not in _cache:
+        from curved_lbm import workloads
+        from oracle.oracle import Oracle2D, available
+
+        if not available():
+            pytest.skip("oracle library not built")
+        geom, mat, spec, kw = workloads.annulus(n)
+        o = Oracle2D(geom, material=mat, boundary=spec, threads=8, **kw)
+        U, disp = workloads.annulus_initial_state(n)
+        o.initialize_from_numpy(U=U, displacement=disp, init_order=2)
+        o.run(steps)
+        _cache[key] = {k: np.array(getattr(o, k)) for k in ("f0", "u_star", "U", "u")}
+    return _cache[key]
+
+
+def _gpu_annulus(n, variant=None, fused=True):
+    from curved_lbm import workloads
+    from curved_lbm.two_d import curved_boundary_warp as c2
+
+    geom, mat, spec, kw = workloads.annulus(n)
+    s = c2.WarpCurvedBoundaryLBM2D(geom, material=mat, boundary=spec, **kw)
+    if variant is not None:
+        s._select_variant(variant)
+    s._set_fused(fused)
+    U, disp = workloads.annulus_initial_state(n)
+    s.initialize_from_numpy(U=U, displacement=disp, init_order=2)
+    return s
+
+
+@pytest.mark.parametrize("n", [100, 200])
+def test_annulus_1000_steps_match_oracle(n):
+    ref = _oracle_annulus(n, 1000)
+    s = _gpu_annulus(n)
+    s.run(1000)
+    for k in ("f0", "u_star", "U", "u"):
+        close_rel(k, s.numpy_field(k), ref[k])
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
+def test_annulus_tile_variants_match_oracle(variant):
+    ref = _oracle_annulus(200, 1000)
+    s = _gpu_annulus(200, variant=variant)
+    s.run(1000)
+    for k in ("f0", "u_star", "U", "u"):
+        close_rel(k, s.numpy_field(k), ref[k])
+
+
+def test_shell_200_steps_match_oracle():
+    from curved_lbm import workloads
+    from curved_lbm.three_d import curved_boundary_warp3d as c3
+    from oracle.oracle import Oracle3D, available
+
+    if not available():
+        pytest.skip("oracle library not built")
+    geom, mat, spec, kw = workloads.shell(40)
+    o = Oracle3D(geom, material=mat, boundary=spec, threads=8, **kw)
+    o.initialize_identity()
+    o.run(200)
+    s = c3.WarpSparseCurvedBoundaryLBM3D(geom, material=mat, boundary=spec, **kw)
+    s.initialize_identity()
+    s.run(200)
+    close_rel("f0", s.active_populations(), o.f0)
+    close_rel("u_star", s.active_ustar(), o.u_star)
+    s.refresh_current()
+    o.refresh()
+    close_rel("U", s.active_system_state(), o.U)
+    close_rel("u", s.active_displacement(), o.u)
+
+
+def test_annulus512_fused_variants_bitwise_equal_per_phase():
+    import torch
+
+    base = _gpu_annulus(512, fused=False)
+    base.run(30)
+    want = [base.numpy_field(k) for k in ("f0", "u_star", "U", "u")]
+    assert np.isfinite(want[0]).all()
+    for v in range(5):
+        s = _gpu_annulus(512, variant=v)
+        s.run(30)
+        for k, w in zip(("f0", "u_star", "U", "u"), want):
+            np.testing.assert_array_equal(s.numpy_field(k), w, err_msg=f"variant {v} {k}")
+        del s
+        torch.cuda.empty_cache()
+
+
+def test_annulus512_graph_equals_run():
+    a = _gpu_annulus(512)
+    b = _gpu_annulus(512)
+    g = a.capture_graph(10)
+    for _ in range(3):
+        g.launch()
+    b.run(30)
+    assert a.time == b.time and a.steps == b.steps
+    for k in ("f0", "u_star", "U", "u"):
+        np.testing.assert_array_equal(a.numpy_field(k), b.numpy_field(k))
