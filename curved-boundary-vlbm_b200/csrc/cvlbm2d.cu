@@ -16,6 +16,9 @@
 // order, the order in which the reference's serial atomics add them.
 #include <cuda_runtime.h>
 
+#include <mutex>
+#include <string>
+
 #include "cvlbm_common.cuh"
 #include "cvlbm_math.cuh"
 
@@ -632,4 +635,89 @@ extern "C" int cvlbm2d_graph_create(const cvlbm2d_problem* p, const cvlbm2d_fiel
   cvlbm2d_fields local = *f;
   return capture_graph(
       [&](cudaStream_t s) { return cvlbm2d_run(p, &local, 0.0, step0, nsteps, 1, s); }, out);
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free step: link scratch in a fixed array compiled into the library.
+//
+// The fused step parks the post-collision populations that leave through cut
+// links in a per-link scratch buffer (6 doubles per link) that cvlbm2d_run
+// takes from the caller.  Some hosts cannot hand one over: an application that
+// has carved all device memory into its own pool before this library is
+// loaded, or a fixed-rate driver loop that must not enter an allocator between
+// steps (cudaMalloc/cudaFree may synchronise the whole device).  For them the
+// scratch lives here instead, in a static device array sized for
+// CVLBM2D_STATIC_SCRATCH_MAX_LINKS cut links (6 * 16384 doubles = 768 KiB per
+// device).  Nothing is allocated on any call: the array's address is looked
+// up once per device (cudaGetSymbolAddress) and cached.
+//
+// Contents: no element has to start at zero.  Within every step the node
+// kernel writes the entry of each cut link before the link kernel reads it.
+// One array per device is shared by all callers: two calls in flight at the
+// same time on one device (different streams or threads) overwrite each
+// other's scratch and give wrong results; the caller serialises them.
+// ---------------------------------------------------------------------------
+namespace {
+
+static __device__ __align__(256) double g_static_link_scratch[6 * CVLBM2D_STATIC_SCRATCH_MAX_LINKS];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_static_mu;
+double* g_static_ptr[kMaxDevices] = {};
+
+// Address of g_static_link_scratch on the current device (set up on first use).
+int static_scratch(double** out) {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return fail(CVLBM_ERR_CUDA, (std::string("cudaGetDevice: ") + cudaGetErrorString(e)).c_str());
+  if (dev < 0 || dev >= kMaxDevices) return fail(CVLBM_ERR_UNSUPPORTED, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_static_mu);
+  if (!g_static_ptr[dev]) {
+    void* addr = nullptr;
+    e = cudaGetSymbolAddress(&addr, g_static_link_scratch);
+    if (e != cudaSuccess || !addr)
+      return fail(CVLBM_ERR_CUDA, (std::string("cudaGetSymbolAddress(static link scratch): ") +
+                                   cudaGetErrorString(e)).c_str());
+    g_static_ptr[dev] = static_cast<double*>(addr);
+  }
+  *out = g_static_ptr[dev];
+  return CVLBM_OK;
+}
+
+}  // namespace
+
+extern "C" int cvlbm2d_run_static_scratch(const cvlbm2d_problem* p, cvlbm2d_fields* f,
+                                          double time0, int64_t step0, int32_t nsteps,
+                                          void* stream) {
+  if (!p || !f) return fail(CVLBM_ERR_INVALID_ARG, "null problem or fields");
+  if (p->n_links > CVLBM2D_STATIC_SCRATCH_MAX_LINKS)
+    return fail(CVLBM_ERR_INVALID_ARG,
+                ("cvlbm2d_run_static_scratch: " + std::to_string(p->n_links) +
+                    " cut links exceed the static scratch of " +
+                    std::to_string(CVLBM2D_STATIC_SCRATCH_MAX_LINKS) +
+                    "; use cvlbm2d_run with a caller-owned link_scratch")
+                       .c_str());
+  if (f->f0) {  // the fields must live on the current device
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, f->f0) == cudaSuccess && attr.type == cudaMemoryTypeDevice) {
+      int dev = -1;
+      cudaGetDevice(&dev);
+      if (attr.device != dev)
+        return fail(CVLBM_ERR_INVALID_ARG,
+                    ("cvlbm2d_run_static_scratch: fields are on device " +
+                     std::to_string(attr.device) + " but device " + std::to_string(dev) +
+                     " is current")
+                        .c_str());
+    }
+  }
+  double* scratch = nullptr;
+  int rc = static_scratch(&scratch);
+  if (rc) return rc;
+  cvlbm2d_fields local = *f;
+  local.link_scratch = scratch;
+  rc = cvlbm2d_run(p, &local, time0, step0, nsteps, 0, stream);
+  // hand back the f0/f1 exchange cvlbm2d_run made, keep the caller's scratch field
+  f->f0 = local.f0;
+  f->f1 = local.f1;
+  return rc;
 }

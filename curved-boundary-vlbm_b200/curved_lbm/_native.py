@@ -109,6 +109,7 @@ EXPORTED = (
     "cvlbm_timer_attach",
     "cvlbm_launch_count",
     "cvlbm2d_tile_variant",
+    "cvlbm2d_run_static_scratch",
 )
 
 
@@ -149,6 +150,7 @@ def load(require_cuda: bool = True):
         "cvlbm_timer_attach": (i32, [pI]),
         "cvlbm_launch_count": (i64, []),
         "cvlbm2d_tile_variant": (i32, [i32]),
+        "cvlbm2d_run_static_scratch": (i32, [P2, F2, f64, i64, i32, pI]),
         "cvlbm_last_error": (C.c_char_p, []),
     }
     for name, (res, args) in sig.items():

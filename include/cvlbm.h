@@ -134,6 +134,20 @@ typedef struct cvlbm2d_fields {
 int cvlbm2d_run(const cvlbm2d_problem *p, cvlbm2d_fields *f, double time0, int64_t step0,
                 int32_t nsteps, int32_t graph_mode, void *stream);
 
+/* Same step as cvlbm2d_run (graph_mode 0) without any allocation and without
+ * a caller-owned link scratch: fields->link_scratch is ignored and the
+ * per-link scratch is a fixed array inside the library, one per device, for
+ * at most CVLBM2D_STATIC_SCRATCH_MAX_LINKS cut links (768 KiB).  Problems
+ * with more cut links are rejected with CVLBM_ERR_INVALID_ARG.  The fields
+ * must live on the current device.  The first call on a device looks up the
+ * array's address (cudaGetSymbolAddress); make that call before any stream
+ * capture begins.  Calls in flight at the same time on one device share the
+ * array and race; serialise them.  For hosts that cannot allocate device
+ * memory between steps.  No counterpart in the reference. */
+#define CVLBM2D_STATIC_SCRATCH_MAX_LINKS 16384
+int cvlbm2d_run_static_scratch(const cvlbm2d_problem *p, cvlbm2d_fields *f, double time0,
+                               int64_t step0, int32_t nsteps, void *stream);
+
 /* Cut-link reconstruction at time t, fpost -> f1, or in place on f0 through a
  * frozen copy in fpost.  Replaces apply_boundary_reconstruction
  * (two_d/curved_boundary_warp.py:4020-4035). */
