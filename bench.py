@@ -223,6 +223,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="annulus512", choices=sorted(BUILDERS))
     ap.add_argument("--inner", type=int, default=100, help="lattice steps per bench step")
+    ap.add_argument("--size", type=int, default=0,
+                    help="lattice nodes per axis (0 = the workload's own size; smaller sizes "
+                         "are for profiler captures, not bench lines)")
     ap.add_argument("--ref-steps", type=int, default=4, help="oracle steps for the CPU legs")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tile-variant", type=int, default=-1,
@@ -246,7 +249,8 @@ def main():
 
     dev = torch.device(f"cuda:{local}")
     torch.cuda.set_device(dev)
-    solver, n_active = BUILDERS[args.workload](device=str(dev))
+    size_kw = {"n": args.size} if args.size > 0 else {}
+    solver, n_active = BUILDERS[args.workload](device=str(dev), **size_kw)
     tuned = {}
     if hasattr(solver, "autotune"):
         if args.tile_variant >= 0:

@@ -511,6 +511,12 @@ __global__ void k_set_ustar3(int N, const double* __restrict__ disp, const doubl
     ustar[(size_t)d * N + n] = disp[(size_t)d * N + n] - 0.5 * dt * U[(size_t)d * N + n];
 }
 
+}  // namespace
+
+#include "cvlbm3d_fused.cuh"
+
+namespace {
+
 __global__ void k_tick3(double* clock, double dt) { clock[0] = clock[0] + dt; }
 __global__ void k_zero_flag3(int* flag) { *flag = 0; }
 
@@ -531,6 +537,19 @@ int check_problem(const cvlbm3d_problem* p, const cvlbm3d_fields* f) {
   if (p->has_char && (!p->char_idx || !p->char_w))
     return fail(CVLBM_ERR_INVALID_ARG, "characteristic stencil tables missing");
   return CVLBM_OK;
+}
+
+// The fused pipeline needs its link tables and scratch, and one sweep per
+// due step (several sweeps per step take the per-phase pipeline).
+bool fused_ok3(const cvlbm3d_problem* p, const cvlbm3d_fields* f) {
+  if (!p->need_slot || p->disp_sweeps > 1) return false;
+  if (p->n_links > 0) {
+    if (!p->link_partner || !f->link_scratch || !f->U_need || p->n_need <= 0 ||
+        !f->link_kind || !f->link_comp_kind || !f->link_bv || !f->link_Fb || !f->link_Pb)
+      return false;
+    if (p->has_char && (!f->char_state || !p->char_slot)) return false;
+  }
+  return true;
 }
 
 Ctx3 make_ctx(const cvlbm3d_problem* p) {
@@ -555,6 +574,53 @@ extern "C" int cvlbm3d_run(const cvlbm3d_problem* p, cvlbm3d_fields* f, double t
   const double* clock = graph_mode ? f->clock : nullptr;
   k_zero_flag3<<<1, 1, 0, s>>>(f->invalid); cv::count_launches(1);
   double t = time0;
+  if (fused_ok3(p, f)) {
+    Fused3 fz{p->need_slot, p->char_slot, p->link_partner, p->link_order, f->link_scratch,
+              f->U_need};
+    const int L = p->n_links;
+    for (int k = 0; k < nsteps; ++k) {
+      const long long step = step0 + k;
+      const int sweep = N > 0 && due(p->disp_interval, step);
+      const int repair = due(p->rep_interval, step);
+      int tk = timer_begin(s);
+      if (N > 0) {
+        k3_moments<<<blocks(N, 256), 256, 0, s>>>(c, f->f0, f->U, sweep ? f->u_next : f->u,
+                                                  f->u_star, f->invalid, sweep);
+        cv::count_launches(1);
+        if (sweep) {
+          k3_sweep<<<blocks(N, 256), 256, 0, s>>>(c, f->U, f->u_next, f->u, f->u_star, clock, t);
+          cv::count_launches(1);
+        }
+        k3_collide<<<blocks(N, kCN), kQ3 * kCN, 0, s>>>(c, fz, f->f0, f->f1, f->U, f->u, repair,
+                                                        k == nsteps - 1);
+        cv::count_launches(1);
+      }
+      timer_end(tk, s);
+      if (L > 0) {
+        if (p->has_char) {
+          k3_link_gather<<<blocks(L, 128 / kGatherLanes), 128, 0, s>>>(c, fz, f->char_state);
+          cv::count_launches(1);
+        }
+        k3_link_prepare<<<blocks(L, 128), 128, 0, s>>>(c, fz, f->u, *f, clock, t, 0.5 * p->dt);
+        cv::count_launches(1);
+        k3_link_rows<<<blocks((long long)L * kC3, 128), 128, 0, s>>>(c, fz, f->f1, *f);
+        cv::count_launches(1);
+        if (p->has_char) {
+          k3_link_char<<<blocks(L, 64), 64, 0, s>>>(c, fz, f->f1, *f);
+          cv::count_launches(1);
+        }
+      }
+      if (graph_mode) {
+        k_tick3<<<1, 1, 0, s>>>(f->clock, p->dt);
+        cv::count_launches(1);
+      }
+      double* tmp = f->f0;
+      f->f0 = f->f1;
+      f->f1 = tmp;
+      t += p->dt;
+    }
+    return check_launch("cvlbm3d_run");
+  }
   for (int k = 0; k < nsteps; ++k) {
     const long long step = step0 + k;
     int tk = timer_begin(s);

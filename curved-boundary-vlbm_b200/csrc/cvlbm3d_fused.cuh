@@ -1,0 +1,569 @@
+// D3Q6x12 step, fused form.  Included by cvlbm3d.cu (shares Ctx3 and the
+// per-link helpers).
+//
+// Node kernels (reference raster order of the active nodes):
+//   k3_moments   f0 -> U (all 12 components), collide-time u into `ucol`
+//                (u_next), invalid flag; when no sweep is due, u and u* too
+//   k3_sweep     u_swept -> u and the trapezoidal u* update, from U and ucol
+//                of the node and its six neighbours plus cut-point anchors
+//   k3_collide   f0 again (six warps per 32 nodes, one per direction):
+//                moments, F repair from the swept u (+-2 star stencil), BGK
+//                collision with damping/source, repair delta and push
+//                streaming to f1; a population whose neighbour is not active
+//                leaves through a cut link and is kept per link
+//                (link_scratch) for the link kernels; the post-step U of
+//                nodes that links read goes to U_need, one 96-byte row each
+// Per active node this reads f0 twice and writes f1 once (the f0 re-read of
+// k3_collide is what a single-pass 3-D fusion would save; its 3-deep halo
+// does not fit shared memory), plus U, u and u* (about 2.1 KB per node
+// against the algorithmic 1.2 KB).
+//
+// Link kernels (the four phases of apply_boundary_reconstruction,
+// three_d/curved_boundary_warp3d.py:4339-4399):
+//   k3_link_gather   16 lanes per link, one per component: value and
+//                    gradient of the characteristic stencil (:2675-2700)
+//   k3_link_prepare  one thread per link: boundary value, F predictor, Newton
+//                    normal solve, P(F_b) (:2887-3151)
+//   k3_link_rows     one thread per (link, row): BFL rows (:3154-3241) that
+//                    the characteristic closure does not overwrite
+//   k3_link_char     one thread per link: characteristic rows (:2812-2884)
+// In the fused step they read the outgoing populations from link_scratch and
+// the post-stream f1 instead of a stored post-collision field.
+#pragma once
+
+namespace {
+
+struct Fused3 {
+  const int32_t* need_slot;  // [N] row of Uneed of a node some link reads, or -1
+  const int32_t* char_slot;  // [64*n_links] characteristic samples as Uneed rows
+  const int32_t* partner;    // [n_links] link at the same node in direction q_in, or -1
+  const int32_t* order;      // [n_links] processing order of one-thread-per-link kernels
+  double* scratch;           // [12*n_links] post-collision population leaving through a link
+  double* Uneed;             // [n_need*12] post-step U, one 96-byte row per node
+};
+
+// Moments with the collision's damping/source half step
+// (three_d/curved_boundary_warp3d.py:2192-2260), summed over q in order.
+__device__ __forceinline__ void moments3(const cvlbm3d_problem& p, const double* __restrict__ f,
+                                         int N, int n, double* S) {
+#pragma unroll
+  for (int a = 0; a < kC3; ++a) {
+    double s = 0.0;
+#pragma unroll
+    for (int q = 0; q < kQ3; ++q) s += f[(size_t)(q * kC3 + a) * N + n];
+    S[a] = s;
+  }
+  const double hdt = 0.5 * p.dt;
+  if (p.source_mode == kSrcConstant) {
+#pragma unroll
+    for (int a = 0; a < kC3; ++a) S[a] += hdt * p.source[a];
+  } else if (p.source_mode == kSrcDamping) {
+    const double den = 1.0 + hdt * p.source[0];
+    S[0] = S[0] / den;
+    S[1] = S[1] / den;
+    S[2] = S[2] / den;
+  }
+}
+
+__global__ void __launch_bounds__(256) k3_moments(Ctx3 c, const double* __restrict__ f0,
+                                                  double* __restrict__ U,
+                                                  double* __restrict__ ucol,
+                                                  double* __restrict__ ustar,
+                                                  int* __restrict__ invalid, int sweep_due) {
+  const int N = c.N;
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const cvlbm3d_problem& p = c.p;
+  double S[kC3];
+  moments3(p, f0, N, n, S);
+#pragma unroll
+  for (int a = 0; a < kC3; ++a) U[(size_t)a * N + n] = S[a];
+  const double hdt = 0.5 * p.dt;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double uu = ustar[(size_t)d * N + n] + hdt * S[d];
+    ucol[(size_t)d * N + n] = uu;
+    // with a sweep due, k3_sweep writes u* = (uu + hdt v) + (u_swept - uu)
+    if (!sweep_due) ustar[(size_t)d * N + n] = uu + hdt * S[d];
+  }
+  if (det3(S[3], S[4], S[5], S[6], S[7], S[8], S[9], S[10], S[11]) <= c.m.jf) *invalid = 1;
+}
+
+// One Jacobi sweep (three_d/curved_boundary_warp3d.py:2402-2540); ucol holds
+// the collide-time u of every node, the swept u goes to `u`.
+__global__ void __launch_bounds__(256) k3_sweep(Ctx3 c, const double* __restrict__ U,
+                                                const double* __restrict__ ucol,
+                                                double* __restrict__ u,
+                                                double* __restrict__ ustar, const double* clock,
+                                                double t_host) {
+  const int N = c.N;
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const cvlbm3d_problem& p = c.p;
+  double d[3] = {0.0, 0.0, 0.0}, r[3] = {0.0, 0.0, 0.0};
+  const double time = time_of(clock, t_host, 0.5 * p.dt);
+  const double w2 = p.weight * p.weight;
+  for (int k = p.node_link_start[n]; k < p.node_link_start[n + 1]; ++k) {
+    const int ell = p.node_link_list[k];
+    const int bid = p.link_bid[ell];
+    bool force_all = false;
+    if (p.disp_bid >= 0) {
+      if (bid != p.disp_bid) continue;
+      force_all = true;
+    }
+    const double x = p.link_xb[ell], y = p.link_yb[ell], z = p.link_zb[ell];
+    const double dbx = x - ((double)p.active_i[n] + 0.5) * p.dx;
+    const double dby = y - ((double)p.active_j[n] + 0.5) * p.dy;
+    const double dbz = z - ((double)p.active_k[n] + 0.5) * p.dz;
+    const int mode = p.bc_mode[bid];
+    const double* pp = p.bc_params + bid * 16;
+    for (int comp = 0; comp < 3; ++comp) {
+      if (!(force_all || p.bc_comp_kind[comp * kMaxIds3 + bid] == kDirichlet)) continue;
+      const double ub = disp3(mode, pp, comp, x, y, z, time);
+      const double* F = U + (size_t)(3 + 3 * comp) * N;
+      double e0 = F[n], e1 = F[(size_t)N + n], e2 = F[2 * (size_t)N + n];
+      if (comp == 0) e0 = e0 - 1.0;
+      if (comp == 1) e1 = e1 - 1.0;
+      if (comp == 2) e2 = e2 - 1.0;
+      const double rhs = ub - (e0 * dbx + e1 * dby + e2 * dbz);
+      d[comp] = d[comp] + w2;
+      r[comp] = r[comp] + w2 * rhs;
+    }
+  }
+  const double* Ub = U + 3 * (size_t)N;
+  double Fs[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) Fs[k] = Ub[(size_t)k * N + n];
+#pragma unroll
+  for (int q = 0; q < kQ3; ++q) {
+    const int m = p.neighbor[(size_t)q * N + n];
+    if (m < 0) continue;
+    const double ddx = (double)dx3(q) * p.dx, ddy = (double)dy3(q) * p.dy,
+                 ddz = (double)dz3(q) * p.dz;
+    const double g0 = 0.5 * ((Fs[0] + Ub[m] - 2.0) * ddx + (Fs[1] + Ub[N + m]) * ddy +
+                             (Fs[2] + Ub[2 * (size_t)N + m]) * ddz);
+    const double g1 = 0.5 * ((Fs[3] + Ub[3 * (size_t)N + m]) * ddx +
+                             (Fs[4] + Ub[4 * (size_t)N + m] - 2.0) * ddy +
+                             (Fs[5] + Ub[5 * (size_t)N + m]) * ddz);
+    const double g2 = 0.5 * ((Fs[6] + Ub[6 * (size_t)N + m]) * ddx +
+                             (Fs[7] + Ub[7 * (size_t)N + m]) * ddy +
+                             (Fs[8] + Ub[8 * (size_t)N + m] - 2.0) * ddz);
+    r[0] += ucol[m] - g0;
+    r[1] += ucol[(size_t)N + m] - g1;
+    r[2] += ucol[2 * (size_t)N + m] - g2;
+    d[0] += 1.0;
+    d[1] += 1.0;
+    d[2] += 1.0;
+  }
+  const double hdt = 0.5 * p.dt;
+#pragma unroll
+  for (int comp = 0; comp < 3; ++comp) {
+    const double uo = ucol[(size_t)comp * N + n];
+    double un = uo;
+    if (d[comp] > 0.0) un = uo + p.relax * (r[comp] / d[comp] - uo);
+    u[(size_t)comp * N + n] = un;
+    ustar[(size_t)comp * N + n] = (uo + hdt * U[(size_t)comp * N + n]) + (un - uo);
+  }
+}
+
+// Collision + F repair + push streaming (three_d/curved_boundary_warp3d.py
+// :2192-2330, 2543-2672).  `u` is the swept displacement of every node.
+//
+// A block takes 32 consecutive active nodes with six warps, warp q owning
+// direction q (lane = node), so every population load and store is one
+// coalesced 256-byte row:
+//   1  warp q loads f0[q][0..11] of its 32 nodes (kept in registers, copied
+//      to shared memory for the moments)
+//   2  moments (summed over q in order) and the nine targets of I + grad u
+//      (+-2 star stencil of the swept u), spread over the block
+//   3  warp 0: P(F); warp 1: the repaired F, P(F_repaired), U / U_need rows
+//   4  warp q: collision, repair delta and push of direction q
+constexpr int kCN = 32;  // nodes per collide block (one per lane)
+
+struct CollideSmem3 {
+  double f[kQ3][kC3][kCN];
+  double S[kC3][kCN];
+  double T[9][kCN];   // I + grad u
+  double Po[9][kCN];  // P(F)
+  double Pn[9][kCN];  // P(F_repaired)
+  double dF[9][kCN];  // F_repaired - F
+  int rep[kCN];
+};
+
+// feq of (q, a) with the moments and P(F) of lane `l` in shared memory; the
+// same operations as feq3 (zero-weight axes included).
+__device__ __forceinline__ double feq3_smem(int q, int a, const CollideSmem3& sm, int l,
+                                            double three_over_c, double sixth) {
+  const double sx = (double)dx3(q), sy = (double)dy3(q), sz = (double)dz3(q);
+  double f0, f1, f2;
+  if (a < 3) {
+    f0 = -sm.Po[3 * a][l];
+    f1 = -sm.Po[3 * a + 1][l];
+    f2 = -sm.Po[3 * a + 2][l];
+  } else {
+    const int r = a - 3, ax = r % 3;
+    const double v = -sm.S[r / 3][l];
+    f0 = ax == 0 ? v : 0.0;
+    f1 = ax == 1 ? v : 0.0;
+    f2 = ax == 2 ? v : 0.0;
+  }
+  return sixth * (sm.S[a][l] + three_over_c * (sx * f0 + sy * f1 + sz * f2));
+}
+
+__global__ void __launch_bounds__(kQ3 * kCN, 4)
+    k3_collide(Ctx3 c, Fused3 fz, const double* __restrict__ f0, double* __restrict__ f1,
+               double* __restrict__ U, const double* __restrict__ u, int do_repair,
+               int store_all) {
+  __shared__ CollideSmem3 sm;
+  const int N = c.N;
+  const cvlbm3d_problem& p = c.p;
+  const Mat& m = c.m;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int n0 = blockIdx.x * kCN;
+  const int n = n0 + lane;
+  const bool live = n < N;
+
+  // 1: populations of direction `warp`
+  double v[kC3];
+  const int q = warp;
+#pragma unroll
+  for (int a = 0; a < kC3; ++a) v[a] = live ? f0[(size_t)(q * kC3 + a) * N + n] : 0.0;
+#pragma unroll
+  for (int a = 0; a < kC3; ++a) sm.f[q][a][lane] = v[a];
+  __syncthreads();
+
+  // 2: moments (12 x 32 sums) and I + grad u (9 x 32 targets)
+  const double hdt = 0.5 * p.dt;
+  for (int t = threadIdx.x; t < kC3 * kCN; t += blockDim.x) {
+    const int a = t / kCN, l = t % kCN;
+    double sacc = 0.0;
+#pragma unroll
+    for (int qq = 0; qq < kQ3; ++qq) sacc += sm.f[qq][a][l];
+    if (p.source_mode == kSrcConstant) {
+      sacc += hdt * p.source[a];
+    } else if (p.source_mode == kSrcDamping && a < 3) {
+      const double den = 1.0 + hdt * p.source[0];
+      sacc = sacc / den;
+    }
+    sm.S[a][l] = sacc;
+  }
+  if (do_repair) {
+    const double h[3] = {p.dx, p.dy, p.dz};
+    for (int t = threadIdx.x; t < 9 * kCN; t += blockDim.x) {
+      const int k = t / kCN, l = t % kCN, comp = k / 3, ax = k % 3;
+      const int nn = n0 + l;
+      double g = 0.0;
+      if (nn < N) g = du_axis3(u + (size_t)comp * N, p.neighbor, N, nn, ax, ax + 3, h[ax]);
+      sm.T[k][l] = comp == ax ? 1.0 + g : g;
+    }
+  }
+  __syncthreads();
+
+  // 3: P(F) on warp 0; repaired F, its Piola and the U rows on warp 1
+  if (warp == 0) {
+    double F[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) F[k] = sm.S[3 + k][lane];
+    const M3 Po = piola3(F, m);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) sm.Po[k][lane] = Po.v[k];
+  } else if (warp == 1) {
+    bool repaired = false;
+    double nn[9];
+    if (do_repair) {
+      const double beta = fmax(0.0, fmin(1.0, p.blend));
+#pragma unroll
+      for (int k = 0; k < 9; ++k)
+        nn[k] = sm.S[3 + k][lane] + beta * (sm.T[k][lane] - sm.S[3 + k][lane]);
+      if (det3v(nn) > m.jf) {
+        repaired = true;
+        const M3 Pn = piola3(nn, m);
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+          sm.Pn[k][lane] = Pn.v[k];
+          sm.dF[k][lane] = nn[k] - sm.S[3 + k][lane];
+        }
+        if (store_all && live) {
+#pragma unroll
+          for (int k = 0; k < 9; ++k) U[(size_t)(3 + k) * N + n] = nn[k];
+        }
+      }
+    }
+    sm.rep[lane] = repaired ? 1 : 0;
+    const int slot = live ? fz.need_slot[n] : -1;
+    if (slot >= 0) {
+      double* row = fz.Uneed + (size_t)slot * kC3;
+      row[0] = sm.S[0][lane];
+      row[1] = sm.S[1][lane];
+      row[2] = sm.S[2][lane];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) row[3 + k] = repaired ? nn[k] : sm.S[3 + k][lane];
+    }
+  }
+  __syncthreads();
+  if (!live) return;
+
+  // 4: collision, repair delta, push of direction q
+  const double k3c = 3.0 / p.c, sixth = 1.0 / 6.0, om = p.omega;
+  const double sw = p.dt * (2.0 - om) * (1.0 / 12.0);
+  const double ff = 0.5 / p.c;
+  const bool repaired = sm.rep[lane] != 0;
+  const int nq = p.neighbor[(size_t)q * N + n];
+  int ell = -1;
+  if (nq < 0) {
+    for (int k = p.node_link_start[n]; k < p.node_link_start[n + 1]; ++k) {
+      const int e = p.node_link_list[k];
+      if (p.link_q[e] == q) ell = e;
+    }
+  }
+  const double sx = (double)dx3(q), sy = (double)dy3(q), sz = (double)dz3(q);
+  const double vel[3] = {sm.S[0][lane], sm.S[1][lane], sm.S[2][lane]};
+#pragma unroll
+  for (int a = 0; a < kC3; ++a) {
+    const double old = v[a];
+    const double fe = feq3_smem(q, a, sm, lane, k3c, sixth);
+    double val = old + om * (fe - old) + sw * source_comp3(a, p.source_mode, p.source, vel);
+    if (repaired) {
+      if (a < 3)
+        val = val - ff * (sx * (sm.Pn[3 * a][lane] - sm.Po[3 * a][lane]) +
+                          sy * (sm.Pn[3 * a + 1][lane] - sm.Po[3 * a + 1][lane]) +
+                          sz * (sm.Pn[3 * a + 2][lane] - sm.Po[3 * a + 2][lane]));
+      else
+        val = val + sixth * sm.dF[a - 3][lane];
+    }
+    if (nq >= 0)
+      f1[(size_t)(q * kC3 + a) * N + nq] = val;
+    else if (ell >= 0)
+      fz.scratch[(size_t)ell * kC3 + a] = val;
+  }
+}
+
+// -- link kernels -------------------------------------------------------------
+constexpr int kGatherLanes = 16;  // lanes per link in the gather (12 components used)
+
+// Value and gradients of the 12 components at a link from its <= 64
+// characteristic samples, in slot order (_sparse_characteristic_gather,
+// :2675-2700).  The 12 lanes of a link read one 96-byte U_need row per sample.
+__global__ void __launch_bounds__(128)
+    k3_link_gather(Ctx3 c, Fused3 fz, double* __restrict__ char_state) {
+  const cvlbm3d_problem& p = c.p;
+  const int L = p.n_links;
+  const int a = threadIdx.x % kGatherLanes;
+  const int ell = blockIdx.x * (128 / kGatherLanes) + threadIdx.x / kGatherLanes;
+  if (ell >= L || a >= kC3 || p.char_idx[ell] < 0) return;
+  double v0 = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
+  // samples in chunks of 8: every load of a chunk is issued before its sums,
+  // which keep the slot order
+  constexpr int kChunk = 8;
+#pragma unroll 1
+  for (int m0 = 0; m0 < kChar; m0 += kChunk) {
+    int q[kChunk];
+    double uv[kChunk], w0[kChunk], w1[kChunk], w2[kChunk], w3[kChunk];
+#pragma unroll
+    for (int k = 0; k < kChunk; ++k) q[k] = fz.char_slot[(size_t)(m0 + k) * L + ell];
+#pragma unroll
+    for (int k = 0; k < kChunk; ++k) {
+      const size_t mm = (size_t)(m0 + k);
+      w0[k] = p.char_w[((size_t)0 * kChar + mm) * L + ell];
+      w1[k] = p.char_w[((size_t)1 * kChar + mm) * L + ell];
+      w2[k] = p.char_w[((size_t)2 * kChar + mm) * L + ell];
+      w3[k] = p.char_w[((size_t)3 * kChar + mm) * L + ell];
+    }
+#pragma unroll
+    for (int k = 0; k < kChunk; ++k) uv[k] = q[k] >= 0 ? fz.Uneed[(size_t)q[k] * kC3 + a] : 0.0;
+#pragma unroll
+    for (int k = 0; k < kChunk; ++k) {
+      if (q[k] >= 0) {
+        v0 += w0[k] * uv[k];
+        gx += w1[k] * uv[k];
+        gy += w2[k] * uv[k];
+        gz += w3[k] * uv[k];
+      }
+    }
+  }
+  char_state[((size_t)0 * 12 + a) * L + ell] = v0;
+  char_state[((size_t)1 * 12 + a) * L + ell] = gx;
+  char_state[((size_t)2 * 12 + a) * L + ell] = gy;
+  char_state[((size_t)3 * 12 + a) * L + ell] = gz;
+}
+
+// Boundary value, F predictor, Newton normal solve and P(F_b) of one link;
+// the results go to the link buffers (link_kind .. link_Pb), which the
+// reference also exposes (three_d/curved_boundary_warp3d.py:4281-4337).
+__global__ void __launch_bounds__(128)
+    k3_link_prepare(Ctx3 c, Fused3 fz, const double* __restrict__ u, cvlbm3d_fields fl,
+                    const double* clock, double t_host, double offset) {
+  const cvlbm3d_problem& p = c.p;
+  const Mat& m = c.m;
+  const int L = p.n_links, N = c.N;
+  const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= L) return;
+  const int ell = fz.order ? fz.order[slot] : slot;
+  const double t = time_of(clock, t_host, offset);
+  const int bid = p.link_bid[ell];
+  const int kind = p.bc_kind[bid], mode = p.bc_mode[bid];
+  int ck[3];
+  for (int r = 0; r < 3; ++r) ck[r] = p.bc_comp_kind[r * kMaxIds3 + bid];
+  const double* pp = p.bc_params + bid * 16;
+  const double x = p.link_xb[ell], y = p.link_yb[ell], z = p.link_zb[ell];
+  const double nx = p.link_nx[ell], ny = p.link_ny[ell], nz = p.link_nz[ell];
+  const int n = p.link_p[ell];
+  const int upid = p.link_up[ell];
+  const double eta = p.link_eta[ell];
+  double T[3];
+  for (int r = 0; r < 3; ++r) T[r] = value3(r, mode, pp, x, y, z, nx, ny, nz, t, m.jf);
+  if (p.dyn_enabled && p.dyn_enabled[ell] != 0)
+    for (int r = 0; r < 3; ++r) T[r] = p.dyn_traction[(size_t)r * L + ell];
+  double Fb[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  double Pb[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  const bool anyN = ck[0] == kNeumann || ck[1] == kNeumann || ck[2] == kNeumann;
+  if (anyN) {
+    const double* Un = fz.Uneed + (size_t)fz.need_slot[n] * kC3;
+    double F[9];
+    for (int k = 0; k < 9; ++k) F[k] = Un[3 + k];
+    if (p.recon == 2 || p.recon == 4) {
+      if (upid >= 0) {
+        const double* Uu = fz.Uneed + (size_t)fz.need_slot[upid] * kC3;
+        for (int k = 0; k < 9; ++k) F[k] = Un[3 + k] + eta * (Un[3 + k] - Uu[3 + k]);
+      }
+      if (p.recon == 2 && p.has_tangent_lsq && p.lsq_valid[ell] != 0) {
+        Frame3 fr = frame3(nx, ny, nz);
+        double du1[3] = {0, 0, 0}, du2[3] = {0, 0, 0}, wt_abs = 0.0;
+        for (int mm = 0; mm < kMaxLsq3; ++mm) {
+          const int q = p.lsq_p[(size_t)ell * kMaxLsq3 + mm];
+          if (q >= 0) {
+            const double w1 = p.lsq_wt1[(size_t)ell * kMaxLsq3 + mm];
+            const double w2 = p.lsq_wt2[(size_t)ell * kMaxLsq3 + mm];
+            for (int r = 0; r < 3; ++r) {
+              du1[r] += w1 * u[(size_t)r * N + q];
+              du2[r] += w2 * u[(size_t)r * N + q];
+            }
+            wt_abs += fabs(w1) + fabs(w2);
+          }
+        }
+        if (wt_abs > 0.0) {
+          double h[3], g1[3], g2[3];
+          for (int r = 0; r < 3; ++r) {
+            h[r] = F[3 * r] * fr.n[0] + F[3 * r + 1] * fr.n[1] + F[3 * r + 2] * fr.n[2];
+            g1[r] = fr.t1[r] + du1[r];
+            g2[r] = fr.t2[r] + du2[r];
+          }
+          for (int r = 0; r < 3; ++r)
+            for (int s = 0; s < 3; ++s)
+              F[3 * r + s] = h[r] * fr.n[s] + g1[r] * fr.t1[s] + g2[r] * fr.t2[s];
+        }
+      }
+    }
+    if (p.recon == 3 && p.has_char && p.char_idx[ell] >= 0)
+      for (int k = 0; k < 9; ++k) F[k] = fl.char_state[((size_t)0 * 12 + 3 + k) * L + ell];
+    else if (p.recon == 3)
+      for (int k = 0; k < 9; ++k) F[k] = 0.0;
+    for (int k = 0; k < 9; ++k) Fb[k] = F[k];
+    if (ck[0] == kNeumann && ck[1] == kNeumann && ck[2] == kNeumann)
+      solve_Fb3(F, nx, ny, nz, T, m, p.normal_solver, Fb);
+    const M3 P = piola3(Fb, m);
+    for (int k = 0; k < 9; ++k) Pb[k] = P.v[k];
+  }
+  fl.link_kind[ell] = kind;
+  for (int r = 0; r < 3; ++r) {
+    fl.link_comp_kind[(size_t)r * L + ell] = ck[r];
+    fl.link_bv[(size_t)r * L + ell] = T[r];
+  }
+  for (int k = 0; k < 9; ++k) {
+    fl.link_Fb[(size_t)k * L + ell] = Fb[k];
+    fl.link_Pb[(size_t)k * L + ell] = Pb[k];
+  }
+}
+
+__device__ __forceinline__ bool char_rows3(const cvlbm3d_problem& p, int ell) {
+  return p.has_char && p.char_idx[ell] >= 0;
+}
+
+// BFL value of row `a` of one link (:3154-3241) with the outgoing populations
+// taken from link_scratch and the post-stream f1.
+__global__ void __launch_bounds__(128)
+    k3_link_rows(Ctx3 c, Fused3 fz, double* __restrict__ f1, cvlbm3d_fields fl) {
+  const cvlbm3d_problem& p = c.p;
+  const int L = p.n_links, N = c.N;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)L * kC3) return;
+  const int ell = (int)(t / kC3), a = (int)(t - (long long)ell * kC3);
+  const int row = a < 3 ? a : (a - 3) / 3;
+  const int ckr = fl.link_comp_kind[(size_t)row * L + ell];
+  const bool anyN = fl.link_comp_kind[ell] == kNeumann ||
+                    fl.link_comp_kind[(size_t)L + ell] == kNeumann ||
+                    fl.link_comp_kind[2 * (size_t)L + ell] == kNeumann;
+  // rows the characteristic closure overwrites are written by k3_link_char
+  if (anyN && ckr == kNeumann && char_rows3(p, ell)) return;
+  const int n = p.link_p[ell], upid = p.link_up[ell], qo = p.link_q[ell];
+  const int qi = opp3(qo);
+  double eta = p.link_eta[ell];
+  if (p.recon == 1) eta = 0.5;
+  const double din[3] = {(double)dx3(qi), (double)dy3(qi), (double)dz3(qi)};
+  const double cc = p.c;
+  double D = 1.0, S = 0.0;
+  if (ckr == kDirichlet) {
+    const double Tr = fl.link_bv[(size_t)row * L + ell];
+    if (a < 3) {
+      D = -1.0;
+      S = fl.link_bv[(size_t)a * L + ell] / 3.0;
+    } else {
+      const int col = (a - 3) - row * 3;
+      S = -din[col] * Tr / cc;
+    }
+  } else {
+    if (a < 3) {
+      const double* Pb = fl.link_Pb;
+      S = -(din[0] * Pb[(size_t)(3 * a) * L + ell] + din[1] * Pb[(size_t)(3 * a + 1) * L + ell] +
+            din[2] * Pb[(size_t)(3 * a + 2) * L + ell]) / cc;
+    } else {
+      D = -1.0;
+      S = fl.link_Fb[(size_t)(a - 3) * L + ell] / 3.0;
+    }
+  }
+  const double fo = fz.scratch[(size_t)ell * kC3 + a];
+  double val;
+  if (eta >= 0.5) {
+    const double fi = upid >= 0 ? f1[(size_t)(qi * kC3 + a) * N + upid]
+                                : fz.scratch[(size_t)fz.partner[ell] * kC3 + a];
+    const double al = 1.0 / (2.0 * eta);
+    val = al * (D * fo + S) + (1.0 - al) * fi;
+  } else {
+    const double up = upid >= 0 ? f1[(size_t)(qo * kC3 + a) * N + n] : fo;
+    val = D * (2.0 * eta * fo + (1.0 - 2.0 * eta) * up) + S;
+  }
+  f1[(size_t)(qi * kC3 + a) * N + n] = val;
+}
+
+// Characteristic rows (:2812-2884) of links with a Neumann row.
+__global__ void __launch_bounds__(64)
+    k3_link_char(Ctx3 c, Fused3 fz, double* __restrict__ f1, cvlbm3d_fields fl) {
+  const cvlbm3d_problem& p = c.p;
+  const Mat& m = c.m;
+  const int L = p.n_links, N = c.N;
+  const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= L) return;
+  const int ell = fz.order ? fz.order[slot] : slot;
+  if (!char_rows3(p, ell)) return;
+  int ck[3];
+  for (int r = 0; r < 3; ++r) ck[r] = fl.link_comp_kind[(size_t)r * L + ell];
+  if (!(ck[0] == kNeumann || ck[1] == kNeumann || ck[2] == kNeumann)) return;
+  const int n = p.link_p[ell], qi = opp3(p.link_q[ell]);
+  const double din[3] = {(double)dx3(qi), (double)dy3(qi), (double)dz3(qi)};
+  double Ub[12], G[3][12];
+  const double* Un = fz.Uneed + (size_t)fz.need_slot[n] * kC3;
+  for (int a = 0; a < 3; ++a)
+    Ub[a] = ck[a] == kDirichlet ? fl.link_bv[(size_t)a * L + ell] : Un[a];
+  for (int k = 0; k < 9; ++k) Ub[3 + k] = fl.link_Fb[(size_t)k * L + ell];
+  if (state_det3(Ub) <= m.jf) *fl.invalid = 1;
+  for (int d = 0; d < 3; ++d)
+    for (int a = 0; a < 12; ++a) G[d][a] = fl.char_state[((size_t)(1 + d) * 12 + a) * L + ell];
+  double out[12];
+  char_population3(Ub, G[0], G[1], G[2], din, p.link_eta[ell], p.dt, p.c, p, m, p.omega, out);
+  for (int a = 0; a < 12; ++a) {
+    const int row = a < 3 ? a : (a - 3) / 3;
+    if (ck[row] == kNeumann) f1[(size_t)(qi * kC3 + a) * N + n] = out[a];
+  }
+}
+
+}  // namespace

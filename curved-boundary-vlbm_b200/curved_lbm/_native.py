@@ -78,13 +78,16 @@ class Problem3D(C.Structure):
         ("node_link_start", pI), ("node_link_list", pI),
         ("bc_kind", pI), ("bc_mode", pI), ("bc_comp_kind", pI), ("bc_params", pI),
         ("dyn_enabled", pI), ("dyn_traction", pI),
+        ("need_slot", pI), ("n_need", i32), ("reserved3", i32), ("char_slot", pI),
+        ("link_partner", pI), ("link_order", pI),
     ]
 
 
 class Fields3D(C.Structure):
     _fields_ = [(name, pI) for name in
                 ("f0", "f1", "U", "u", "u_next", "u_star", "link_kind", "link_comp_kind",
-                 "link_bv", "link_Fb", "link_Pb", "char_state", "invalid", "clock")]
+                 "link_bv", "link_Fb", "link_Pb", "char_state", "invalid", "clock",
+                 "link_scratch", "U_need")]
 
 
 EXPORTED = (

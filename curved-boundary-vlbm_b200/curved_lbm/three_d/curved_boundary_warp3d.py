@@ -152,6 +152,52 @@ def _recon_name(rid: int) -> str:
         int(rid), f"unknown({rid})")
 
 
+def _fused_tables3(tables, link_q, comp_kind, stencil, n_active):
+    """Tables of the fused 3-D step, or None when the links do not allow it.
+
+    * need_slot: for each active node whose post-step U some cut link reads
+      (the cut node, its upstream node and the characteristic stencil) its
+      row in the U_need buffer, -1 elsewhere; char_slot: the characteristic
+      stencil's node ids mapped to those rows;
+    * partner: for link (p, q_out) whose upstream node p - c_q is not active,
+      the link (p, q_in) at the same node, whose stored outgoing population is
+      this link's post-collision f[q_in](p); -1 when the upstream is active;
+    * order: links with a Neumann row first, so the warps of the
+      one-thread-per-link kernels take the same branches.
+    """
+    link_p = np.asarray(tables["link_p"], dtype=np.int64)
+    up = np.asarray(tables["link_upstream"], dtype=np.int64)
+    q = np.asarray(link_q, dtype=np.int64)
+    nl = link_p.size
+    need = np.zeros(n_active, dtype=bool)
+    if nl:
+        need[link_p] = True
+        need[up[up >= 0]] = True
+    idx = None
+    if stencil is not None:
+        idx = np.asarray(stencil["indices"], dtype=np.int64)
+        need[idx[idx >= 0]] = True
+    need_slot = np.full(n_active, -1, dtype=np.int32)
+    need_slot[need] = np.arange(int(need.sum()), dtype=np.int32)
+    char_slot = None
+    if idx is not None:
+        char_slot = np.where(idx >= 0, need_slot[np.maximum(idx, 0)], -1).astype(np.int32)
+    partner = np.full(nl, -1, dtype=np.int32)
+    if nl:
+        key = link_p * 6 + q
+        pos = {int(k): e for e, k in enumerate(key)}
+        for e in np.flatnonzero(up < 0):
+            qi = (int(q[e]) + 3) % 6
+            j = pos.get(int(link_p[e]) * 6 + qi, -1)
+            if j < 0:
+                return None
+            partner[e] = j
+    neumann = (np.any(np.asarray(comp_kind).reshape(3, -1) == BC_NEUMANN, axis=0) if nl
+               else np.zeros(0, bool))
+    order = np.concatenate([np.flatnonzero(neumann), np.flatnonzero(~neumann)]).astype(np.int32)
+    return need_slot, char_slot, partner, np.ascontiguousarray(order)
+
+
 def _node_link_csr(link_node: np.ndarray, n_nodes: int):
     valid = link_node >= 0
     ids = np.flatnonzero(valid).astype(np.int32)
@@ -316,6 +362,17 @@ class WarpSparseCurvedBoundaryLBM3D:
         if self.characteristic_stencil is not None:
             t["char_idx"] = dev_i(self.characteristic_stencil["indices"])
             t["char_w"] = dev_f(self.characteristic_stencil["weights"])
+        fused = _fused_tables3(tables, geometry.link_q, ck, self.characteristic_stencil,
+                               self.n_active)
+        self._n_need = 0
+        if fused is not None:
+            need_slot, char_slot, partner, order = fused
+            self._n_need = int(need_slot.max()) + 1 if need_slot.size else 0
+            t["need_slot"] = dev_i(need_slot)
+            if char_slot is not None:
+                t["char_slot"] = dev_i(char_slot)
+            t["link_partner"] = dev_i(partner)
+            t["link_order"] = dev_i(order)
         self._tables = t
         self.neighbor = t["neighbor"]
         self.link_p = t["link_p"]
@@ -339,6 +396,8 @@ class WarpSparseCurvedBoundaryLBM3D:
                            else torch.zeros((1, 1, 1), dtype=f64, device=dev))
         self.invalid = torch.zeros(1, dtype=i32, device=dev)
         self._clock = torch.zeros(1, dtype=f64, device=dev)
+        self.link_scratch = torch.zeros(max(1, 12 * nl), dtype=f64, device=dev)
+        self.U_need = torch.zeros(max(1, 12 * self._n_need), dtype=f64, device=dev)
         self.source_params_wp = self.source_params.copy()
         self._problem = self._make_problem()
         self.initialize_identity()
@@ -369,6 +428,7 @@ class WarpSparseCurvedBoundaryLBM3D:
         p.blend = self.local_compatibility_blend
         for name, tensor in self._tables.items():
             setattr(p, name, _native.ptr(tensor))
+        p.n_need = self._n_need
         p.dyn_enabled = _native.ptr(self.dynamic_traction_override_enabled)
         p.dyn_traction = _native.ptr(self.dynamic_traction_override)
         return p
@@ -383,7 +443,8 @@ class WarpSparseCurvedBoundaryLBM3D:
                              ("link_bv", self.link_bv), ("link_Fb", self.link_Fb),
                              ("link_Pb", self.link_Pb),
                              ("char_state", self.char_state if has_char else None),
-                             ("invalid", self.invalid), ("clock", self._clock)):
+                             ("invalid", self.invalid), ("clock", self._clock),
+                             ("link_scratch", self.link_scratch), ("U_need", self.U_need)):
             setattr(fl, name, _native.ptr(tensor))
         return fl
 

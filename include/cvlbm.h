@@ -199,6 +199,18 @@ typedef struct cvlbm3d_problem {
   const double *bc_params;                        /* [16*16] */
   const int32_t *dyn_enabled;                     /* [n_links] */
   const double *dyn_traction;                     /* [3*n_links] */
+  /* fused step (optional; need_slot, link_partner and fields->link_scratch,
+     fields->U_need all set enable it when disp_sweeps <= 1) */
+  const int32_t *need_slot;                       /* [n_active] row of U_need holding the
+                                                     node's post-step U, or -1 */
+  int32_t n_need;                                 /* rows of U_need */
+  int32_t reserved3;
+  const int32_t *char_slot;                       /* [64*n_links] char_idx mapped to
+                                                     U_need rows (-1 unused) */
+  const int32_t *link_partner;                    /* [n_links] link at the same node in the
+                                                     incoming direction, or -1 */
+  const int32_t *link_order;                      /* [n_links] processing order of the
+                                                     one-thread-per-link kernels (optional) */
 } cvlbm3d_problem;
 
 typedef struct cvlbm3d_fields {
@@ -211,6 +223,10 @@ typedef struct cvlbm3d_fields {
   double *char_state;       /* [4*12*n_links] value, d/dx, d/dy, d/dz */
   int32_t *invalid;
   double *clock;
+  double *link_scratch;     /* [12*n_links] fused step: post-collision populations
+                               leaving through each cut link */
+  double *U_need;           /* [n_need*12] fused step: post-step U of the nodes cut
+                               links read, one 96-byte row per node */
 } cvlbm3d_fields;
 
 /* Replaces WarpSparseCurvedBoundaryLBM3D.step
