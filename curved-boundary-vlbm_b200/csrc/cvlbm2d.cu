@@ -721,3 +721,8 @@ extern "C" int cvlbm2d_run_static_scratch(const cvlbm2d_problem* p, cvlbm2d_fiel
   f->f1 = local.f1;
   return rc;
 }
+
+// ---------------------------------------------------------------------------
+// Batched step of many independent 2-D problems (see cvlbm2d_batch.cuh).
+// ---------------------------------------------------------------------------
+#include "cvlbm2d_batch.cuh"

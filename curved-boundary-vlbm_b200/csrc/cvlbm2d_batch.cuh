@@ -1,0 +1,368 @@
+// Batched D2Q4x6 step: many independent problems (geometries, load cases,
+// uneven lattice sizes) advanced together.  Included at the end of
+// cvlbm2d.cu; reuses the fused tile body (fused2_tile) and the cooperative
+// link body (link2_group).
+//
+// Per lattice step three launches cover every instance:
+//   k_batch_nodes2   persistent: a grid of (SMs x resident blocks) walks the
+//                    work list of (instance, tile) pairs
+//   k_batch_links2   persistent: walks (instance, 8-link group) pairs
+//   k_batch_tick2    advances each active instance's clock and step counter
+// Every `check_every` steps the node kernel also stores U and u of every
+// active node, k_batch_partial2 reduces v.v and u.u per (instance, tile) in a
+// fixed order and k_batch_residual2 retires instances whose residual
+// dt*|v|_2/|u|_2 fell below the tolerance (after a minimum time, e.g. the end
+// of a load ramp).  Retired instances' work items return at once.  The whole
+// step sequence is captured in one CUDA graph (cvlbm2d_batch_graph_create).
+//
+// Each instance keeps its own population and u* ping-pong; the buffer that
+// holds the current state is selected by the parity of the steps the instance
+// has taken inside the batch.
+#pragma once
+
+#include <vector>
+
+namespace {
+
+struct Inst2 {
+  Ctx2 c;
+  const uint8_t* need;
+  const int32_t* partner;
+  double* scratch;
+  double* f[2];   // population buffers; f[par] holds the current state
+  double* us[2];  // u* buffers
+  double* U;
+  double* u;
+  int* invalid;
+};
+
+struct InstState2 {
+  long long step;       // step index of the instance (interval tests)
+  long long base;       // step index at batch creation (buffer parity)
+  double clock;         // device time
+  double residual;      // last residual, -1 before the first check
+  int active;           // 1 while stepping
+  int status;           // 0 running, 1 converged, -1 invalid state
+};
+
+__device__ __forceinline__ int parity_of(const InstState2& s) { return (int)((s.step - s.base) & 1); }
+
+template <int TY, int MINB>
+__global__ void __launch_bounds__(kTX * TY, MINB)
+    k_batch_nodes2(const Inst2* __restrict__ inst, InstState2* __restrict__ st,
+                   const int2* __restrict__ work, int n_work, int store_all) {
+  extern __shared__ double smem2[];
+  for (int w = blockIdx.x; w < n_work; w += gridDim.x) {
+    __syncthreads();  // the previous item's phase C still reads shared memory
+    const int2 wk = work[w];
+    if (!st[wk.x].active) continue;
+    const Inst2& I = inst[wk.x];
+    const long long step = st[wk.x].step;
+    const int par = parity_of(st[wk.x]);
+    const cvlbm2d_problem& p = I.c.p;
+    const int sweep = p.disp_interval > 0 && step % p.disp_interval == 0;
+    const int repair = p.rep_interval > 0 && step % p.rep_interval == 0;
+    Fused2 fz{nullptr, 0, p.tiles_j, I.need, I.partner, I.scratch, store_all};
+    fused2_tile<TY>(I.c, fz, wk.y, I.f[par], I.f[par ^ 1], I.U, I.u, I.us[par], I.us[par ^ 1],
+                    I.invalid, &st[wk.x].clock, 0.0, sweep, repair, smem2);
+  }
+}
+
+__global__ void __launch_bounds__(128)
+    k_batch_links2(const Inst2* __restrict__ inst, const InstState2* __restrict__ st,
+                   const int2* __restrict__ work, int n_work) {
+  __shared__ LinkShared2 sh[128 / kLG];
+  const int lane = threadIdx.x & (kLG - 1);
+  const int grp = threadIdx.x / kLG;
+  for (int w = blockIdx.x; w < n_work; w += gridDim.x) {
+    __syncwarp();
+    const int2 wk = work[w];
+    if (!st[wk.x].active) continue;
+    const Inst2& I = inst[wk.x];
+    double* f1 = I.f[parity_of(st[wk.x]) ^ 1];
+    link2_group(I.c, sh[grp], lane, wk.y + grp, f1, f1, I.U, I.u, &st[wk.x].clock, 0.0,
+                0.5 * I.c.p.dt, 1, I.scratch, I.partner);
+  }
+}
+
+__global__ void k_batch_tick2(const Inst2* __restrict__ inst, InstState2* __restrict__ st, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || !st[i].active) return;
+  st[i].clock = st[i].clock + inst[i].c.p.dt;
+  st[i].step = st[i].step + 1;
+  if (*inst[i].invalid) {  // non-positive Jacobian: stop this instance, keep the others
+    st[i].active = 0;
+    st[i].status = -1;
+  }
+}
+
+// Per (instance, tile): sum of |v|^2 and |u|^2 over the tile's active nodes,
+// reduced in a fixed order (deterministic for a given tile height).
+template <int TY>
+__global__ void __launch_bounds__(kTX * TY)
+    k_batch_partial2(const Inst2* __restrict__ inst, const InstState2* __restrict__ st,
+                     const int2* __restrict__ work, int n_work, double2* __restrict__ partial) {
+  __shared__ double sv[kTX * TY], su[kTX * TY];
+  for (int w = blockIdx.x; w < n_work; w += gridDim.x) {
+    __syncthreads();
+    const int2 wk = work[w];
+    const Inst2& I = inst[wk.x];
+    const cvlbm2d_problem& p = I.c.p;
+    const int N = I.c.N;
+    const int i = (wk.y / p.tiles_j) * TY + (int)(threadIdx.x >> 5);
+    const int j = (wk.y % p.tiles_j) * kTX + (int)(threadIdx.x & 31);
+    double v2 = 0.0, u2 = 0.0;
+    if (st[wk.x].active && i < p.nx && j < p.ny && p.active[i * p.ny + j]) {
+      const int n = i * p.ny + j;
+      const double v0 = I.U[n], v1 = I.U[(size_t)N + n];
+      const double u0 = I.u[n], u1 = I.u[(size_t)N + n];
+      v2 = v0 * v0 + v1 * v1;
+      u2 = u0 * u0 + u1 * u1;
+    }
+    sv[threadIdx.x] = v2;
+    su[threadIdx.x] = u2;
+    __syncthreads();
+    for (int h = (kTX * TY) / 2; h > 0; h >>= 1) {
+      if ((int)threadIdx.x < h) {
+        sv[threadIdx.x] += sv[threadIdx.x + h];
+        su[threadIdx.x] += su[threadIdx.x + h];
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[w] = make_double2(sv[0], su[0]);
+  }
+}
+
+__global__ void k_batch_residual2(const Inst2* __restrict__ inst, InstState2* __restrict__ st,
+                                  const int* __restrict__ work_start,
+                                  const double2* __restrict__ partial, int n, double tol,
+                                  double t_min) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || !st[i].active) return;
+  double sv = 0.0, su = 0.0;
+  for (int w = work_start[i]; w < work_start[i + 1]; ++w) {
+    sv += partial[w].x;
+    su += partial[w].y;
+  }
+  const double dt = inst[i].c.p.dt;
+  const double r = su > 0.0 ? dt * sqrt(sv) / sqrt(su) : (sv > 0.0 ? 1.0 : 0.0);
+  st[i].residual = r;
+  if (st[i].clock >= t_min && r < tol) {
+    st[i].active = 0;
+    st[i].status = 1;
+  }
+}
+
+using BatchNodesFn = void (*)(const Inst2*, InstState2*, const int2*, int, int);
+using BatchPartialFn = void (*)(const Inst2*, const InstState2*, const int2*, int, double2*);
+
+struct BatchVariant2 {
+  BatchNodesFn nodes;
+  BatchPartialFn partial;
+  int threads;
+  size_t smem;
+  int tile_i;
+};
+
+BatchVariant2 batch_variant(int v) {
+  switch (v) {
+    case 1: return {k_batch_nodes2<8, 2>, k_batch_partial2<8>, kTX * 8, fused_smem2<8>(), 8};
+    case 2: return {k_batch_nodes2<8, 3>, k_batch_partial2<8>, kTX * 8, fused_smem2<8>(), 8};
+    case 3: return {k_batch_nodes2<16, 2>, k_batch_partial2<16>, kTX * 16, fused_smem2<16>(), 16};
+    case 4: return {k_batch_nodes2<4, 4>, k_batch_partial2<4>, kTX * 4, fused_smem2<4>(), 4};
+    default: return {k_batch_nodes2<16, 1>, k_batch_partial2<16>, kTX * 16, fused_smem2<16>(), 16};
+  }
+}
+
+}  // namespace
+
+struct cvlbm2d_batch {
+  int n_inst = 0;
+  int variant = 0;
+  int node_grid = 0, link_grid = 0;
+  int n_work = 0, n_lwork = 0;
+  Inst2* d_inst = nullptr;
+  InstState2* d_state = nullptr;
+  int2* d_work = nullptr;
+  int2* d_lwork = nullptr;
+  int* d_work_start = nullptr;
+  double2* d_partial = nullptr;
+};
+
+namespace {
+
+void batch_free(cvlbm2d_batch* b) {
+  if (!b) return;
+  cudaFree(b->d_inst);
+  cudaFree(b->d_state);
+  cudaFree(b->d_work);
+  cudaFree(b->d_lwork);
+  cudaFree(b->d_work_start);
+  cudaFree(b->d_partial);
+  delete b;
+}
+
+void batch_step(cvlbm2d_batch* b, int store_all, cudaStream_t s) {
+  const BatchVariant2 v = batch_variant(b->variant);
+  if (b->n_work > 0) {
+    v.nodes<<<b->node_grid, v.threads, v.smem, s>>>(b->d_inst, b->d_state, b->d_work, b->n_work,
+                                                    store_all);
+    cv::count_launches(1);
+  }
+  if (b->n_lwork > 0) {
+    k_batch_links2<<<b->link_grid, 128, 0, s>>>(b->d_inst, b->d_state, b->d_lwork, b->n_lwork);
+    cv::count_launches(1);
+  }
+  k_batch_tick2<<<blocks(b->n_inst, 128), 128, 0, s>>>(b->d_inst, b->d_state, b->n_inst);
+  cv::count_launches(1);
+}
+
+}  // namespace
+
+extern "C" int cvlbm2d_batch_create(int32_t n_inst, const cvlbm2d_problem* problems,
+                                    const cvlbm2d_fields* fields, const int64_t* step0,
+                                    const double* time0, int32_t tile_variant,
+                                    int32_t grid_blocks, cvlbm2d_batch** out) {
+  if (!out || !problems || !fields || !step0 || !time0 || n_inst <= 0)
+    return fail(CVLBM_ERR_INVALID_ARG, "cvlbm2d_batch_create: bad arguments");
+  *out = nullptr;
+  const int tile_i = cvlbm2d_tile_variant(tile_variant);
+  if (tile_i <= 0) return fail(CVLBM_ERR_INVALID_ARG, "cvlbm2d_batch_create: unknown tile variant");
+  std::vector<Inst2> hi(n_inst);
+  std::vector<InstState2> hs(n_inst);
+  std::vector<int2> work, lwork;
+  std::vector<int> work_start(n_inst + 1, 0);
+  std::vector<int> tiles;
+  for (int i = 0; i < n_inst; ++i) {
+    const cvlbm2d_problem* p = &problems[i];
+    const cvlbm2d_fields* f = &fields[i];
+    int rc = check_problem(p, f);
+    if (rc) return rc;
+    if (!fused_ok(p, f) || p->tile_i != tile_i)
+      return fail(CVLBM_ERR_INVALID_ARG,
+                  "cvlbm2d_batch_create: every instance needs the fused-step tables built for "
+                  "the batch's tile variant");
+    hi[i].c = make_ctx(p);
+    hi[i].need = p->need_fields;
+    hi[i].partner = p->link_partner;
+    hi[i].scratch = f->link_scratch;
+    hi[i].f[0] = f->f0;
+    hi[i].f[1] = f->f1;
+    hi[i].us[0] = f->u_star;
+    hi[i].us[1] = f->u_next;
+    hi[i].U = f->U;
+    hi[i].u = f->u;
+    hi[i].invalid = f->invalid;
+    hs[i] = InstState2{step0[i], step0[i], time0[i], -1.0, 1, 0};
+    tiles.resize(p->n_tiles);
+    if (p->n_tiles > 0 &&
+        cudaMemcpy(tiles.data(), p->tiles, sizeof(int) * p->n_tiles, cudaMemcpyDeviceToHost) !=
+            cudaSuccess)
+      return fail(CVLBM_ERR_CUDA, "cvlbm2d_batch_create: reading a tile list failed");
+    work_start[i] = (int)work.size();
+    for (int t : tiles) work.push_back(make_int2(i, t));
+    for (int l = 0; l < p->n_links; l += 128 / kLG) lwork.push_back(make_int2(i, l));
+  }
+  work_start[n_inst] = (int)work.size();
+  cvlbm2d_batch* b = new cvlbm2d_batch();
+  b->n_inst = n_inst;
+  b->variant = tile_variant;
+  b->n_work = (int)work.size();
+  b->n_lwork = (int)lwork.size();
+  const BatchVariant2 v = batch_variant(tile_variant);
+  cudaFuncSetAttribute(v.nodes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v.smem);
+  int dev = 0, sms = 148, per_sm = 1, per_sm_l = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.nodes, v.threads, v.smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_l, k_batch_links2, 128, 0);
+  const int full = sms * (per_sm > 0 ? per_sm : 1);
+  b->node_grid = grid_blocks > 0 ? grid_blocks : full;
+  if (b->node_grid > b->n_work) b->node_grid = b->n_work > 0 ? b->n_work : 1;
+  b->link_grid = sms * (per_sm_l > 0 ? per_sm_l : 1);
+  if (b->link_grid > b->n_lwork) b->link_grid = b->n_lwork > 0 ? b->n_lwork : 1;
+  bool ok = cudaMalloc(&b->d_inst, sizeof(Inst2) * n_inst) == cudaSuccess &&
+            cudaMalloc(&b->d_state, sizeof(InstState2) * n_inst) == cudaSuccess &&
+            cudaMalloc(&b->d_work, sizeof(int2) * (work.size() + 1)) == cudaSuccess &&
+            cudaMalloc(&b->d_lwork, sizeof(int2) * (lwork.size() + 1)) == cudaSuccess &&
+            cudaMalloc(&b->d_work_start, sizeof(int) * (n_inst + 1)) == cudaSuccess &&
+            cudaMalloc(&b->d_partial, sizeof(double2) * (work.size() + 1)) == cudaSuccess;
+  ok = ok && cudaMemcpy(b->d_inst, hi.data(), sizeof(Inst2) * n_inst,
+                        cudaMemcpyHostToDevice) == cudaSuccess;
+  ok = ok && cudaMemcpy(b->d_state, hs.data(), sizeof(InstState2) * n_inst,
+                        cudaMemcpyHostToDevice) == cudaSuccess;
+  ok = ok && (work.empty() || cudaMemcpy(b->d_work, work.data(), sizeof(int2) * work.size(),
+                                         cudaMemcpyHostToDevice) == cudaSuccess);
+  ok = ok && (lwork.empty() || cudaMemcpy(b->d_lwork, lwork.data(), sizeof(int2) * lwork.size(),
+                                          cudaMemcpyHostToDevice) == cudaSuccess);
+  ok = ok && cudaMemcpy(b->d_work_start, work_start.data(), sizeof(int) * (n_inst + 1),
+                        cudaMemcpyHostToDevice) == cudaSuccess;
+  if (!ok) {
+    batch_free(b);
+    return fail(CVLBM_ERR_CUDA, "cvlbm2d_batch_create: device allocation or upload failed");
+  }
+  *out = b;
+  return CVLBM_OK;
+}
+
+extern "C" int cvlbm2d_batch_run(cvlbm2d_batch* b, int32_t nsteps, int32_t check_every,
+                                 double tol, double t_min, void* stream) {
+  if (!b) return fail(CVLBM_ERR_INVALID_ARG, "null batch");
+  if (nsteps < 0) return fail(CVLBM_ERR_INVALID_ARG, "negative step count");
+  cudaStream_t s = (cudaStream_t)stream;
+  const BatchVariant2 v = batch_variant(b->variant);
+  for (int k = 0; k < nsteps; ++k) {
+    const bool check = check_every > 0 && (k + 1) % check_every == 0;
+    int tk = timer_begin(s);
+    batch_step(b, check ? 1 : 0, s);
+    timer_end(tk, s);
+    if (check && b->n_work > 0) {
+      v.partial<<<b->node_grid, v.threads, 0, s>>>(b->d_inst, b->d_state, b->d_work, b->n_work,
+                                                   b->d_partial);
+      cv::count_launches(1);
+      k_batch_residual2<<<blocks(b->n_inst, 128), 128, 0, s>>>(
+          b->d_inst, b->d_state, b->d_work_start, b->d_partial, b->n_inst, tol, t_min);
+      cv::count_launches(1);
+    }
+  }
+  return check_launch("cvlbm2d_batch_run");
+}
+
+extern "C" int cvlbm2d_batch_graph_create(cvlbm2d_batch* b, int32_t nsteps, int32_t check_every,
+                                          double tol, double t_min, cvlbm_graph** out) {
+  if (!b || !out) return fail(CVLBM_ERR_INVALID_ARG, "null batch or output");
+  if (nsteps <= 0) return fail(CVLBM_ERR_INVALID_ARG, "nsteps must be positive");
+  return capture_graph(
+      [&](cudaStream_t s) { return cvlbm2d_batch_run(b, nsteps, check_every, tol, t_min, s); },
+      out);
+}
+
+extern "C" int cvlbm2d_batch_status(cvlbm2d_batch* b, int32_t* active, int32_t* status,
+                                    int64_t* steps, double* time, double* residual,
+                                    void* stream) {
+  if (!b) return fail(CVLBM_ERR_INVALID_ARG, "null batch");
+  std::vector<InstState2> hs(b->n_inst);
+  cudaStream_t s = (cudaStream_t)stream;
+  if (cudaMemcpyAsync(hs.data(), b->d_state, sizeof(InstState2) * b->n_inst,
+                      cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return fail(CVLBM_ERR_CUDA, "cvlbm2d_batch_status: copy failed");
+  for (int i = 0; i < b->n_inst; ++i) {
+    if (active) active[i] = hs[i].active;
+    if (status) status[i] = hs[i].status;
+    if (steps) steps[i] = hs[i].step;
+    if (time) time[i] = hs[i].clock;
+    if (residual) residual[i] = hs[i].residual;
+  }
+  return CVLBM_OK;
+}
+
+extern "C" int cvlbm2d_batch_launch_grid(const cvlbm2d_batch* b, int32_t* node_grid,
+                                         int32_t* n_work) {
+  if (!b) return fail(CVLBM_ERR_INVALID_ARG, "null batch");
+  if (node_grid) *node_grid = b->node_grid;
+  if (n_work) *n_work = b->n_work;
+  return CVLBM_OK;
+}
+
+extern "C" void cvlbm2d_batch_destroy(cvlbm2d_batch* b) { batch_free(b); }

@@ -62,19 +62,18 @@ constexpr size_t fused_smem2() {
          sizeof(int) * kRX * (TY + 2 * kH);
 }
 
-// Tile kTX x TY, one node per thread; MINB resident blocks per SM bounds the
-// registers per thread (tuned per problem, see curved_lbm autotune).
-template <int TY, int MINB>
-__global__ void __launch_bounds__(kTX * TY, MINB)
-    k_fused2(Ctx2 c, Fused2 fz, const double* __restrict__ f0, double* __restrict__ f1,
-             double* __restrict__ Ug, double* __restrict__ ug,
-             const double* __restrict__ ustar, double* __restrict__ ustar_out,
-             int* __restrict__ invalid, const double* clock, double t_host, int do_sweep,
-             int do_repair) {
+// One tile of the fused step (phases A-C above); `tile` is a tile id of the
+// problem's tile list.  Every thread of the block calls it; it returns
+// early only after the last block-wide barrier.
+template <int TY>
+__device__ __forceinline__ void fused2_tile(
+    const Ctx2& c, const Fused2& fz, int tile, const double* __restrict__ f0,
+    double* __restrict__ f1, double* __restrict__ Ug, double* __restrict__ ug,
+    const double* __restrict__ ustar, double* __restrict__ ustar_out, int* __restrict__ invalid,
+    const double* clock, double t_host, int do_sweep, int do_repair, double* smem2) {
   constexpr int kTY = TY;
   constexpr int kRN = kRX * (TY + 2 * kH);
   constexpr int kSN = kSX * (TY + 4);
-  extern __shared__ double smem2[];
   double(*sF)[kRN] = reinterpret_cast<double(*)[kRN]>(smem2);            // collide-time F
   double(*sU)[kRN] = reinterpret_cast<double(*)[kRN]>(smem2 + 4 * kRN);  // collide-time u
   double(*sN)[kSN] = reinterpret_cast<double(*)[kSN]>(smem2 + 6 * kRN);  // swept u, tile+2
@@ -82,7 +81,6 @@ __global__ void __launch_bounds__(kTX * TY, MINB)
 
   const cvlbm2d_problem& p = c.p;
   const int N = c.N, nx = p.nx, ny = p.ny;
-  const int tile = fz.tiles[blockIdx.x];
   const int i0 = (tile / fz.tiles_j) * kTY, j0 = (tile % fz.tiles_j) * kTX;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   const int i = i0 + ty, j = j0 + tx;
@@ -90,7 +88,6 @@ __global__ void __launch_bounds__(kTX * TY, MINB)
   const int n = i * ny + j;
   const bool own_act = own && p.active[n] != 0;
   const int r_own = (ty + kH) * kRX + tx + kH;
-  const double hdt = 0.5 * p.dt;
 
   // -- A: region moments -----------------------------------------------------
   double S[6];
@@ -343,6 +340,20 @@ __global__ void __launch_bounds__(kTX * TY, MINB)
   }
 }
 
+// Tile kTX x TY, one node per thread; MINB resident blocks per SM bounds the
+// registers per thread (tuned per problem, see curved_lbm autotune).
+template <int TY, int MINB>
+__global__ void __launch_bounds__(kTX * TY, MINB)
+    k_fused2(Ctx2 c, Fused2 fz, const double* __restrict__ f0, double* __restrict__ f1,
+             double* __restrict__ Ug, double* __restrict__ ug,
+             const double* __restrict__ ustar, double* __restrict__ ustar_out,
+             int* __restrict__ invalid, const double* clock, double t_host, int do_sweep,
+             int do_repair) {
+  extern __shared__ double smem2[];
+  fused2_tile<TY>(c, fz, fz.tiles[blockIdx.x], f0, f1, Ug, ug, ustar, ustar_out, invalid, clock,
+                  t_host, do_sweep, do_repair, smem2);
+}
+
 // ---------------------------------------------------------------------------
 // Cooperative cut-link kernel: 16 lanes per link, 8 links per 128-thread block.
 // Lanes 0-5 gather d/dx of component `lane`, lanes 6-11 d/dy, lanes 12-15 the
@@ -378,23 +389,19 @@ __device__ __forceinline__ double lsq_sum(const int* __restrict__ node, const do
   return out;
 }
 
-__global__ void __launch_bounds__(128)
-    k_links2g(Ctx2 c, const double* __restrict__ fpost, double* __restrict__ fout,
-              const double* __restrict__ U, const double* __restrict__ u, const double* clock,
-              double t_host, double offset, int fused, const double* __restrict__ scratch,
-              const int32_t* __restrict__ partner, double* clock_next) {
-  __shared__ LinkShared2 sh[128 / kLG];
+// One cut link (processing slot `slot`) on the 16 lanes of a group; every
+// lane of the group calls it (only __syncwarp inside).
+__device__ __forceinline__ void link2_group(
+    const Ctx2& c, LinkShared2& S, int lane, int slot, const double* __restrict__ fpost,
+    double* __restrict__ fout, const double* __restrict__ U, const double* __restrict__ u,
+    const double* clock, double t_host, double offset, int fused,
+    const double* __restrict__ scratch, const int32_t* __restrict__ partner) {
   const cvlbm2d_problem& p = c.p;
   const Mat& m = c.m;
-  const int lane = threadIdx.x & (kLG - 1);
-  const int grp = threadIdx.x / kLG;
-  const int slot = blockIdx.x * (128 / kLG) + grp;
   const bool live = slot < p.n_links;
   const int ell = live ? (p.link_order ? p.link_order[slot] : slot) : 0;
-  LinkShared2& S = sh[grp];
   const int N = c.N, nx = p.nx, ny = p.ny, recon = p.recon;
   const double tmid = time_of(clock, t_host, offset);
-  if (clock_next && blockIdx.x == 0 && threadIdx.x == 0) *clock_next = clock[0] + p.dt;
 
   int i = 0, j = 0, qo = 0, qi = 2, kind = kDirichlet, mode = 0, n = 0, nu = 0;
   double eta = 0.5, xb = 0, yb = 0, nxb = 1, nyb = 0, bv0 = 0, bv1 = 0;
@@ -610,6 +617,20 @@ __global__ void __launch_bounds__(128)
     }
     fout[(size_t)(qi * 6 + a) * N + n] = val;
   }
+}
+
+__global__ void __launch_bounds__(128)
+    k_links2g(Ctx2 c, const double* __restrict__ fpost, double* __restrict__ fout,
+              const double* __restrict__ U, const double* __restrict__ u, const double* clock,
+              double t_host, double offset, int fused, const double* __restrict__ scratch,
+              const int32_t* __restrict__ partner, double* clock_next) {
+  __shared__ LinkShared2 sh[128 / kLG];
+  const int lane = threadIdx.x & (kLG - 1);
+  const int grp = threadIdx.x / kLG;
+  const int slot = blockIdx.x * (128 / kLG) + grp;
+  if (clock_next && blockIdx.x == 0 && threadIdx.x == 0) *clock_next = clock[0] + c.p.dt;
+  link2_group(c, sh[grp], lane, slot, fpost, fout, U, u, clock, t_host, offset, fused, scratch,
+              partner);
 }
 
 }  // namespace

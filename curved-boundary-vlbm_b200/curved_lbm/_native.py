@@ -113,6 +113,12 @@ EXPORTED = (
     "cvlbm_launch_count",
     "cvlbm2d_tile_variant",
     "cvlbm2d_run_static_scratch",
+    "cvlbm2d_batch_create",
+    "cvlbm2d_batch_run",
+    "cvlbm2d_batch_graph_create",
+    "cvlbm2d_batch_status",
+    "cvlbm2d_batch_launch_grid",
+    "cvlbm2d_batch_destroy",
 )
 
 
@@ -155,6 +161,14 @@ def load(require_cuda: bool = True):
         "cvlbm2d_tile_variant": (i32, [i32]),
         "cvlbm2d_run_static_scratch": (i32, [P2, F2, f64, i64, i32, pI]),
         "cvlbm_last_error": (C.c_char_p, []),
+        "cvlbm2d_batch_create": (i32, [i32, P2, F2, C.POINTER(i64), C.POINTER(f64), i32, i32,
+                                       C.POINTER(pI)]),
+        "cvlbm2d_batch_run": (i32, [pI, i32, i32, f64, f64, pI]),
+        "cvlbm2d_batch_graph_create": (i32, [pI, i32, i32, f64, f64, C.POINTER(pI)]),
+        "cvlbm2d_batch_status": (i32, [pI, C.POINTER(i32), C.POINTER(i32), C.POINTER(i64),
+                                       C.POINTER(f64), C.POINTER(f64), pI]),
+        "cvlbm2d_batch_launch_grid": (i32, [pI, C.POINTER(i32), C.POINTER(i32)]),
+        "cvlbm2d_batch_destroy": (None, [pI]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -98,3 +98,112 @@ def shell(n: int = 192):
                   local_displacement_boundary_weight=100.0, local_displacement_boundary_id=2,
                   local_compatibility_interval=1, local_compatibility_blend=0.5)
     return geom, mat, spec, solver
+
+
+# ---------------------------------------------------------------------------
+# Batched superellipse shells
+# ---------------------------------------------------------------------------
+SUPERELLIPSE_RAMP_TIME = 0.1
+
+
+def superellipse_params(n_inst: int = 256, seed: int = 20261203, n_min: int = 96,
+                        n_max: int = 512) -> list[dict]:
+    """Seeded instance table of the batched benchmark.
+
+    Lattice n ~ U{n_min..n_max} on [0, 1.4]^2 (the square [-0.7, 0.7]^2 centred
+    at (0.7, 0.7)); outer boundary a superellipse |xi/a|^p + |eta/b|^p = 1
+    rotated by theta, with p ~ U[2, 6], a, b ~ U[0.35, 0.5], theta ~ U[0, pi);
+    a clamped circular hole of radius r_in ~ U[0.1, 0.2]; outer normal
+    traction T ~ U[0.01, 0.06], ramped linearly over SUPERELLIPSE_RAMP_TIME.
+    """
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n_inst):
+        out.append({"n": int(rng.integers(n_min, n_max + 1)), "p": float(rng.uniform(2.0, 6.0)),
+                    "a": float(rng.uniform(0.35, 0.5)), "b": float(rng.uniform(0.35, 0.5)),
+                    "theta": float(rng.uniform(0.0, math.pi)),
+                    "r_in": float(rng.uniform(0.1, 0.2)),
+                    "traction": float(rng.uniform(0.01, 0.06))})
+    return out
+
+
+def superellipse_geometry(prm: dict):
+    """Level-set geometry of one batched instance (analytic normals)."""
+    from .two_d import curved_boundary_warp as c2
+
+    L, c = 1.4, 0.7
+    a, b, pw, ri = prm["a"], prm["b"], prm["p"], prm["r_in"]
+    ct, st = math.cos(prm["theta"]), math.sin(prm["theta"])
+    split = 0.5 * (ri + min(a, b))
+
+    def outer_phi(x, y):
+        dx, dy = x - c, y - c
+        xi, eta = ct * dx + st * dy, -st * dx + ct * dy
+        return (abs(xi) / a) ** pw + (abs(eta) / b) ** pw - 1.0
+
+    def phi(x, y):
+        return max(outer_phi(x, y), ri - math.hypot(x - c, y - c))
+
+    def normal(x, y):
+        dx, dy = x - c, y - c
+        r = math.hypot(dx, dy)
+        if r < split:
+            return -dx / max(r, 1e-30), -dy / max(r, 1e-30)
+        xi, eta = ct * dx + st * dy, -st * dx + ct * dy
+        gx = pw * math.copysign(abs(xi) ** (pw - 1.0), xi) / a ** pw
+        gy = pw * math.copysign(abs(eta) ** (pw - 1.0), eta) / b ** pw
+        return ct * gx - st * gy, st * gx + ct * gy
+
+    def boundary_id(x, y, _nx, _ny):
+        return 2 if math.hypot(x - c, y - c) < split else 1
+
+    n = prm["n"]
+    return c2.CurvedBoundaryGeometry.from_level_set(nx=n, ny=n, length_x=L, length_y=L, phi=phi,
+                                                   normal=normal, boundary_id=boundary_id,
+                                                   label="superellipse_batch")
+
+
+def superellipse_case(prm: dict):
+    """(material, boundary spec, solver kwargs) of one batched instance."""
+    from .two_d import curved_boundary_warp as c2
+
+    mat = c2.WarpHyperelasticMaterial(model="neo_hooke", lam=1.0, mu=1.0)
+    params = (prm["traction"], SUPERELLIPSE_RAMP_TIME)
+    spec = c2.CurvedBoundarySpec(kind="neumann", value_mode=105, params=params,
+                                 id_kinds={1: "neumann", 2: "dirichlet"},
+                                 id_value_modes={1: 105, 2: 0},
+                                 id_params={1: params, 2: ()})
+    _, _, _, kw = annulus(16)
+    return mat, spec, kw
+
+
+def superellipse_geometries(params: list[dict], processes: int | None = None) -> list:
+    """Build the instance geometries, in a spawned process pool when asked."""
+    if processes is None or processes <= 1 or len(params) <= 1:
+        return [superellipse_geometry(p) for p in params]
+    import multiprocessing as mp
+
+    with mp.get_context("spawn").Pool(processes) as pool:
+        return pool.map(superellipse_geometry, params, chunksize=1)
+
+
+def superellipse_solvers(params: list[dict], geometries: list, device=None) -> list:
+    """Solvers of the given instances, initialised to the undeformed state."""
+    from .two_d import curved_boundary_warp as c2
+
+    solvers = []
+    for prm, g in zip(params, geometries):
+        mat, spec, kw = superellipse_case(prm)
+        s = c2.WarpCurvedBoundaryLBM2D(g, material=mat, boundary=spec, device=device, **kw)
+        U, disp = annulus_initial_state(prm["n"])
+        s.initialize_from_numpy(U=U, displacement=disp, init_order=2)
+        solvers.append(s)
+    return solvers
+
+
+def superellipse_batch(n_inst: int = 256, seed: int = 20261203, device=None,
+                       processes: int | None = None, n_min: int = 96, n_max: int = 512):
+    """(instance table, solvers) of the batched benchmark."""
+    params = superellipse_params(n_inst, seed, n_min, n_max)
+    geoms = superellipse_geometries(params, processes)
+    return params, superellipse_solvers(params, geoms, device)

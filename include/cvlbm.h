@@ -158,6 +158,56 @@ int cvlbm2d_apply_boundary(const cvlbm2d_problem *p, cvlbm2d_fields *f, double t
  * Replaces refresh_current (two_d/curved_boundary_warp.py:4260-4291). */
 int cvlbm2d_refresh(const cvlbm2d_problem *p, cvlbm2d_fields *f, void *stream);
 
+/* ------------------------------------------------------------------------ */
+/* Batched D2Q4x6: many independent problems advanced together               */
+/* ------------------------------------------------------------------------ */
+
+/* A batch of independent 2-D problems (different geometries, load cases and
+ * lattice sizes) stepped together: per lattice step one persistent node
+ * launch walks the (instance, tile) work list of every instance, one
+ * persistent link launch walks all instances' cut links, and a tick advances
+ * each instance's device clock and step index.  Instances retire
+ * individually when their residual dt*|v|_2/|u|_2 over active nodes falls
+ * below a tolerance, or when their state becomes invalid (non-positive
+ * Jacobian).  The reference runs one solver per geometry
+ * (two_d/curved_boundary_warp.py:4163-4258 per instance); batching, the
+ * residual criterion and early retirement have no counterpart there. */
+typedef struct cvlbm2d_batch cvlbm2d_batch;
+
+/* problems[i]/fields[i] describe instance i exactly as for cvlbm2d_run, with
+ * the fused-step tables (tiles, need_fields, link_partner, lsq_node,
+ * link_scratch) built for `tile_variant`; step0[i]/time0[i] are its step
+ * index and time.  The batch keeps the field pointers: fields->f0 and
+ * fields->u_star hold the state when the instance has taken an even number of
+ * batch steps, f1 and u_next when odd (cvlbm2d_batch_status reports steps).
+ * grid_blocks = 0 sizes the persistent node grid to the SMs' resident
+ * capacity.  Allocates the work lists on the device. */
+int cvlbm2d_batch_create(int32_t n_inst, const cvlbm2d_problem *problems,
+                         const cvlbm2d_fields *fields, const int64_t *step0,
+                         const double *time0, int32_t tile_variant, int32_t grid_blocks,
+                         cvlbm2d_batch **out);
+
+/* Advance every active instance by up to nsteps lattice steps; after every
+ * check_every-th step, retire instances with time >= t_min and residual < tol
+ * (check_every = 0: no checks).  Asynchronous on `stream`. */
+int cvlbm2d_batch_run(cvlbm2d_batch *b, int32_t nsteps, int32_t check_every, double tol,
+                      double t_min, void *stream);
+
+/* cvlbm2d_batch_run captured into a replayable CUDA graph. */
+int cvlbm2d_batch_graph_create(cvlbm2d_batch *b, int32_t nsteps, int32_t check_every,
+                               double tol, double t_min, struct cvlbm_graph **out);
+
+/* Per-instance state (any pointer may be NULL): active flag, status (0
+ * running, 1 converged, -1 invalid), step index, time, last residual (-1 if
+ * never checked).  Synchronises `stream`. */
+int cvlbm2d_batch_status(cvlbm2d_batch *b, int32_t *active, int32_t *status, int64_t *steps,
+                         double *time, double *residual, void *stream);
+
+/* Persistent node grid size and number of (instance, tile) work items. */
+int cvlbm2d_batch_launch_grid(const cvlbm2d_batch *b, int32_t *node_grid, int32_t *n_work);
+
+void cvlbm2d_batch_destroy(cvlbm2d_batch *b);
+
 /* First Piola stress and Cauchy stress of the current U buffer at active
  * nodes (inactive nodes untouched).  The reference stores P and sigma in its
  * collision and repair kernels (two_d/curved_boundary_warp.py:1795-1803,
