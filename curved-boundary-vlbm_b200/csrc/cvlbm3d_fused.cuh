@@ -182,6 +182,9 @@ constexpr int kCN = 32;  // nodes per collide block (one per lane)
 
 struct CollideSmem3 {
   double f[kQ3][kC3][kCN];
+  double un[kQ3][3][kCN];  // swept u of the neighbour in direction q
+  double u0[3][kCN];       // swept u of the node
+  int nb[kQ3][kCN];        // neighbour in direction q, -1 if not active
   double S[kC3][kCN];
   double T[9][kCN];   // I + grad u
   double Po[9][kCN];  // P(F)
@@ -223,13 +226,22 @@ __global__ void __launch_bounds__(kQ3 * kCN, 4)
   const int n = n0 + lane;
   const bool live = n < N;
 
-  // 1: populations of direction `warp`
+  // 1: populations of direction `warp`, its neighbour and (for the repair)
+  // the neighbour's swept u
   double v[kC3];
   const int q = warp;
 #pragma unroll
   for (int a = 0; a < kC3; ++a) v[a] = live ? f0[(size_t)(q * kC3 + a) * N + n] : 0.0;
+  const int nq = live ? p.neighbor[(size_t)q * N + n] : -1;
+  if (do_repair) {
+#pragma unroll
+    for (int comp = 0; comp < 3; ++comp)
+      sm.un[q][comp][lane] = nq >= 0 ? u[(size_t)comp * N + nq] : 0.0;
+    if (warp < 3) sm.u0[warp][lane] = live ? u[(size_t)warp * N + n] : 0.0;
+  }
 #pragma unroll
   for (int a = 0; a < kC3; ++a) sm.f[q][a][lane] = v[a];
+  sm.nb[q][lane] = nq;
   __syncthreads();
 
   // 2: moments (12 x 32 sums) and I + grad u (9 x 32 targets)
@@ -248,12 +260,33 @@ __global__ void __launch_bounds__(kQ3 * kCN, 4)
     sm.S[a][l] = sacc;
   }
   if (do_repair) {
+    // derivative of the swept u along each axis, as du_axis3: centred with
+    // both neighbours, second-order one-sided with two on one side, first
+    // order with one, zero with none
     const double h[3] = {p.dx, p.dy, p.dz};
     for (int t = threadIdx.x; t < 9 * kCN; t += blockDim.x) {
       const int k = t / kCN, l = t % kCN, comp = k / 3, ax = k % 3;
-      const int nn = n0 + l;
+      const int pp = sm.nb[ax][l], pm = sm.nb[ax + 3][l];
+      const double* uc = u + (size_t)comp * N;
+      const double hh = h[ax];
       double g = 0.0;
-      if (nn < N) g = du_axis3(u + (size_t)comp * N, p.neighbor, N, nn, ax, ax + 3, h[ax]);
+      if (n0 + l < N) {
+        if (pp >= 0 && pm >= 0) {
+          g = (sm.un[ax][comp][l] - sm.un[ax + 3][comp][l]) / (2.0 * hh);
+        } else if (pp >= 0) {
+          const int pp2 = p.neighbor[(size_t)ax * N + pp];
+          if (pp2 >= 0)
+            g = (-3.0 * sm.u0[comp][l] + 4.0 * sm.un[ax][comp][l] - uc[pp2]) / (2.0 * hh);
+          else
+            g = (sm.un[ax][comp][l] - sm.u0[comp][l]) / hh;
+        } else if (pm >= 0) {
+          const int pm2 = p.neighbor[(size_t)(ax + 3) * N + pm];
+          if (pm2 >= 0)
+            g = (3.0 * sm.u0[comp][l] - 4.0 * sm.un[ax + 3][comp][l] + uc[pm2]) / (2.0 * hh);
+          else
+            g = (sm.u0[comp][l] - sm.un[ax + 3][comp][l]) / hh;
+        }
+      }
       sm.T[k][l] = comp == ax ? 1.0 + g : g;
     }
   }
@@ -308,7 +341,6 @@ __global__ void __launch_bounds__(kQ3 * kCN, 4)
   const double sw = p.dt * (2.0 - om) * (1.0 / 12.0);
   const double ff = 0.5 / p.c;
   const bool repaired = sm.rep[lane] != 0;
-  const int nq = p.neighbor[(size_t)q * N + n];
   int ell = -1;
   if (nq < 0) {
     for (int k = p.node_link_start[n]; k < p.node_link_start[n + 1]; ++k) {
@@ -343,41 +375,50 @@ constexpr int kGatherLanes = 16;  // lanes per link in the gather (12 components
 
 // Value and gradients of the 12 components at a link from its <= 64
 // characteristic samples, in slot order (_sparse_characteristic_gather,
-// :2675-2700).  The 12 lanes of a link read one 96-byte U_need row per sample.
+// :2675-2700).  A block takes 8 consecutive links: their sample slots and
+// weights are staged in shared memory with coalesced loads, then the 12
+// lanes of a link read one 96-byte U_need row per sample, 16 samples per
+// batch of independent loads.
+constexpr int kGatherLinks = 128 / kGatherLanes;
+
 __global__ void __launch_bounds__(128)
     k3_link_gather(Ctx3 c, Fused3 fz, double* __restrict__ char_state) {
+  __shared__ int s_slot[kGatherLinks][kChar];
+  __shared__ double s_w[4][kChar][kGatherLinks];
   const cvlbm3d_problem& p = c.p;
   const int L = p.n_links;
+  const int ell0 = blockIdx.x * kGatherLinks;
+  for (int t = threadIdx.x; t < kChar * kGatherLinks; t += blockDim.x) {
+    const int mm = t / kGatherLinks, g = t % kGatherLinks;
+    const int ell = ell0 + g;
+    s_slot[g][mm] = ell < L ? fz.char_slot[(size_t)mm * L + ell] : -1;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      s_w[k][mm][g] = ell < L ? p.char_w[((size_t)k * kChar + mm) * L + ell] : 0.0;
+  }
+  __syncthreads();
   const int a = threadIdx.x % kGatherLanes;
-  const int ell = blockIdx.x * (128 / kGatherLanes) + threadIdx.x / kGatherLanes;
+  const int g = threadIdx.x / kGatherLanes;
+  const int ell = ell0 + g;
   if (ell >= L || a >= kC3 || p.char_idx[ell] < 0) return;
   double v0 = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
-  // samples in chunks of 8: every load of a chunk is issued before its sums,
-  // which keep the slot order
-  constexpr int kChunk = 8;
+  constexpr int kChunk = 16;
 #pragma unroll 1
   for (int m0 = 0; m0 < kChar; m0 += kChunk) {
-    int q[kChunk];
-    double uv[kChunk], w0[kChunk], w1[kChunk], w2[kChunk], w3[kChunk];
-#pragma unroll
-    for (int k = 0; k < kChunk; ++k) q[k] = fz.char_slot[(size_t)(m0 + k) * L + ell];
+    double uv[kChunk];
 #pragma unroll
     for (int k = 0; k < kChunk; ++k) {
-      const size_t mm = (size_t)(m0 + k);
-      w0[k] = p.char_w[((size_t)0 * kChar + mm) * L + ell];
-      w1[k] = p.char_w[((size_t)1 * kChar + mm) * L + ell];
-      w2[k] = p.char_w[((size_t)2 * kChar + mm) * L + ell];
-      w3[k] = p.char_w[((size_t)3 * kChar + mm) * L + ell];
+      const int q = s_slot[g][m0 + k];
+      uv[k] = q >= 0 ? fz.Uneed[(size_t)q * kC3 + a] : 0.0;
     }
 #pragma unroll
-    for (int k = 0; k < kChunk; ++k) uv[k] = q[k] >= 0 ? fz.Uneed[(size_t)q[k] * kC3 + a] : 0.0;
-#pragma unroll
     for (int k = 0; k < kChunk; ++k) {
-      if (q[k] >= 0) {
-        v0 += w0[k] * uv[k];
-        gx += w1[k] * uv[k];
-        gy += w2[k] * uv[k];
-        gz += w3[k] * uv[k];
+      const int mm = m0 + k;
+      if (s_slot[g][mm] >= 0) {
+        v0 += s_w[0][mm][g] * uv[k];
+        gx += s_w[1][mm][g] * uv[k];
+        gy += s_w[2][mm][g] * uv[k];
+        gz += s_w[3][mm][g] * uv[k];
       }
     }
   }
