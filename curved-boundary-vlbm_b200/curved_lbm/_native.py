@@ -119,6 +119,7 @@ EXPORTED = (
     "cvlbm2d_batch_status",
     "cvlbm2d_batch_launch_grid",
     "cvlbm2d_batch_destroy",
+    "cvlbm_gemm_bf16",
 )
 
 
@@ -169,6 +170,7 @@ def load(require_cuda: bool = True):
                                        C.POINTER(f64), C.POINTER(f64), pI]),
         "cvlbm2d_batch_launch_grid": (i32, [pI, C.POINTER(i32), C.POINTER(i32)]),
         "cvlbm2d_batch_destroy": (None, [pI]),
+        "cvlbm_gemm_bf16": (i32, [pI, pI, pI, i32, i32, i32, i32, i32, i32, i32, pI, pI]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
