@@ -162,7 +162,7 @@ def batch_bench(args, dev):
                    "tile_variant": batch.tile_variant,
                    "autotune_ms_per_step": {str(k): round(v, 4) for k, v in tuned.items()},
                    "persistent_node_grid": ng, "work_items": nw,
-                   "residual": "dt*|v|_2/|u|_2 over active nodes, checked every 100 steps "
+                   "residual": "|u-u_prev|_2/(100 |u|_2) over active nodes, checked every 100 steps "
                                f"after t >= {workloads.SUPERELLIPSE_RAMP_TIME}",
                    "tol": args.tol, "host_setup_s": round(setup_s, 1),
                    "l2": "working set (%.1f GB of populations) far above L2"

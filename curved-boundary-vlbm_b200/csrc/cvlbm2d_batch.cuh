@@ -9,11 +9,16 @@
 //   k_batch_links2   persistent: walks (instance, 8-link group) pairs
 //   k_batch_tick2    advances each active instance's clock and step counter
 // Every `check_every` steps the node kernel also stores U and u of every
-// active node, k_batch_partial2 reduces v.v and u.u per (instance, tile) in a
-// fixed order and k_batch_residual2 retires instances whose residual
-// dt*|v|_2/|u|_2 fell below the tolerance (after a minimum time, e.g. the end
-// of a load ramp).  Retired instances' work items return at once.  The whole
-// step sequence is captured in one CUDA graph (cvlbm2d_batch_graph_create).
+// active node, k_batch_partial2 reduces |u - u_prev|^2 and |u|^2 per
+// (instance, tile) in a fixed order (u_prev = u at the previous check) and
+// k_batch_residual2 retires instances whose residual
+// |u - u_prev|_2 / (check_every * |u|_2), the relative displacement change per
+// step, fell below the tolerance (after a minimum time, e.g. the end of a load
+// ramp).  The velocity moment is no measure of convergence here: with the
+// displacement sweep the damped steady state keeps a small constant v whose
+// increments the sweep cancels every step.  Retired instances' work items
+// return at once.  The whole step sequence is captured in one CUDA graph
+// (cvlbm2d_batch_graph_create).
 //
 // Each instance keeps its own population and u* ping-pong; the buffer that
 // holds the current state is selected by the parity of the steps the instance
@@ -33,6 +38,7 @@ struct Inst2 {
   double* us[2];  // u* buffers
   double* U;
   double* u;
+  double* u_prev;  // [2*N] u at the previous residual check (batch-owned)
   int* invalid;
 };
 
@@ -40,9 +46,11 @@ struct InstState2 {
   long long step;       // step index of the instance (interval tests)
   long long base;       // step index at batch creation (buffer parity)
   double clock;         // device time
-  double residual;      // last residual, -1 before the first check
+  double residual;      // last residual, -1 before the second check
   int active;           // 1 while stepping
   int status;           // 0 running, 1 converged, -1 invalid state
+  int checks;           // residual checks done
+  int pad;
 };
 
 __device__ __forceinline__ int parity_of(const InstState2& s) { return (int)((s.step - s.base) & 1); }
@@ -96,8 +104,9 @@ __global__ void k_batch_tick2(const Inst2* __restrict__ inst, InstState2* __rest
   }
 }
 
-// Per (instance, tile): sum of |v|^2 and |u|^2 over the tile's active nodes,
-// reduced in a fixed order (deterministic for a given tile height).
+// Per (instance, tile): sum of |u - u_prev|^2 and |u|^2 over the tile's
+// active nodes, reduced in a fixed order (deterministic for a given tile
+// height); u_prev is then replaced by u.
 template <int TY>
 __global__ void __launch_bounds__(kTX * TY)
     k_batch_partial2(const Inst2* __restrict__ inst, const InstState2* __restrict__ st,
@@ -114,10 +123,12 @@ __global__ void __launch_bounds__(kTX * TY)
     double v2 = 0.0, u2 = 0.0;
     if (st[wk.x].active && i < p.nx && j < p.ny && p.active[i * p.ny + j]) {
       const int n = i * p.ny + j;
-      const double v0 = I.U[n], v1 = I.U[(size_t)N + n];
       const double u0 = I.u[n], u1 = I.u[(size_t)N + n];
-      v2 = v0 * v0 + v1 * v1;
+      const double d0 = u0 - I.u_prev[n], d1 = u1 - I.u_prev[(size_t)N + n];
+      v2 = d0 * d0 + d1 * d1;
       u2 = u0 * u0 + u1 * u1;
+      I.u_prev[n] = u0;
+      I.u_prev[(size_t)N + n] = u1;
     }
     sv[threadIdx.x] = v2;
     su[threadIdx.x] = u2;
@@ -136,7 +147,7 @@ __global__ void __launch_bounds__(kTX * TY)
 __global__ void k_batch_residual2(const Inst2* __restrict__ inst, InstState2* __restrict__ st,
                                   const int* __restrict__ work_start,
                                   const double2* __restrict__ partial, int n, double tol,
-                                  double t_min) {
+                                  double t_min, int interval) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || !st[i].active) return;
   double sv = 0.0, su = 0.0;
@@ -144,8 +155,9 @@ __global__ void k_batch_residual2(const Inst2* __restrict__ inst, InstState2* __
     sv += partial[w].x;
     su += partial[w].y;
   }
-  const double dt = inst[i].c.p.dt;
-  const double r = su > 0.0 ? dt * sqrt(sv) / sqrt(su) : (sv > 0.0 ? 1.0 : 0.0);
+  const double r = su > 0.0 ? sqrt(sv) / ((double)interval * sqrt(su)) : (sv > 0.0 ? 1.0 : 0.0);
+  st[i].checks = st[i].checks + 1;
+  if (st[i].checks < 2) return;  // no earlier displacement to compare with
   st[i].residual = r;
   if (st[i].clock >= t_min && r < tol) {
     st[i].active = 0;
@@ -186,6 +198,7 @@ struct cvlbm2d_batch {
   int2* d_work = nullptr;
   int2* d_lwork = nullptr;
   int* d_work_start = nullptr;
+  double* d_uprev = nullptr;
   double2* d_partial = nullptr;
 };
 
@@ -199,6 +212,7 @@ void batch_free(cvlbm2d_batch* b) {
   cudaFree(b->d_lwork);
   cudaFree(b->d_work_start);
   cudaFree(b->d_partial);
+  cudaFree(b->d_uprev);
   delete b;
 }
 
@@ -253,7 +267,7 @@ extern "C" int cvlbm2d_batch_create(int32_t n_inst, const cvlbm2d_problem* probl
     hi[i].U = f->U;
     hi[i].u = f->u;
     hi[i].invalid = f->invalid;
-    hs[i] = InstState2{step0[i], step0[i], time0[i], -1.0, 1, 0};
+    hs[i] = InstState2{step0[i], step0[i], time0[i], -1.0, 1, 0, 0, 0};
     tiles.resize(p->n_tiles);
     if (p->n_tiles > 0 &&
         cudaMemcpy(tiles.data(), p->tiles, sizeof(int) * p->n_tiles, cudaMemcpyDeviceToHost) !=
@@ -265,6 +279,20 @@ extern "C" int cvlbm2d_batch_create(int32_t n_inst, const cvlbm2d_problem* probl
   }
   work_start[n_inst] = (int)work.size();
   cvlbm2d_batch* b = new cvlbm2d_batch();
+  size_t uprev_total = 0;
+  for (int i = 0; i < n_inst; ++i) uprev_total += 2 * (size_t)hi[i].c.N;
+  if (cudaMalloc(&b->d_uprev, sizeof(double) * uprev_total) != cudaSuccess ||
+      cudaMemset(b->d_uprev, 0, sizeof(double) * uprev_total) != cudaSuccess) {
+    batch_free(b);
+    return fail(CVLBM_ERR_CUDA, "cvlbm2d_batch_create: residual buffer allocation failed");
+  }
+  {
+    size_t off = 0;
+    for (int i = 0; i < n_inst; ++i) {
+      hi[i].u_prev = b->d_uprev + off;
+      off += 2 * (size_t)hi[i].c.N;
+    }
+  }
   b->n_inst = n_inst;
   b->variant = tile_variant;
   b->n_work = (int)work.size();
@@ -321,7 +349,8 @@ extern "C" int cvlbm2d_batch_run(cvlbm2d_batch* b, int32_t nsteps, int32_t check
                                                    b->d_partial);
       cv::count_launches(1);
       k_batch_residual2<<<blocks(b->n_inst, 128), 128, 0, s>>>(
-          b->d_inst, b->d_state, b->d_work_start, b->d_partial, b->n_inst, tol, t_min);
+          b->d_inst, b->d_state, b->d_work_start, b->d_partial, b->n_inst, tol, t_min,
+          check_every);
       cv::count_launches(1);
     }
   }

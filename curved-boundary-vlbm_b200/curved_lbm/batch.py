@@ -7,12 +7,13 @@ every instance (see ``cvlbm2d_batch_create`` in ``include/cvlbm.h``), the step
 sequence is replayed from a CUDA graph, and each instance retires on its own
 once its residual
 
-    r = dt * ||v||_2 / ||u||_2      (sums over active nodes)
+    r = ||u - u_prev||_2 / (check_every * ||u||_2)   (sums over active nodes)
 
-- the relative displacement increment per step - falls below a tolerance
-after a minimum time (the end of its load ramp).  The reference runs one
-solver object per geometry and has only an ``rms_v`` steady check in its
-case scripts; batching and this residual criterion are additions.
+- the relative displacement change per step since the previous check - falls
+below a tolerance after a minimum time (the end of its load ramp).  The
+reference runs one solver object per geometry and has only an ``rms_v``
+steady check in its case scripts; batching and this residual criterion are
+additions.
 
 Every instance follows exactly the arithmetic of its solo ``run``: a batched
 instance's populations equal the solo solver's after the same number of

@@ -167,9 +167,10 @@ int cvlbm2d_refresh(const cvlbm2d_problem *p, cvlbm2d_fields *f, void *stream);
  * launch walks the (instance, tile) work list of every instance, one
  * persistent link launch walks all instances' cut links, and a tick advances
  * each instance's device clock and step index.  Instances retire
- * individually when their residual dt*|v|_2/|u|_2 over active nodes falls
- * below a tolerance, or when their state becomes invalid (non-positive
- * Jacobian).  The reference runs one solver per geometry
+ * individually when their residual |u - u_prev|_2 / (check_every |u|_2) over
+ * active nodes (the relative displacement change per step since the previous
+ * check) falls below a tolerance, or when their state becomes invalid
+ * (non-positive Jacobian).  The reference runs one solver per geometry
  * (two_d/curved_boundary_warp.py:4163-4258 per instance); batching, the
  * residual criterion and early retirement have no counterpart there. */
 typedef struct cvlbm2d_batch cvlbm2d_batch;
@@ -181,7 +182,8 @@ typedef struct cvlbm2d_batch cvlbm2d_batch;
  * fields->u_star hold the state when the instance has taken an even number of
  * batch steps, f1 and u_next when odd (cvlbm2d_batch_status reports steps).
  * grid_blocks = 0 sizes the persistent node grid to the SMs' resident
- * capacity.  Allocates the work lists on the device. */
+ * capacity.  Allocates the work lists and a previous-displacement buffer
+ * (2 doubles per lattice node) on the device. */
 int cvlbm2d_batch_create(int32_t n_inst, const cvlbm2d_problem *problems,
                          const cvlbm2d_fields *fields, const int64_t *step0,
                          const double *time0, int32_t tile_variant, int32_t grid_blocks,
@@ -198,8 +200,8 @@ int cvlbm2d_batch_graph_create(cvlbm2d_batch *b, int32_t nsteps, int32_t check_e
                                double tol, double t_min, struct cvlbm_graph **out);
 
 /* Per-instance state (any pointer may be NULL): active flag, status (0
- * running, 1 converged, -1 invalid), step index, time, last residual (-1 if
- * never checked).  Synchronises `stream`. */
+ * running, 1 converged, -1 invalid), step index, time, last residual (-1
+ * before the second check).  Synchronises `stream`. */
 int cvlbm2d_batch_status(cvlbm2d_batch *b, int32_t *active, int32_t *status, int64_t *steps,
                          double *time, double *residual, void *stream);
 
