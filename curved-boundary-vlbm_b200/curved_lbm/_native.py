@@ -120,6 +120,15 @@ EXPORTED = (
     "cvlbm2d_batch_launch_grid",
     "cvlbm2d_batch_destroy",
     "cvlbm_gemm_bf16",
+    "cvlbm_fno_pointwise_fwd",
+    "cvlbm_fno_gelu_bwd",
+    "cvlbm_fno_pointwise_bwd",
+    "cvlbm_fno_pointwise_scratch",
+    "cvlbm_fno_spec_mix_fwd",
+    "cvlbm_fno_spec_mix_bwd",
+    "cvlbm_fno_to_bf16",
+    "cvlbm_fno_mse",
+    "cvlbm_fno_adam",
 )
 
 
@@ -171,6 +180,17 @@ def load(require_cuda: bool = True):
         "cvlbm2d_batch_launch_grid": (i32, [pI, C.POINTER(i32), C.POINTER(i32)]),
         "cvlbm2d_batch_destroy": (None, [pI]),
         "cvlbm_gemm_bf16": (i32, [pI, pI, pI, i32, i32, i32, i32, i32, i32, i32, pI, pI]),
+        "cvlbm_fno_pointwise_fwd": (i32, [i32, i32, i32, i32, pI, pI, pI, pI, i32, pI, pI, pI]),
+        "cvlbm_fno_gelu_bwd": (i32, [i64, pI, pI, pI, pI]),
+        "cvlbm_fno_pointwise_bwd": (i32, [i32, i32, i32, i32, pI, pI, pI, pI, i32, pI, pI, pI,
+                                          pI]),
+        "cvlbm_fno_pointwise_scratch": (i64, [i32, i32, i32, i32]),
+        "cvlbm_fno_spec_mix_fwd": (i32, [i32, i32, i32, pI, pI, pI, pI]),
+        "cvlbm_fno_spec_mix_bwd": (i32, [i32, i32, i32, pI, pI, pI, pI, pI, pI]),
+        "cvlbm_fno_to_bf16": (i32, [i64, pI, pI, pI]),
+        "cvlbm_fno_mse": (i32, [i32, i32, i32, pI, pI, pI, pI, C.c_float, pI, pI, i32, pI]),
+        "cvlbm_fno_adam": (i32, [i64, pI, pI, pI, pI, C.c_float, C.c_float, C.c_float,
+                                 C.c_float, pI]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

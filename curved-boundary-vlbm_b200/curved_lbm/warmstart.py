@@ -1,0 +1,475 @@
+"""Learned warm start of the 3-D solver: a Fourier neural operator (FNO).
+
+The surrogate maps a tube case (level set of the geometry and the end load:
+stretch and twist) to the equilibrium displacement u and deformation
+gradient F on the solver lattice.  The solver then starts from that state
+(populations at equilibrium of U = (0, F), u* from u; the end displacement
+applied at once) instead of the undeformed state with a load ramp, and the
+plain damped relaxation converges from there; a prediction with a
+non-positive Jacobian anywhere falls back to the cold start.  The reference
+has no learned component; this module is an addition.
+
+Network (channel-major activations x[b][c][g], g = lattice node):
+
+    h0 = W0 x + b0                                  (lift, 8 -> 32 channels)
+    h_{l+1} = act(W_l h_l + b_l + S_l(h_l)),  l = 0..3  (act = GELU, none last)
+    y = Wp h_4 + bp                                 (project, 32 -> 12)
+    S_l(h) = (h Phi) R_l Phi^T    (per retained mode k: 32 x 32 channel mix)
+
+Phi is a truncated real Fourier basis on the lattice (cos / sin of the
+lowest modes along each axis, orthonormal, padded with zero columns to a
+multiple of 64).  The two spectral transforms of every layer, forward and
+backward, run on the tensor cores (cvlbm_gemm_bf16: bf16 operands, fp32
+accumulation); channel mixing, activations, the loss and Adam are this
+library's CUDA-core kernels.  Weights are fp32.
+"""
+
+from __future__ import annotations
+
+import math
+import time as _time
+
+import numpy as np
+
+from . import _native
+
+C_IN = 8
+C_OUT = 12
+
+
+def axis_basis(n: int, m: int) -> np.ndarray:
+    """n x (2m-1) orthonormal real Fourier columns at cell centres."""
+    x = (np.arange(n) + 0.5) / n
+    cols = [np.full(n, 1.0 / math.sqrt(n))]
+    for k in range(1, m):
+        cols.append(math.sqrt(2.0 / n) * np.cos(2 * math.pi * k * x))
+        cols.append(math.sqrt(2.0 / n) * np.sin(2 * math.pi * k * x))
+    return np.stack(cols, axis=1)
+
+
+def fourier_basis(shape, modes) -> np.ndarray:
+    """G x M basis of the (nx, ny, nz) lattice (k fastest), M padded to 64."""
+    bx, by, bz = (axis_basis(n, m) for n, m in zip(shape, modes))
+    phi = np.einsum("ia,jb,kc->ijkabc", bx, by, bz).reshape(int(np.prod(shape)), -1)
+    m = phi.shape[1]
+    mp = -(-m // 64) * 64
+    return np.pad(phi, ((0, 0), (0, mp - m)))
+
+
+class FNO:
+    """Fourier neural operator with native forward/backward (see module doc)."""
+
+    def __init__(self, shape, *, modes=(4, 4, 8), width: int = 32, layers: int = 4,
+                 batch: int = 4, device="cuda:0", seed: int = 0):
+        import torch
+
+        self.shape = tuple(int(s) for s in shape)
+        self.G = int(np.prod(self.shape))
+        if self.G % 64:
+            raise ValueError("lattice node count must be a multiple of 64")
+        if (batch * width) % 128:
+            raise ValueError("batch * width must be a multiple of 128")
+        self.C, self.L, self.B = int(width), int(layers), int(batch)
+        self.dev = torch.device(device)
+        self._lib = _native.load()
+        phi = fourier_basis(self.shape, modes)
+        self.M = phi.shape[1]
+        bf = torch.bfloat16
+        self.phi = torch.as_tensor(phi, dtype=torch.float32, device=self.dev).to(bf).contiguous()
+        self.phiT = self.phi.t().contiguous()
+        rng = np.random.default_rng(seed)
+        C = self.C
+
+        def w(o, i):
+            return rng.normal(0.0, 1.0 / math.sqrt(i), (o, i))
+
+        p = {"W0": w(C, C_IN), "b0": np.zeros(C)}
+        for l in range(self.L):
+            p[f"W{l + 1}"] = w(C, C)
+            p[f"b{l + 1}"] = np.zeros(C)
+            p[f"R{l + 1}"] = rng.normal(0.0, 1.0 / C, (self.M, C, C))
+        p["Wp"] = w(C_OUT, C)
+        p["bp"] = np.zeros(C_OUT)
+        self.params = {k: torch.as_tensor(v, dtype=torch.float32, device=self.dev).contiguous()
+                       for k, v in p.items()}
+        self.grads = {k: torch.zeros_like(v) for k, v in self.params.items()}
+        self._adam = None
+        self._err = torch.zeros(1, dtype=torch.int32, device=self.dev)
+        n_scr = max(int(self._lib.cvlbm_fno_pointwise_scratch(self.B, self.G, ci, co))
+                    for ci, co in ((C_IN, C), (C, C), (C, C_OUT)))
+        self._scratch = torch.empty(n_scr, dtype=torch.float32, device=self.dev)
+
+    # -- native plumbing --------------------------------------------------------
+    def _s(self):
+        return _native.stream_ptr(self.dev)
+
+    def _gemm(self, A, Bm, C, accumulate=0):
+        M, K = A.shape
+        N = Bm.shape[0]
+        _native.check(self._lib.cvlbm_gemm_bf16(_native.ptr(A), _native.ptr(Bm), _native.ptr(C),
+                                                M, N, K, A.stride(0), Bm.stride(0), C.stride(0),
+                                                accumulate, _native.ptr(self._err), self._s()),
+                      "cvlbm_gemm_bf16")
+
+    def _bf16(self, x):
+        import torch
+
+        out = torch.empty(x.shape, dtype=torch.bfloat16, device=self.dev)
+        _native.check(self._lib.cvlbm_fno_to_bf16(x.numel(), _native.ptr(x), _native.ptr(out),
+                                                  self._s()), "cvlbm_fno_to_bf16")
+        return out
+
+    def _pw(self, x, W, b, s=None, act=0, keep_z=False):
+        import torch
+
+        Cout, Cin = W.shape
+        y = torch.empty((self.B, Cout, self.G), dtype=torch.float32, device=self.dev)
+        z = torch.empty_like(y) if keep_z else None
+        _native.check(self._lib.cvlbm_fno_pointwise_fwd(
+            self.B, self.G, Cin, Cout, _native.ptr(x), _native.ptr(W), _native.ptr(b),
+            _native.ptr(s), act, _native.ptr(z), _native.ptr(y), self._s()),
+            "cvlbm_fno_pointwise_fwd")
+        return y, z
+
+    def _pw_bwd(self, dz, x, W, dW, db, dx=None, accumulate=0):
+        Cout, Cin = W.shape
+        _native.check(self._lib.cvlbm_fno_pointwise_bwd(
+            self.B, self.G, Cin, Cout, _native.ptr(dz), _native.ptr(x), _native.ptr(W),
+            _native.ptr(dx), accumulate, _native.ptr(dW), _native.ptr(db),
+            _native.ptr(self._scratch), self._s()), "cvlbm_fno_pointwise_bwd")
+
+    # -- forward / backward ------------------------------------------------------
+    def forward(self, x):
+        """x: [B, 8, G] fp32 -> y: [B, 12, G]; keeps what backward needs."""
+        import torch
+
+        P, B, C, G, M = self.params, self.B, self.C, self.G, self.M
+        cache = {"x": x}
+        h, _ = self._pw(x, P["W0"], P["b0"])
+        for l in range(1, self.L + 1):
+            hb = self._bf16(h).view(B * C, G)
+            a = torch.empty((B * C, M), dtype=torch.float32, device=self.dev)
+            self._gemm(hb, self.phiT, a)  # a = h Phi
+            bh = torch.empty((B * C, M), dtype=torch.bfloat16, device=self.dev)
+            _native.check(self._lib.cvlbm_fno_spec_mix_fwd(B, C, M, _native.ptr(a),
+                                                           _native.ptr(P[f"R{l}"]),
+                                                           _native.ptr(bh), self._s()),
+                          "cvlbm_fno_spec_mix_fwd")
+            s = torch.empty((B * C, G), dtype=torch.float32, device=self.dev)
+            self._gemm(bh, self.phi, s)  # s = bh Phi^T
+            act = 1 if l < self.L else 0
+            hn, z = self._pw(h, P[f"W{l}"], P[f"b{l}"], s=s, act=act, keep_z=True)
+            cache[l] = (h, a, z)
+            h = hn
+        cache["h"] = h
+        y, _ = self._pw(h, P["Wp"], P["bp"])
+        self._cache = cache
+        return y
+
+    def backward(self, dy):
+        """Gradients of all parameters from dL/dy (into self.grads)."""
+        import torch
+
+        P, Gr, B, C, G, M = self.params, self.grads, self.B, self.C, self.G, self.M
+        cache = self._cache
+        dh = torch.empty((B, C, G), dtype=torch.float32, device=self.dev)
+        self._pw_bwd(dy, cache["h"], P["Wp"], Gr["Wp"], Gr["bp"], dx=dh)
+        for l in range(self.L, 0, -1):
+            h, a, z = cache[l]
+            if l < self.L:
+                dz = torch.empty_like(dh)
+                _native.check(self._lib.cvlbm_fno_gelu_bwd(dh.numel(), _native.ptr(z),
+                                                           _native.ptr(dh), _native.ptr(dz),
+                                                           self._s()), "cvlbm_fno_gelu_bwd")
+            else:
+                dz = dh
+            dprev = torch.empty((B, C, G), dtype=torch.float32, device=self.dev)
+            self._pw_bwd(dz, h, P[f"W{l}"], Gr[f"W{l}"], Gr[f"b{l}"], dx=dprev)
+            dzb = self._bf16(dz).view(B * C, G)
+            dbh = torch.empty((B * C, M), dtype=torch.float32, device=self.dev)
+            self._gemm(dzb, self.phiT, dbh)  # dbh = dz Phi
+            da = torch.empty((B * C, M), dtype=torch.bfloat16, device=self.dev)
+            _native.check(self._lib.cvlbm_fno_spec_mix_bwd(
+                B, C, M, _native.ptr(a), _native.ptr(dbh), _native.ptr(P[f"R{l}"]),
+                _native.ptr(da), _native.ptr(Gr[f"R{l}"]), self._s()), "cvlbm_fno_spec_mix_bwd")
+            self._gemm(da, self.phi, dprev.view(B * C, G), accumulate=1)  # += da Phi^T
+            dh = dprev
+        self._pw_bwd(dh, cache["x"], P["W0"], Gr["W0"], Gr["b0"])
+        return Gr
+
+    def loss_grad(self, y, t, mask, wch):
+        """Masked weighted MSE and dL/dy (native)."""
+        import torch
+
+        n_parts = 256
+        dy = torch.empty_like(y)
+        part = torch.empty(n_parts, dtype=torch.float32, device=self.dev)
+        cnt = float(mask.sum().item()) * C_OUT
+        _native.check(self._lib.cvlbm_fno_mse(self.B, C_OUT, self.G, _native.ptr(y),
+                                              _native.ptr(t), _native.ptr(mask),
+                                              _native.ptr(wch), 1.0 / max(cnt, 1.0),
+                                              _native.ptr(dy), _native.ptr(part), n_parts,
+                                              self._s()), "cvlbm_fno_mse")
+        return part, dy
+
+    def adam_step(self, lr=1e-3, b1=0.9, b2=0.999, eps=1e-8):
+        import torch
+
+        if self._adam is None:
+            self._adam = {"t": 0, "m": {k: torch.zeros_like(v) for k, v in self.params.items()},
+                          "v": {k: torch.zeros_like(v) for k, v in self.params.items()}}
+        st = self._adam
+        st["t"] += 1
+        lr_t = lr * math.sqrt(1 - b2 ** st["t"]) / (1 - b1 ** st["t"])
+        for k, p in self.params.items():
+            _native.check(self._lib.cvlbm_fno_adam(p.numel(), _native.ptr(p),
+                                                   _native.ptr(self.grads[k]),
+                                                   _native.ptr(st["m"][k]),
+                                                   _native.ptr(st["v"][k]), lr_t, b1, b2, eps,
+                                                   self._s()), "cvlbm_fno_adam")
+
+    def gemm_ok(self) -> bool:
+        return int(self._err.item()) == 0
+
+
+# ---------------------------------------------------------------------------
+# Tube data: features, solver equilibria, warm and cold starts
+# ---------------------------------------------------------------------------
+def tube_features(prm: dict, nxy: int) -> tuple[np.ndarray, np.ndarray]:
+    """([8, G] input channels, [G] material mask) of one tube case."""
+    from . import workloads
+
+    nx, ny, nz, dx = workloads.tube_lattice(nxy)
+    cx, cy = 0.5 * nx * dx, 0.5 * ny * dx
+    z0 = 0.5 * (nz * dx - workloads.TUBE_LENGTH)
+    x = (np.arange(nx) + 0.5) * dx
+    y = (np.arange(ny) + 0.5) * dx
+    z = (np.arange(nz) + 0.5) * dx
+    X, Y, Z = np.meshgrid(x, y, z, indexing="ij")
+    r = np.sqrt((X - cx) ** 2 + (Y - cy) ** 2)
+    phi = np.maximum.reduce((r - prm["r_out"], prm["r_in"] - r, z0 - Z,
+                             Z - z0 - workloads.TUBE_LENGTH))
+    mask = (phi <= 0.0).astype(np.float32)
+    zeta = np.clip((Z - z0) / workloads.TUBE_LENGTH, 0.0, 1.0)
+    f = np.stack([mask, np.clip(phi / 0.3, -1, 1), (X - cx) / 0.9, (Y - cy) / 0.9,
+                  2 * zeta - 1, mask * zeta * (prm["stretch"] - 1.0) / 0.3,
+                  mask * zeta * prm["twist"] / (math.pi / 4), np.ones_like(X)])
+    return f.reshape(C_IN, -1).astype(np.float32), mask.reshape(-1)
+
+
+def solver_targets(solver) -> np.ndarray:
+    """[12, G]: u (3) and F - I (9) on the lattice, zero outside the material."""
+    ai, aj, ak = solver.active_i, solver.active_j, solver.active_k
+    nx, ny, nz = solver.nx, solver.ny, solver.nz
+    u = solver.active_displacement()
+    U = solver.active_system_state()
+    F = U[3:12].copy()
+    F[0] -= 1.0
+    F[4] -= 1.0
+    F[8] -= 1.0
+    out = np.zeros((12, nx, ny, nz))
+    out[:3, ai, aj, ak] = u
+    out[3:, ai, aj, ak] = F
+    return out.reshape(12, -1)
+
+
+def make_tube_solver(prm: dict, nxy: int, *, ramp_time: float, device="cuda:0"):
+    from . import workloads
+    from .three_d import curved_boundary_warp3d as c3
+
+    g = workloads.tube_geometry(prm, nxy)
+    mat, spec, kw = workloads.tube_case(prm, nxy, ramp_time=ramp_time)
+    return c3.WarpSparseCurvedBoundaryLBM3D(g, material=mat, boundary=spec, device=device, **kw)
+
+
+def run_to_residual(solver, tol: float, *, check: int = 100, t_min: float = 0.0,
+                    max_steps: int = 400_000, graph=None) -> dict:
+    """Step until |u - u_prev|_2 / (check |u|_2) < tol (relative displacement
+    change per step over a check interval), after t >= t_min."""
+    import torch
+
+    g = graph if graph is not None else solver.capture_graph(check)
+    prev = solver.u.clone()
+    torch.cuda.synchronize()
+    t0 = _time.perf_counter()
+    steps0 = solver.steps
+    r = float("inf")
+    while solver.steps - steps0 < max_steps:
+        g.launch()
+        du = torch.linalg.vector_norm(solver.u - prev).item()
+        nu = torch.linalg.vector_norm(solver.u).item()
+        r = du / (check * nu) if nu > 0 else float("inf")
+        prev.copy_(solver.u)
+        if solver.time >= t_min and r < tol:
+            break
+    torch.cuda.synchronize()
+    return {"wall_s": _time.perf_counter() - t0, "steps": solver.steps - steps0, "residual": r,
+            "invalid": bool(solver.invalid_state())}
+
+
+def warm_initialize(solver, pred: np.ndarray) -> bool:
+    """Start `solver` from a predicted [12, G] (u, F - I) field; returns False
+    (and leaves the solver undeformed) if the prediction has det F <= floor
+    at some active node."""
+    nx, ny, nz = solver.nx, solver.ny, solver.nz
+    p = pred.reshape(12, nx, ny, nz)[:, solver.active_i, solver.active_j, solver.active_k]
+    F = p[3:12].copy()
+    F[0] += 1.0
+    F[4] += 1.0
+    F[8] += 1.0
+    Fm = F.reshape(3, 3, -1)
+    det = (Fm[0, 0] * (Fm[1, 1] * Fm[2, 2] - Fm[1, 2] * Fm[2, 1])
+           - Fm[0, 1] * (Fm[1, 0] * Fm[2, 2] - Fm[1, 2] * Fm[2, 0])
+           + Fm[0, 2] * (Fm[1, 0] * Fm[2, 1] - Fm[1, 1] * Fm[2, 0]))
+    if not np.all(det > 10.0 * solver.jacobian_floor):
+        return False
+    U = np.zeros((12, solver.n_active))
+    U[3:] = F
+    solver._initialize_from_active(U, p[:3], init_order=1)
+    return True
+
+
+def generate_equilibria(params: list[dict], nxy: int, tol: float, device="cuda:0",
+                        check: int = 100) -> list[dict]:
+    """Cold-start solves of the given tube cases to the residual tolerance:
+    the solver's own equilibria, the surrogate's training data."""
+    from . import workloads
+
+    out = []
+    for prm in params:
+        s = make_tube_solver(prm, nxy, ramp_time=workloads.TUBE_RAMP_TIME, device=device)
+        info = run_to_residual(s, tol, check=check, t_min=workloads.TUBE_RAMP_TIME)
+        x, mask = tube_features(prm, nxy)
+        out.append({"params": prm, "x": x, "mask": mask, "target": solver_targets(s),
+                    "steps": info["steps"], "wall_s": info["wall_s"],
+                    "residual": info["residual"], "invalid": info["invalid"]})
+    return out
+
+
+class Surrogate:
+    """FNO plus the per-channel output scaling of the training set."""
+
+    def __init__(self, nxy: int, *, modes=(4, 4, 8), batch: int = 4, device="cuda:0",
+                 seed: int = 0):
+        from . import workloads
+
+        nx, ny, nz, _ = workloads.tube_lattice(nxy)
+        self.nxy = nxy
+        self.net = FNO((nx, ny, nz), modes=modes, batch=batch, device=device, seed=seed)
+        self.scale = np.ones(C_OUT, dtype=np.float32)
+        self.history: list[float] = []
+
+    def _batches(self, data, rng):
+        B = self.net.B
+        idx = rng.permutation(len(data))
+        if len(idx) % B:
+            idx = np.concatenate([idx, rng.choice(len(data), B - len(idx) % B)])
+        return idx.reshape(-1, B)
+
+    def fit(self, data, *, epochs: int = 100, lr: float = 2e-3, seed: int = 0) -> list[float]:
+        import torch
+
+        net = self.net
+        dev = net.dev
+        t_all = np.stack([d["target"] for d in data])
+        m_all = np.stack([d["mask"] for d in data])
+        w = m_all[:, None, :]
+        std = np.sqrt((t_all ** 2 * w).sum(axis=(0, 2)) / np.maximum(w.sum(axis=(0, 2)), 1))
+        self.scale = np.maximum(std, 1e-6).astype(np.float32)
+        X = torch.as_tensor(np.stack([d["x"] for d in data]), device=dev)
+        T = torch.as_tensor((t_all / self.scale[None, :, None]).astype(np.float32), device=dev)
+        Mk = torch.as_tensor(m_all.astype(np.float32), device=dev)
+        wch = torch.ones(C_OUT, dtype=torch.float32, device=dev)
+        rng = np.random.default_rng(seed)
+        hist = []
+        n_batches = 0
+        for ep in range(epochs):
+            lr_e = lr * 0.5 * (1 + math.cos(math.pi * ep / epochs))
+            tot = torch.zeros((), dtype=torch.float64, device=dev)
+            for b in self._batches(data, rng):
+                bi = torch.as_tensor(b, device=dev)
+                y = net.forward(X[bi].contiguous())
+                part, dy = net.loss_grad(y, T[bi].contiguous(), Mk[bi].contiguous(), wch)
+                net.backward(dy)
+                net.adam_step(lr=lr_e)
+                tot += part.sum().double()
+                n_batches += 1
+            hist.append(float(tot.item()) / len(self._batches(data, np.random.default_rng(0))))
+        if not net.gemm_ok():
+            raise RuntimeError("tensor-core GEMM reported incomplete MMAs during training")
+        self.history = hist
+        return hist
+
+    def predict(self, feats: list[np.ndarray]) -> list[np.ndarray]:
+        import torch
+
+        net = self.net
+        out = []
+        for k in range(0, len(feats), net.B):
+            chunk = feats[k:k + net.B]
+            pad = chunk + [chunk[-1]] * (net.B - len(chunk))
+            y = net.forward(torch.as_tensor(np.stack(pad), device=net.dev))
+            y = y.double().cpu().numpy() * self.scale[None, :, None]
+            out.extend(list(y[:len(chunk)]))
+        return out
+
+
+def _rel_err(a: np.ndarray, b: np.ndarray, mask: np.ndarray) -> float:
+    m = mask.astype(bool)
+    return float(np.linalg.norm((a - b)[:, m]) / max(np.linalg.norm(b[:, m]), 1e-300))
+
+
+def train_and_compare(*, nxy: int = 32, n_train: int = 64, n_test: int = 4, epochs: int = 200,
+                      tol: float = 1e-8, seed: int = 7, device="cuda:0", modes=(4, 4, 8),
+                      lr: float = 2e-3) -> dict:
+    """Generate solver equilibria, train the surrogate, then compare warm and
+    cold starts on held-out cases.
+
+    Per held-out case: the cold start (undeformed, end load ramped over
+    TUBE_RAMP_TIME) and the warm start (surrogate prediction, end load at
+    once) both run to `tol`; the cold run then continues to tol/100, whose
+    field is the converged reference both final errors are measured against.
+    """
+    from . import workloads
+
+    params = workloads.tube_params(n_train + n_test, seed)
+    t0 = _time.perf_counter()
+    train = generate_equilibria(params[:n_train], nxy, tol, device)
+    gen_s = _time.perf_counter() - t0
+    sur = Surrogate(nxy, modes=modes, device=device, seed=seed)
+    t0 = _time.perf_counter()
+    hist = sur.fit(train, epochs=epochs, lr=lr, seed=seed)
+    fit_s = _time.perf_counter() - t0
+    cases = []
+    for prm in params[n_train:]:
+        x, mask = tube_features(prm, nxy)
+        pred = sur.predict([x])[0]
+        cold = make_tube_solver(prm, nxy, ramp_time=workloads.TUBE_RAMP_TIME, device=device)
+        ci = run_to_residual(cold, tol, t_min=workloads.TUBE_RAMP_TIME)
+        u_cold = solver_targets(cold)
+        run_to_residual(cold, tol / 100.0)
+        ref = solver_targets(cold)
+        warm = make_tube_solver(prm, nxy, ramp_time=0.0, device=device)
+        ok = warm_initialize(warm, pred)
+        if ok:
+            wi = run_to_residual(warm, tol)
+        else:  # fallback: the plain cold start
+            warm = make_tube_solver(prm, nxy, ramp_time=workloads.TUBE_RAMP_TIME, device=device)
+            wi = run_to_residual(warm, tol, t_min=workloads.TUBE_RAMP_TIME)
+        u_warm = solver_targets(warm)
+        cases.append({"params": prm, "warm_ok": ok, "cold_steps": ci["steps"],
+                      "warm_steps": wi["steps"], "cold_wall_s": ci["wall_s"],
+                      "warm_wall_s": wi["wall_s"], "cold_err": _rel_err(u_cold, ref, mask),
+                      "warm_err": _rel_err(u_warm, ref, mask),
+                      "prediction_err": _rel_err(pred, ref, mask),
+                      "warm_invalid": wi["invalid"], "cold_invalid": ci["invalid"]})
+    cold_w = sum(c["cold_wall_s"] for c in cases)
+    warm_w = sum(c["warm_wall_s"] for c in cases)
+    return {"nxy": nxy, "n_train": n_train, "n_test": n_test, "epochs": epochs, "tol": tol,
+            "modes": list(modes), "generate_s": gen_s, "fit_s": fit_s,
+            "train_loss_first": hist[0], "train_loss_last": hist[-1],
+            "train_steps_mean": float(np.mean([d["steps"] for d in train])),
+            "cases": cases, "cold_wall_s": cold_w, "warm_wall_s": warm_w,
+            "speedup_wall": cold_w / max(warm_w, 1e-12),
+            "speedup_steps": sum(c["cold_steps"] for c in cases)
+            / max(sum(c["warm_steps"] for c in cases), 1)}

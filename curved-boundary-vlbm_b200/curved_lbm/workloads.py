@@ -207,3 +207,92 @@ def superellipse_batch(n_inst: int = 256, seed: int = 20261203, device=None,
     params = superellipse_params(n_inst, seed, n_min, n_max)
     geoms = superellipse_geometries(params, processes)
     return params, superellipse_solvers(params, geoms, device)
+
+
+# ---------------------------------------------------------------------------
+# Finite tube under end stretch and twist (warm-start data set)
+# ---------------------------------------------------------------------------
+TUBE_LENGTH = 2.0
+TUBE_RAMP_TIME = 2.0
+
+
+def tube_params(n: int, seed: int = 7) -> list[dict]:
+    """Seeded tube cases: r_in ~ U[0.3, 0.5], r_out ~ U[0.6, 0.9],
+    stretch ~ U[1.0, 1.3] (axial end displacement (stretch - 1) * length),
+    twist ~ U[0, pi/4]."""
+    rng = np.random.default_rng(seed)
+    return [{"r_in": float(rng.uniform(0.3, 0.5)), "r_out": float(rng.uniform(0.6, 0.9)),
+             "stretch": float(rng.uniform(1.0, 1.3)),
+             "twist": float(rng.uniform(0.0, math.pi / 4))} for _ in range(n)]
+
+
+def tube_lattice(nxy: int = 32):
+    """(nx, ny, nz, dx): the tube lattice, nxy^2 x 2 nxy nodes of spacing 1.92/nxy
+    (x and y span 1.92 >= 2 * 0.9; z spans 3.84 around the length-2 tube)."""
+    dx = 1.92 / nxy
+    return nxy, nxy, 2 * nxy, dx
+
+
+def tube_geometry(prm: dict, nxy: int = 32):
+    """Tube r_in <= rho <= r_out, z0 <= z <= z0 + 2 on the tube lattice.
+
+    Boundary ids as the reference's tube case (cases/tube_pull_torsion.py):
+    1 outer wall, 2 inner wall (both traction free), 3 left end (clamped),
+    4 right end (prescribed stretch and twist)."""
+    from .three_d import curved_boundary_warp3d as c3
+
+    nx, ny, nz, dx = tube_lattice(nxy)
+    cx, cy = 0.5 * nx * dx, 0.5 * ny * dx
+    z0 = 0.5 * (nz * dx - TUBE_LENGTH)
+    z1 = z0 + TUBE_LENGTH
+    ri, ro = prm["r_in"], prm["r_out"]
+
+    def phiv(X, Y, Z):
+        X, Y, Z = np.broadcast_arrays(X, Y, Z)
+        r = np.sqrt((X - cx) ** 2 + (Y - cy) ** 2)
+        return np.maximum.reduce((r - ro, ri - r, z0 - Z, Z - z1))
+
+    def normv(X, Y, Z):
+        X, Y, Z = np.broadcast_arrays(X, Y, Z)
+        r = np.maximum(np.sqrt((X - cx) ** 2 + (Y - cy) ** 2), 1e-30)
+        ex, ey = (X - cx) / r, (Y - cy) / r
+        d = np.stack([np.abs(r - ro), np.abs(r - ri), np.abs(Z - z0), np.abs(Z - z1)])
+        m = np.argmin(d, axis=0)
+        nxv = np.select([m == 0, m == 1], [ex, -ex], 0.0)
+        nyv = np.select([m == 0, m == 1], [ey, -ey], 0.0)
+        nzv = np.select([m == 2, m == 3], [-np.ones_like(Z), np.ones_like(Z)], 0.0)
+        return nxv, nyv, nzv
+
+    def bid(x, y, z, *_):
+        r = math.sqrt((x - cx) ** 2 + (y - cy) ** 2)
+        d = [abs(r - ro), abs(r - ri), abs(z - z0), abs(z - z1)]
+        return (1, 2, 3, 4)[int(np.argmin(d))]
+
+    return c3.CurvedBoundaryGeometry3D.from_level_set(
+        nx=nx, ny=ny, nz=nz, length_x=nx * dx, length_y=ny * dx, length_z=nz * dx,
+        phi=lambda x, y, z: float(phiv(np.asarray(x), np.asarray(y), np.asarray(z))),
+        boundary_id=bid, phi_vectorized=phiv, normal_vectorized=normv, label="tube")
+
+
+def tube_case(prm: dict, nxy: int = 32, ramp_time: float = TUBE_RAMP_TIME):
+    """(material, boundary spec, solver kwargs) of one tube case.  The right
+    end follows the exact stretch + twist displacement of
+    CURVED3D_VALUE_Z_STRETCH_EXACT_TWIST_VELOCITY, ramped over `ramp_time`
+    (0: applied at once, as a warm start needs)."""
+    from .three_d import curved_boundary_warp3d as c3
+
+    nx, ny, _, dx = tube_lattice(nxy)
+    cx, cy = 0.5 * nx * dx, 0.5 * ny * dx
+    mat = c3.WarpHyperelasticMaterial3D(model="neo_hooke", lam=1.0, mu=1.0)
+    right = (cx, cy, (prm["stretch"] - 1.0) * TUBE_LENGTH, prm["twist"], float(ramp_time))
+    spec = c3.CurvedBoundarySpec3D(
+        kind="neumann", value_mode=c3.CURVED3D_VALUE_ZERO,
+        id_kinds={1: "neumann", 2: "neumann", 3: "dirichlet", 4: "dirichlet"},
+        id_value_modes={1: 0, 2: 0, 3: 0, 4: c3.CURVED3D_VALUE_Z_STRETCH_EXACT_TWIST_VELOCITY},
+        id_params={4: right})
+    kw = dict(lattice_speed=10.0, collision_omega=1.8, boundary_reconstruction="local_f",
+              source_mode="damping", damping_gamma=10.0, local_displacement_interval=1,
+              local_displacement_sweeps=1, local_displacement_relax=0.85,
+              local_displacement_boundary_weight=100.0, local_displacement_boundary_id=-1,
+              local_compatibility_interval=1, local_compatibility_blend=0.5)
+    return mat, spec, kw

@@ -356,6 +356,41 @@ int cvlbm_gemm_bf16(const void *A, const void *B, float *C, int32_t M, int32_t N
                     int32_t lda, int32_t ldb, int32_t ldc, int32_t accumulate, int32_t *error,
                     void *stream);
 
+/* ------------------------------------------------------------------------ */
+/* Warm-start surrogate (Fourier neural operator): CUDA-core kernels          */
+/* ------------------------------------------------------------------------ */
+/* Activations are channel-major per sample, x[b][c][g] (g = lattice node);
+ * spectral coefficients a[b][c][k] (k = retained real Fourier mode); weights
+ * W[o][i], R[k][i][o].  All fp32 except the bf16 operands of
+ * cvlbm_gemm_bf16.  At most 32 channels.  No counterpart in the reference. */
+
+/* z = W x + bias (+ s), y = gelu(z) if act (z may be NULL). */
+int cvlbm_fno_pointwise_fwd(int32_t B, int32_t G, int32_t Cin, int32_t Cout, const float *x,
+                            const float *W, const float *bias, const float *s, int32_t act,
+                            float *z, float *y, void *stream);
+/* dz = dy * gelu'(z) over n elements. */
+int cvlbm_fno_gelu_bwd(int64_t n, const float *z, const float *dy, float *dz, void *stream);
+/* dx (+)= W^T dz (dx may be NULL); dW = sum dz x^T, db = sum dz over samples and
+ * nodes (deterministic order).  scratch: cvlbm_fno_pointwise_scratch() floats. */
+int cvlbm_fno_pointwise_bwd(int32_t B, int32_t G, int32_t Cin, int32_t Cout, const float *dz,
+                            const float *x, const float *W, float *dx, int32_t accumulate_dx,
+                            float *dW, float *db, float *scratch, void *stream);
+int64_t cvlbm_fno_pointwise_scratch(int32_t B, int32_t G, int32_t Cin, int32_t Cout);
+/* bh[b][o][k] = sum_i a[b][i][k] R[k][i][o], stored as bf16. */
+int cvlbm_fno_spec_mix_fwd(int32_t B, int32_t C, int32_t M, const float *a, const float *R,
+                           void *bh_bf16, void *stream);
+/* da = R dbh (bf16 out) and dR[k][i][o] = sum_b a[b][i][k] dbh[b][o][k]. */
+int cvlbm_fno_spec_mix_bwd(int32_t B, int32_t C, int32_t M, const float *a, const float *dbh,
+                           const float *R, void *da_bf16, float *dR, void *stream);
+int cvlbm_fno_to_bf16(int64_t n, const float *src, void *dst, void *stream);
+/* masked weighted MSE: part[p] (n_parts blocks) sum to the loss; dy its gradient. */
+int cvlbm_fno_mse(int32_t B, int32_t C, int32_t G, const float *y, const float *t,
+                  const float *mask, const float *w, float inv_count, float *dy, float *part,
+                  int32_t n_parts, void *stream);
+/* Adam step, bias correction folded into lr. */
+int cvlbm_fno_adam(int64_t n, float *p, const float *g, float *m, float *v, float lr, float b1,
+                   float b2, float eps, void *stream);
+
 /* Library version (major*10000 + minor*100 + patch) and last error text. */
 int cvlbm_version(void);
 const char *cvlbm_last_error(void);

@@ -1,0 +1,119 @@
+"""Warm-start surrogate: gradients against the FP64 oracle, and the gain of the
+trained network over the cold start.
+
+CPU: the oracle's own gradients against central finite differences; the
+Fourier basis is orthonormal.  GPU: the native forward/backward (tensor-core
+spectral transforms, CUDA-core mixing) against the oracle with the same bf16
+rounding; a small trained surrogate must cut the steps to the residual
+tolerance against the cold start while reaching the same converged field.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import fno_oracle as fo
+
+
+def _random_params(rng, cin, c, cout, M, L):
+    p = {"W0": rng.normal(0, 0.5, (c, cin)), "b0": rng.normal(0, 0.1, c)}
+    for l in range(1, L + 1):
+        p[f"W{l}"] = rng.normal(0, 1 / np.sqrt(c), (c, c))
+        p[f"b{l}"] = rng.normal(0, 0.1, c)
+        p[f"R{l}"] = rng.normal(0, 1 / c, (M, c, c))
+    p["Wp"] = rng.normal(0, 1 / np.sqrt(c), (cout, c))
+    p["bp"] = rng.normal(0, 0.1, cout)
+    return p
+
+
+def test_fourier_basis_is_orthonormal():
+    from curved_lbm.warmstart import fourier_basis
+
+    phi = fourier_basis((8, 6, 10), (3, 2, 4))
+    m = 5 * 3 * 7
+    assert phi.shape == (480, 128)
+    gram = phi[:, :m].T @ phi[:, :m]
+    assert np.allclose(gram, np.eye(m), atol=1e-12)
+    assert not phi[:, m:].any()
+
+
+def test_oracle_gradients_match_finite_differences():
+    rng = np.random.default_rng(0)
+    B, cin, c, cout, G, L = 2, 3, 4, 2, 12, 2
+    phi = rng.normal(0, 0.3, (G, 5))
+    p = _random_params(rng, cin, c, cout, 5, L)
+    x = rng.normal(0, 1, (B, cin, G))
+    t = rng.normal(0, 1, (B, cout, G))
+    mask = (rng.random((B, G)) > 0.3).astype(float)
+    wch = rng.uniform(0.5, 2.0, cout)
+
+    def loss(pp):
+        y, _ = fo.forward(pp, x, phi, L, bf16=False)
+        return fo.mse(y, t, mask, wch)[0]
+
+    y, cache = fo.forward(p, x, phi, L, bf16=False)
+    _, dy = fo.mse(y, t, mask, wch)
+    g = fo.backward(p, cache, dy, phi, L, bf16=False)
+    for key in p:
+        flat = p[key].reshape(-1)
+        for idx in rng.choice(flat.size, size=min(4, flat.size), replace=False):
+            h = 1e-6
+            old = flat[idx]
+            flat[idx] = old + h
+            lp = loss(p)
+            flat[idx] = old - h
+            lm = loss(p)
+            flat[idx] = old
+            fd = (lp - lm) / (2 * h)
+            assert abs(fd - g[key].reshape(-1)[idx]) <= 1e-6 + 1e-5 * abs(fd), (key, idx)
+
+
+@pytest.mark.gpu
+def test_native_gradients_match_oracle():
+    import torch
+
+    from curved_lbm.warmstart import C_IN, C_OUT, FNO, fourier_basis
+
+    shape, modes, L = (8, 8, 8), (2, 2, 2), 4
+    net = FNO(shape, modes=modes, layers=L, batch=4, seed=1)
+    rng = np.random.default_rng(2)
+    G = int(np.prod(shape))
+    x = rng.normal(0, 1, (4, C_IN, G)).astype(np.float32)
+    t = rng.normal(0, 1, (4, C_OUT, G)).astype(np.float32)
+    mask = (rng.random((4, G)) > 0.4).astype(np.float32)
+    wch = rng.uniform(0.5, 2.0, C_OUT).astype(np.float32)
+    dev = net.dev
+    xt, tt = torch.as_tensor(x, device=dev), torch.as_tensor(t, device=dev)
+    mt, wt = torch.as_tensor(mask, device=dev), torch.as_tensor(wch, device=dev)
+    y = net.forward(xt)
+    part, dy = net.loss_grad(y, tt, mt, wt)
+    net.backward(dy)
+    torch.cuda.synchronize()
+    assert net.gemm_ok()
+    p64 = {k: v.double().cpu().numpy() for k, v in net.params.items()}
+    phi = fourier_basis(shape, modes)
+    y_o, cache = fo.forward(p64, x.astype(np.float64), phi, L)
+    loss_o, dy_o = fo.mse(y_o, t.astype(np.float64), mask.astype(np.float64),
+                          wch.astype(np.float64))
+    g_o = fo.backward(p64, cache, dy_o, phi, L)
+    y_n = y.double().cpu().numpy()
+    assert np.linalg.norm(y_n - y_o) <= 2e-3 * np.linalg.norm(y_o)
+    assert abs(float(part.sum().item()) - loss_o) <= 2e-3 * abs(loss_o)
+    for k, go in g_o.items():
+        gn = net.grads[k].double().cpu().numpy()
+        err = np.linalg.norm(gn - go) / max(np.linalg.norm(go), 1e-30)
+        assert err <= 2e-2, (k, err)
+
+
+@pytest.mark.gpu
+def test_trained_surrogate_beats_cold_start():
+    from curved_lbm import warmstart as ws
+
+    rep = ws.train_and_compare(nxy=16, n_train=12, n_test=2, epochs=60, tol=1e-7, seed=3)
+    for case in rep["cases"]:
+        assert case["warm_ok"], case
+        assert case["warm_steps"] < case["cold_steps"], case
+        # both runs reach the converged field to within the tolerance's reach
+        assert case["warm_err"] <= max(10 * case["cold_err"], 1e-4), case
+    assert rep["train_loss_last"] < 0.5 * rep["train_loss_first"]
