@@ -176,7 +176,7 @@ __global__ void __launch_bounds__(256) k3_sweep(Ctx3 c, const double* __restrict
 //      to shared memory for the moments)
 //   2  moments (summed over q in order) and the nine targets of I + grad u
 //      (+-2 star stencil of the swept u), spread over the block
-//   3  warp 0: P(F); warp 1: the repaired F, P(F_repaired), U / U_need rows
+//   3  P(F) and P(F_repaired), one row per warp (six rows), U / U_need rows
 //   4  warp q: collision, repair delta and push of direction q
 constexpr int kCN = 32;  // nodes per collide block (one per lane)
 
@@ -292,45 +292,53 @@ __global__ void __launch_bounds__(kQ3 * kCN, 4)
   }
   __syncthreads();
 
-  // 3: P(F) on warp 0; repaired F, its Piola and the U rows on warp 1
-  if (warp == 0) {
+  // 3: P(F) and P(F_repaired), one row of each per warp: warps 0-2 row
+  // `warp` of P(F), warps 3-5 row `warp - 3` of the repaired F and its Piola;
+  // warp 3 also writes the repaired flag and the U / U_need rows
+  {
+    const int row = warp < 3 ? warp : warp - 3;
     double F[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) F[k] = sm.S[3 + k][lane];
-    const M3 Po = piola3(F, m);
+    if (warp < 3) {
+      double Pr[3];
+      piola3_row(F, m, row, Pr);
 #pragma unroll
-    for (int k = 0; k < 9; ++k) sm.Po[k][lane] = Po.v[k];
-  } else if (warp == 1) {
-    bool repaired = false;
-    double nn[9];
-    if (do_repair) {
-      const double beta = fmax(0.0, fmin(1.0, p.blend));
+      for (int c2 = 0; c2 < 3; ++c2) sm.Po[3 * row + c2][lane] = Pr[c2];
+    } else {
+      bool repaired = false;
+      double nn[9];
+      if (do_repair) {
+        const double beta = fmax(0.0, fmin(1.0, p.blend));
 #pragma unroll
-      for (int k = 0; k < 9; ++k)
-        nn[k] = sm.S[3 + k][lane] + beta * (sm.T[k][lane] - sm.S[3 + k][lane]);
-      if (det3v(nn) > m.jf) {
-        repaired = true;
-        const M3 Pn = piola3(nn, m);
+        for (int k = 0; k < 9; ++k) nn[k] = F[k] + beta * (sm.T[k][lane] - F[k]);
+        if (det3v(nn) > m.jf) {
+          repaired = true;
+          double Pr[3];
+          piola3_row(nn, m, row, Pr);
 #pragma unroll
-        for (int k = 0; k < 9; ++k) {
-          sm.Pn[k][lane] = Pn.v[k];
-          sm.dF[k][lane] = nn[k] - sm.S[3 + k][lane];
+          for (int c2 = 0; c2 < 3; ++c2) {
+            sm.Pn[3 * row + c2][lane] = Pr[c2];
+            sm.dF[3 * row + c2][lane] = nn[3 * row + c2] - F[3 * row + c2];
+          }
         }
-        if (store_all && live) {
+      }
+      if (warp == 3) {
+        sm.rep[lane] = repaired ? 1 : 0;
+        if (repaired && store_all && live) {
 #pragma unroll
           for (int k = 0; k < 9; ++k) U[(size_t)(3 + k) * N + n] = nn[k];
         }
-      }
-    }
-    sm.rep[lane] = repaired ? 1 : 0;
-    const int slot = live ? fz.need_slot[n] : -1;
-    if (slot >= 0) {
-      double* row = fz.Uneed + (size_t)slot * kC3;
-      row[0] = sm.S[0][lane];
-      row[1] = sm.S[1][lane];
-      row[2] = sm.S[2][lane];
+        const int slot = live ? fz.need_slot[n] : -1;
+        if (slot >= 0) {
+          double* rowp = fz.Uneed + (size_t)slot * kC3;
+          rowp[0] = sm.S[0][lane];
+          rowp[1] = sm.S[1][lane];
+          rowp[2] = sm.S[2][lane];
 #pragma unroll
-      for (int k = 0; k < 9; ++k) row[3 + k] = repaired ? nn[k] : sm.S[3 + k][lane];
+          for (int k = 0; k < 9; ++k) rowp[3 + k] = repaired ? nn[k] : F[k];
+        }
+      }
     }
   }
   __syncthreads();
