@@ -432,7 +432,8 @@ def train_and_compare(*, nxy: int = 32, n_train: int = 64, n_test: int = 4, epoc
     """
     from . import workloads
 
-    params = workloads.tube_params(n_train + n_test, seed)
+    dx = workloads.tube_lattice(nxy)[3]
+    params = workloads.tube_params(n_train + n_test, seed, min_wall=4.0 * dx)
     t0 = _time.perf_counter()
     train = generate_equilibria(params[:n_train], nxy, tol, device)
     gen_s = _time.perf_counter() - t0
@@ -465,7 +466,7 @@ def train_and_compare(*, nxy: int = 32, n_train: int = 64, n_test: int = 4, epoc
                       "warm_invalid": wi["invalid"], "cold_invalid": ci["invalid"]})
     cold_w = sum(c["cold_wall_s"] for c in cases)
     warm_w = sum(c["warm_wall_s"] for c in cases)
-    return {"nxy": nxy, "n_train": n_train, "n_test": n_test, "epochs": epochs, "tol": tol,
+    return {"nxy": nxy, "dx": dx, "min_wall": 4.0 * dx, "n_train": n_train, "n_test": n_test, "epochs": epochs, "tol": tol,
             "modes": list(modes), "generate_s": gen_s, "fit_s": fit_s,
             "train_loss_first": hist[0], "train_loss_last": hist[-1],
             "train_steps_mean": float(np.mean([d["steps"] for d in train])),

@@ -216,14 +216,21 @@ TUBE_LENGTH = 2.0
 TUBE_RAMP_TIME = 2.0
 
 
-def tube_params(n: int, seed: int = 7) -> list[dict]:
-    """Seeded tube cases: r_in ~ U[0.3, 0.5], r_out ~ U[0.6, 0.9],
+def tube_params(n: int, seed: int = 7, min_wall: float = 0.0) -> list[dict]:
+    """Seeded tube cases: r_in ~ U[0.3, 0.5], r_out ~ U[max(0.6, r_in + min_wall), 0.9],
     stretch ~ U[1.0, 1.3] (axial end displacement (stretch - 1) * length),
-    twist ~ U[0, pi/4]."""
+    twist ~ U[0, pi/4].  `min_wall` keeps the wall several lattice cells thick
+    on coarse lattices (the local_f characteristic stencil needs a full-rank
+    quadratic fit within three cells); r_in is capped so that the range of
+    r_out stays non-empty."""
     rng = np.random.default_rng(seed)
-    return [{"r_in": float(rng.uniform(0.3, 0.5)), "r_out": float(rng.uniform(0.6, 0.9)),
-             "stretch": float(rng.uniform(1.0, 1.3)),
-             "twist": float(rng.uniform(0.0, math.pi / 4))} for _ in range(n)]
+    out = []
+    for _ in range(n):
+        ri = float(rng.uniform(0.3, min(0.5, 0.9 - min_wall)))
+        ro = float(rng.uniform(max(0.6, ri + min_wall), 0.9))
+        out.append({"r_in": ri, "r_out": ro, "stretch": float(rng.uniform(1.0, 1.3)),
+                    "twist": float(rng.uniform(0.0, math.pi / 4))})
+    return out
 
 
 def tube_lattice(nxy: int = 32):

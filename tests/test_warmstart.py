@@ -110,7 +110,7 @@ def test_native_gradients_match_oracle():
 def test_trained_surrogate_beats_cold_start():
     from curved_lbm import warmstart as ws
 
-    rep = ws.train_and_compare(nxy=16, n_train=12, n_test=2, epochs=60, tol=1e-7, seed=3)
+    rep = ws.train_and_compare(nxy=24, n_train=12, n_test=2, epochs=60, tol=1e-7, seed=3)
     for case in rep["cases"]:
         assert case["warm_ok"], case
         assert case["warm_steps"] < case["cold_steps"], case
