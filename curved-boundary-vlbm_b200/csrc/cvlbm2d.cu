@@ -355,6 +355,7 @@ __device__ __forceinline__ double interp_link(const double* Uc, const int* act, 
 }  // namespace
 
 #include "cvlbm2d_fused.cuh"
+#include "cvlbm2d_split.cuh"
 
 namespace {
 
@@ -490,12 +491,16 @@ struct FusedLaunch2 {
 
 // Compiled tile variants: (tile rows, resident blocks per SM).  The tile list
 // in the problem must have been built for the variant's tile height.
+// Variant 5 selects the split form (cvlbm2d_split.cuh) instead of a tile shape.
+constexpr int kSplitVariant = 5;
+
 FusedLaunch2 fused_variant(int v) {
   switch (v) {
     case 1: return {k_fused2<8, 2>, kTX * 8, fused_smem2<8>(), 8};
     case 2: return {k_fused2<8, 3>, kTX * 8, fused_smem2<8>(), 8};
     case 3: return {k_fused2<16, 2>, kTX * 16, fused_smem2<16>(), 16};
     case 4: return {k_fused2<4, 4>, kTX * 4, fused_smem2<4>(), 4};
+    case kSplitVariant: return {nullptr, 0, 0, 16};  // split kernels, no tiles used
     default: return {k_fused2<16, 1>, kTX * 16, fused_smem2<16>(), 16};
   }
 }
@@ -521,7 +526,9 @@ extern "C" int cvlbm2d_run(const cvlbm2d_problem* p, cvlbm2d_fields* f, double t
   double t = time0;
   const bool fused = fused_ok(p, f);
   FusedLaunch2 fl = fused_variant(p->tile_variant);
-  if (fused) cudaFuncSetAttribute(fl.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fl.smem);
+  const bool split = fused && p->tile_variant == kSplitVariant;
+  if (fused && !split)
+    cudaFuncSetAttribute(fl.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fl.smem);
   // the fused kernel reads u* in the halo of its tile, so it ping-pongs
   // between u_star and u_next; an odd count ends with one copy back
   double* us_cur = f->u_star;
@@ -533,7 +540,22 @@ extern "C" int cvlbm2d_run(const cvlbm2d_problem* p, cvlbm2d_fields* f, double t
     // kernel writes clock[(k+1)&1] (no separate tick launch)
     const double* clock = graph_mode ? f->clock + (k & 1) : nullptr;
     double* clock_next = graph_mode ? f->clock + ((k + 1) & 1) : nullptr;
-    if (fused) {
+    if (split) {
+      int tk = timer_begin(s);
+      k2s_moments<<<blocks(N, 256), 256, 0, s>>>(c, f->f0, f->U, sweep ? f->u_next : f->u,
+                                                 f->u_star, f->invalid, sweep);
+      cv::count_launches(1);
+      if (sweep) {
+        k2s_sweep<<<blocks(N, 256), 256, 0, s>>>(c, f->U, f->u_next, f->u, f->u_star, clock, t);
+        cv::count_launches(1);
+      }
+      k2s_collide<<<blocks(N, 128), 128, 0, s>>>(c, f->f0, f->f1, f->U, f->u, p->need_fields,
+                                                 f->link_scratch, repair, k == nsteps - 1);
+      cv::count_launches(1);
+      timer_end(tk, s);
+      launch_links(c, f->f1, f->f1, f->U, f->u, clock, t, 0.5 * p->dt, s, 1, f->link_scratch,
+                   p->link_partner, clock_next);
+    } else if (fused) {
       Fused2 fz{p->tiles, p->n_tiles, p->tiles_j, p->need_fields, p->link_partner,
                 f->link_scratch, k == nsteps - 1};
       int tk = timer_begin(s);
@@ -615,7 +637,7 @@ extern "C" int cvlbm2d_refresh(const cvlbm2d_problem* p, cvlbm2d_fields* f, void
 }
 
 extern "C" int cvlbm2d_tile_variant(int32_t v) {
-  if (v < 0 || v > 4) return 0;
+  if (v < 0 || v > kSplitVariant) return 0;
   return fused_variant(v).tile_i;
 }
 

@@ -241,7 +241,8 @@ extern "C" int cvlbm2d_batch_create(int32_t n_inst, const cvlbm2d_problem* probl
     return fail(CVLBM_ERR_INVALID_ARG, "cvlbm2d_batch_create: bad arguments");
   *out = nullptr;
   const int tile_i = cvlbm2d_tile_variant(tile_variant);
-  if (tile_i <= 0) return fail(CVLBM_ERR_INVALID_ARG, "cvlbm2d_batch_create: unknown tile variant");
+  if (tile_i <= 0 || tile_variant == kSplitVariant)
+    return fail(CVLBM_ERR_INVALID_ARG, "cvlbm2d_batch_create: unknown tile variant");
   std::vector<Inst2> hi(n_inst);
   std::vector<InstState2> hs(n_inst);
   std::vector<int2> work, lwork;

@@ -178,7 +178,7 @@ class BatchedCurvedBoundaryLBM2D:
 
         saved = [(s.f0.clone(), s.f1.clone(), s.u_star.clone(), s.u_local_next.clone(),
                   s.U.clone(), s.u.clone(), s.time, s.steps) for s in self.solvers]
-        cand = [v for v in (variants if variants is not None else range(8))
+        cand = [v for v in (variants if variants is not None else range(5))
                 if int(self._lib.cvlbm2d_tile_variant(int(v))) > 0]
         times = {}
         for v in cand:

@@ -75,7 +75,7 @@ def test_annulus_1000_steps_match_oracle(n):
         close_rel(k, s.numpy_field(k), ref[k])
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
 def test_annulus_tile_variants_match_oracle(variant):
     ref = _oracle_annulus(200, 1000)
     s = _gpu_annulus(200, variant=variant)
@@ -113,7 +113,7 @@ def test_annulus512_fused_variants_bitwise_equal_per_phase():
     base.run(30)
     want = [base.numpy_field(k) for k in ("f0", "u_star", "U", "u")]
     assert np.isfinite(want[0]).all()
-    for v in range(5):
+    for v in range(6):
         s = _gpu_annulus(512, variant=v)
         s.run(30)
         for k, w in zip(("f0", "u_star", "U", "u"), want):
