@@ -2,7 +2,8 @@
 
 The surrogate maps a tube case (level set of the geometry and the end load:
 stretch and twist) to the equilibrium displacement u and deformation
-gradient F on the solver lattice.  The solver then starts from that state
+gradient F on the solver lattice, as a correction to the end kinematics
+spread linearly along the tube (`kinematic_guess`).  The solver then starts from that state
 (populations at equilibrium of U = (0, F), u* from u; the end displacement
 applied at once) instead of the undeformed state with a load ramp, and the
 plain damped relaxation converges from there; a prediction with a
@@ -235,8 +236,7 @@ class FNO:
 # ---------------------------------------------------------------------------
 # Tube data: features, solver equilibria, warm and cold starts
 # ---------------------------------------------------------------------------
-def tube_features(prm: dict, nxy: int) -> tuple[np.ndarray, np.ndarray]:
-    """([8, G] input channels, [G] material mask) of one tube case."""
+def _tube_grid(prm: dict, nxy: int):
     from . import workloads
 
     nx, ny, nz, dx = workloads.tube_lattice(nxy)
@@ -246,14 +246,46 @@ def tube_features(prm: dict, nxy: int) -> tuple[np.ndarray, np.ndarray]:
     y = (np.arange(ny) + 0.5) * dx
     z = (np.arange(nz) + 0.5) * dx
     X, Y, Z = np.meshgrid(x, y, z, indexing="ij")
+    zeta = np.clip((Z - z0) / workloads.TUBE_LENGTH, 0.0, 1.0)
+    return X, Y, Z, cx, cy, z0, zeta, dx
+
+
+def kinematic_guess(prm: dict, nxy: int) -> np.ndarray:
+    """[12, G] (u, F - I) of the end kinematics spread linearly along the tube:
+    at axial fraction zeta the section is stretched by zeta (stretch - 1) L and
+    turned by zeta * twist - exactly the clamped left end and the prescribed
+    right end, with no radial (Poisson) or end-layer correction.  The
+    surrogate learns the correction to this field."""
+    from . import workloads
+
+    X, Y, Z, cx, cy, z0, zeta, dx = _tube_grid(prm, nxy)
+    th = zeta * prm["twist"]
+    c, s = np.cos(th), np.sin(th)
+    ux = (c - 1.0) * (X - cx) - s * (Y - cy)
+    uy = s * (X - cx) + (c - 1.0) * (Y - cy)
+    uz = zeta * (prm["stretch"] - 1.0) * workloads.TUBE_LENGTH
+    u = np.stack([ux, uy, uz])
+    F = np.zeros((9,) + X.shape)
+    for r in range(3):
+        g = np.gradient(u[r], dx, axis=(0, 1, 2))
+        for col in range(3):
+            F[3 * r + col] = g[col]
+    return np.concatenate([u, F]).reshape(12, -1)
+
+
+def tube_features(prm: dict, nxy: int) -> tuple[np.ndarray, np.ndarray]:
+    """([8, G] input channels, [G] material mask) of one tube case: mask, level
+    set, coordinates and the kinematic guess of u."""
+    from . import workloads
+
+    X, Y, Z, cx, cy, z0, zeta, dx = _tube_grid(prm, nxy)
     r = np.sqrt((X - cx) ** 2 + (Y - cy) ** 2)
     phi = np.maximum.reduce((r - prm["r_out"], prm["r_in"] - r, z0 - Z,
                              Z - z0 - workloads.TUBE_LENGTH))
     mask = (phi <= 0.0).astype(np.float32)
-    zeta = np.clip((Z - z0) / workloads.TUBE_LENGTH, 0.0, 1.0)
+    g = kinematic_guess(prm, nxy)[:3].reshape((3,) + X.shape)
     f = np.stack([mask, np.clip(phi / 0.3, -1, 1), (X - cx) / 0.9, (Y - cy) / 0.9,
-                  2 * zeta - 1, mask * zeta * (prm["stretch"] - 1.0) / 0.3,
-                  mask * zeta * prm["twist"] / (math.pi / 4), np.ones_like(X)])
+                  2 * zeta - 1, g[0] / 0.3, g[1] / 0.3, g[2] / 0.6])
     return f.reshape(C_IN, -1).astype(np.float32), mask.reshape(-1)
 
 
@@ -340,7 +372,8 @@ def generate_equilibria(params: list[dict], nxy: int, tol: float, device="cuda:0
         s = make_tube_solver(prm, nxy, ramp_time=workloads.TUBE_RAMP_TIME, device=device)
         info = run_to_residual(s, tol, check=check, t_min=workloads.TUBE_RAMP_TIME)
         x, mask = tube_features(prm, nxy)
-        out.append({"params": prm, "x": x, "mask": mask, "target": solver_targets(s),
+        out.append({"params": prm, "x": x, "mask": mask,
+                    "target": solver_targets(s) - kinematic_guess(prm, nxy) * mask[None, :],
                     "steps": info["steps"], "wall_s": info["wall_s"],
                     "residual": info["residual"], "invalid": info["invalid"]})
     return out
@@ -444,7 +477,7 @@ def train_and_compare(*, nxy: int = 32, n_train: int = 64, n_test: int = 4, epoc
     cases = []
     for prm in params[n_train:]:
         x, mask = tube_features(prm, nxy)
-        pred = sur.predict([x])[0]
+        pred = sur.predict([x])[0] + kinematic_guess(prm, nxy) * mask[None, :]
         cold = make_tube_solver(prm, nxy, ramp_time=workloads.TUBE_RAMP_TIME, device=device)
         ci = run_to_residual(cold, tol, t_min=workloads.TUBE_RAMP_TIME)
         u_cold = solver_targets(cold)
@@ -463,6 +496,7 @@ def train_and_compare(*, nxy: int = 32, n_train: int = 64, n_test: int = 4, epoc
                       "warm_wall_s": wi["wall_s"], "cold_err": _rel_err(u_cold, ref, mask),
                       "warm_err": _rel_err(u_warm, ref, mask),
                       "prediction_err": _rel_err(pred, ref, mask),
+                      "guess_err": _rel_err(kinematic_guess(prm, nxy) * mask[None, :], ref, mask),
                       "warm_invalid": wi["invalid"], "cold_invalid": ci["invalid"]})
     cold_w = sum(c["cold_wall_s"] for c in cases)
     warm_w = sum(c["warm_wall_s"] for c in cases)
