@@ -99,13 +99,13 @@ def batch_bench(args, dev):
     """
     import torch
 
-    from curved_lbm import _native, workloads
+    from curved_lbm import _native, replicas, workloads
     from curved_lbm.batch import BatchedCurvedBoundaryLBM2D
 
     n_inst = args.instances
     world, rank = args.world, args.rank
     t0 = time.perf_counter()
-    params = workloads.superellipse_params(n_inst)[rank::world]
+    params = replicas.deal(workloads.superellipse_params(n_inst), rank, world)
     geoms = workloads.superellipse_geometries(
         params, processes=max(1, (os.cpu_count() or 1) // world))
     solvers = workloads.superellipse_solvers(params, geoms, device=str(dev))
@@ -137,15 +137,9 @@ def batch_bench(args, dev):
     updates = float((active * steps).sum())
     ng, nw = batch.launch_grid()
     n_conv, n_bad = int((st["status"] == 1).sum()), int((st["status"] == -1).sum())
-    if world > 1:
-        import torch.distributed as dist
-
-        t = torch.tensor([device_ms, wall_s], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        u = torch.tensor([updates, n_conv, n_bad], dtype=torch.float64, device=dev)
-        dist.all_reduce(u)
-        device_ms, wall_s = float(t[0]), float(t[1])
-        updates, n_conv, n_bad = float(u[0]), int(u[1]), int(u[2])
+    (device_ms, wall_s), (updates, n_conv, n_bad) = replicas.reduce_times_and_counts(
+        [device_ms, wall_s], [updates, n_conv, n_bad], device=dev)
+    n_conv, n_bad = int(n_conv), int(n_bad)
     if rank != 0:
         return 0
     sum_n2 = int(sum(p["n"] ** 2 for p in workloads.superellipse_params(n_inst)))
@@ -251,44 +245,42 @@ def ncu_traffic(workload: str):
         return None
 
 
-def cpu_baseline(workload: str, steps: int, threads: int):
-    """Oracle (C port of the reference kernels) on the host cores, bounded sample."""
+def cpu_baseline(workload: str, seconds: float, threads: int):
+    """Oracle (C port of the reference kernels) on the host cores: lattice steps
+    of the workload in chunks of 5 until `seconds` of CPU time have passed."""
     from oracle import oracle as orc
 
     orc.load()
     builder = BUILDERS[workload]
     s, n_active = builder(oracle=True, threads=threads)
     s.step()  # warm the page cache and OpenMP pool
+    steps = 0
     t0 = time.perf_counter()
-    for _ in range(steps):
-        s.step()
-    dt = time.perf_counter() - t0
+    while True:
+        for _ in range(5):
+            s.step()
+        steps += 5
+        dt = time.perf_counter() - t0
+        if dt >= seconds:
+            break
     return {"value": n_active * steps / dt / 1e6, "unit": "MLUPS", "cores": threads,
             "kind": "port",
             "sample": f"{steps} lattice time steps of {workload} ({n_active} active nodes), "
-                      f"oracle/cvlbm_oracle.c, OpenMP {threads} threads, {dt:.2f} s"}
+                      f"oracle/cvlbm_oracle.c, OpenMP {threads} threads, {dt:.1f} s"}
 
 
 # ---------------------------------------------------------------------------
 def init_dist():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import torch
-        import torch.distributed as dist
-        from datetime import timedelta
+    from curved_lbm import replicas
 
-        backend = "nccl" if torch.cuda.is_available() else "gloo"
-        dist.init_process_group(backend, timeout=timedelta(seconds=600))
-    return world, rank, local
+    return replicas.init(timeout_s=600.0)
 
 
 def reference_arm(args, world, rank):
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    base = cpu_baseline(args.workload, max(1, args.ref_steps), threads)
+    base = cpu_baseline(args.workload, args.ref_seconds, threads)
     line = {
         "impl": "reference", "metric": "MLUPS FP64", "value": base["value"], "unit": "MLUPS",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -320,7 +312,8 @@ def main():
     ap.add_argument("--size", type=int, default=0,
                     help="lattice nodes per axis (0 = the workload's own size; smaller sizes "
                          "are for profiler captures, not bench lines)")
-    ap.add_argument("--ref-steps", type=int, default=4, help="oracle steps for the CPU legs")
+    ap.add_argument("--ref-seconds", type=float, default=12.0,
+                    help="CPU time of the oracle sample (CPU baseline and reference arm)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tile-variant", type=int, default=-1,
                     help="fused 2-D tile shape; -1 = autotune on the workload")
@@ -399,10 +392,9 @@ def main():
         if world > 1:
             dist.barrier()
     total_ms = float(sum(step_ms))
-    if world > 1:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    from curved_lbm import replicas
+
+    (total_ms,), _ = replicas.reduce_times_and_counts([total_ms], [], device=dev)
     updates = float(n_active) * args.inner * args.steps * world
     value = updates / (total_ms * 1e-3) / 1e6
 
@@ -458,7 +450,7 @@ def main():
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            base = cpu_baseline(args.workload, args.ref_steps, os.cpu_count() or 1)
+            base = cpu_baseline(args.workload, args.ref_seconds, os.cpu_count() or 1)
         except Exception as exc:  # the oracle is optional for the GPU number
             base = {"value": None, "unit": "MLUPS", "cores": 0, "kind": "port",
                     "sample": f"unavailable: {exc}"}
