@@ -14,6 +14,11 @@ Workloads (synthetic, seeded geometry; no external data):
   shell192    D3Q6x12 spherical shell, 192^3 lattice on [0,2.2]^3, inner
               r=0.5 clamped, outer r=1.0 radial traction ramped 0 -> 0.05
               over 10000 steps; same physical parameters.
+  batch256    256 D2Q4x6 superellipse shells, lattices 96^2..512^2 (seeded),
+              solved together to residual 1e-8 (see batch_bench).
+  tube_warmstart  3-D tubes under end stretch and twist: solver-generated
+              equilibria, surrogate training, warm vs cold time-to-residual
+              (see warmstart_bench).
 
 One bench step = `--inner` lattice time steps replayed from one CUDA graph.
 L2 (126 MB) is flushed between bench steps, outside the timed events.
@@ -85,6 +90,34 @@ def build_shell(device=None, n=192, oracle=False, threads=1):
 
 
 BUILDERS = {"annulus512": build_annulus, "shell192": build_shell}
+
+
+def warmstart_bench(args, dev):
+    """tube_warmstart: time-to-residual 1e-8 of 3-D tube solves, warm vs cold.
+
+    Generates `--train` tube equilibria with the solver itself (cold starts to
+    the tolerance), trains the FNO surrogate on the GPU (tensor-core spectral
+    transforms), then solves `--test` held-out cases from the cold start
+    (undeformed, end load ramped) and from the surrogate's prediction (end
+    load at once).  `value` is the wall-time ratio cold / warm over the
+    held-out cases; both runs reach the same final error against the
+    converged FP64 field (reported per case).
+    """
+    from curved_lbm import warmstart
+
+    rep = warmstart.train_and_compare(nxy=args.tube_nxy, n_train=args.train, n_test=args.test,
+                                      epochs=args.epochs, tol=args.tol, seed=7,
+                                      device=str(dev))
+    line = {"metric": "time-to-residual 1e-8, cold / warm", "value": rep["speedup_wall"],
+            "unit": "x", "higher_is_better": True, "n_gpus": 1, "dtype": "f64 solver, bf16 "
+            "tensor-core surrogate (fp32 accumulate)", "data": "synthetic (solver-generated)",
+            "config": {"workload": "tube_warmstart",
+                       "lattice": [args.tube_nxy, args.tube_nxy, 2 * args.tube_nxy],
+                       "train_cases": args.train, "test_cases": args.test,
+                       "epochs": args.epochs, "tol": args.tol},
+            "report": rep}
+    print(json.dumps(line, default=float), flush=True)
+    return 0
 
 
 def batch_bench(args, dev):
@@ -304,7 +337,12 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="annulus512", choices=sorted(BUILDERS) + ["batch256"])
+    ap.add_argument("--workload", default="annulus512",
+                    choices=sorted(BUILDERS) + ["batch256", "tube_warmstart"])
+    ap.add_argument("--tube-nxy", type=int, default=32, help="tube_warmstart: lattice nx = ny")
+    ap.add_argument("--train", type=int, default=128, help="tube_warmstart: training cases")
+    ap.add_argument("--test", type=int, default=4, help="tube_warmstart: held-out cases")
+    ap.add_argument("--epochs", type=int, default=200, help="tube_warmstart: training epochs")
     ap.add_argument("--instances", type=int, default=256, help="batch256: instance count")
     ap.add_argument("--tol", type=float, default=1e-8, help="batch256: residual tolerance")
     ap.add_argument("--max-replays", type=int, default=100000, help="batch256: replay cap")
@@ -337,6 +375,13 @@ def main():
     dev = torch.device(f"cuda:{local}")
     torch.cuda.set_device(dev)
     args.local, args.world, args.rank = local, world, rank
+    if args.workload == "tube_warmstart":
+        rc = warmstart_bench(args, dev) if rank == 0 else 0
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+        return rc
     if args.workload == "batch256":
         if args.inner == 100:
             args.inner = 1000
