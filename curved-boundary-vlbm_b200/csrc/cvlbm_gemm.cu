@@ -6,16 +6,18 @@
 // A and B are bf16, K-major (row-major with K contiguous).  M % 128 == 0,
 // N % 64 == 0, K % 64 == 0, lda/ldb % 8 == 0 (16-byte rows of 8 elements).
 //
-// One CTA (4 warps) computes a 128 x 64 tile of C.  For every 64-wide slice
-// of K the CTA copies the A (128 x 64) and B (64 x 64) tiles into shared
-// memory in the canonical no-swizzle K-major layout of the tensor core: core
-// matrices of 8 rows x 16 bytes, the two 8-element halves of a 16-element K
-// step LBO = 128 bytes apart and consecutive 8-row groups SBO = 256 bytes
-// apart.  Thread 0 issues four 128x64x16 MMAs (kind::f16, bf16 inputs, fp32
-// accumulation in 64 TMEM columns) and commits them to an mbarrier; the CTA
-// waits on it (bounded) before refilling shared memory.  The epilogue reads
-// the accumulator with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31 = rows)
-// and stores fp32 rows.
+// One CTA (4 warps) computes a 128 x BN tile of C (BN = 128 when N allows,
+// else 64).  For every 64-wide slice of K the CTA stages the A (128 x 64) and
+// B (BN x 64) tiles in shared memory in the canonical no-swizzle K-major
+// layout of the tensor core: core matrices of 8 rows x 16 bytes, the two
+// 8-element halves of a 16-element K step LBO = 128 bytes apart and
+// consecutive 8-row groups SBO = 256 bytes apart.  Two stages: while thread 0
+// has the four 128xBNx16 MMAs of one slice in flight (kind::f16, bf16 inputs,
+// fp32 accumulation in BN TMEM columns, committed to that stage's mbarrier),
+// all threads load the next slice from global memory into registers.  Long
+// K with few output tiles is split over gridDim.z into fp32 partials that a
+// second kernel adds in a fixed order.  The epilogue reads the accumulator
+// with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31 = rows).
 //
 // Every wait is bounded: a CTA whose MMAs do not complete within about a
 // second raises the error word, waits once more (bounded), frees its TMEM and
@@ -32,7 +34,6 @@ using namespace cv;
 namespace {
 
 constexpr int kBM = 128, kBN = 64, kBK = 64;
-constexpr int kTmemCols = 64;
 constexpr long long kWaitCycles = 2000000000LL;  // about one second at 2 GHz
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -87,60 +88,106 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// One CTA computes a 128 x BN tile of C over the K range
+// [blockIdx.z * kchunk, (blockIdx.z + 1) * kchunk): two shared-memory stages,
+// the global loads of slice k+1 in flight while the MMAs of slice k run.
+// With gridDim.z > 1 the tile goes to partial[blockIdx.z] (reduced later in
+// a fixed order), else to C.
+template <int BN>
 __global__ void __launch_bounds__(128)
     k_gemm_bf16(const __nv_bfloat16* __restrict__ A, const __nv_bfloat16* __restrict__ B,
-                float* __restrict__ C, int M, int N, int K, int lda, int ldb, int ldc,
-                int accumulate, int* __restrict__ error) {
-  __shared__ __align__(1024) uint8_t sA[kBM * kBK * 2];  // 16 KB, 4 slabs of 128x16
-  __shared__ __align__(1024) uint8_t sB[kBN * kBK * 2];  //  8 KB, 4 slabs of 64x16
-  __shared__ __align__(8) uint64_t bar;
+                float* __restrict__ C, float* __restrict__ partial, int M, int N, int kchunk,
+                int lda, int ldb, int ldc, int accumulate, int* __restrict__ error) {
+  extern __shared__ __align__(1024) uint8_t smem_g[];
+  uint8_t* sA[2] = {smem_g, smem_g + kBM * kBK * 2};
+  uint8_t* sB[2] = {smem_g + 2 * kBM * kBK * 2, smem_g + 2 * kBM * kBK * 2 + BN * kBK * 2};
+  __shared__ __align__(8) uint64_t bar[2];
   __shared__ uint32_t tmem_slot;
-  const int tid = threadIdx.x, warp = tid >> 5;
-  const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * kBN;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * BN;
+  const int kbeg = blockIdx.z * kchunk, nk = kchunk / kBK;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
                      smem_u32(&tmem_slot)),
-                 "r"(kTmemCols));
+                 "r"(BN));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
   }
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&bar)));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&bar[0])));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&bar[1])));
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   const uint32_t tmem = tmem_slot;
-  const uint32_t bar_a = smem_u32(&bar);
-  const uint32_t idesc = instr_desc_bf16(kBM, kBN);
+  const uint32_t idesc = instr_desc_bf16(kBM, BN);
+
+  // 16-byte chunk c of a tile: a warp covers 8 rows x 4 consecutive chunks,
+  // so 8 lanes store one core matrix (128 contiguous bytes, no bank conflict)
+  // and lanes l, l+8 read adjacent halves of one 32-byte sector
+  auto chunk_pos = [](int c, int& row, int& kc) {
+    const int w = c >> 5, l = c & 31;
+    row = (w >> 1) * 8 + (l & 7);
+    kc = (w & 1) * 4 + (l >> 3);
+  };
+  constexpr int kAChunks = kBM * 8 / 128, kBChunks = BN * 8 / 128;
+  uint4 ra[kAChunks], rb[kBChunks];
+  auto load_slice = [&](int kb) {
+    const int kk = kbeg + kb * kBK;
+#pragma unroll
+    for (int t = 0; t < kAChunks; ++t) {
+      int row, kc;
+      chunk_pos(tid + t * 128, row, kc);
+      ra[t] = *reinterpret_cast<const uint4*>(A + (size_t)(m0 + row) * lda + kk + kc * 8);
+    }
+#pragma unroll
+    for (int t = 0; t < kBChunks; ++t) {
+      int row, kc;
+      chunk_pos(tid + t * 128, row, kc);
+      rb[t] = *reinterpret_cast<const uint4*>(B + (size_t)(n0 + row) * ldb + kk + kc * 8);
+    }
+  };
+  auto store_slice = [&](int s) {
+#pragma unroll
+    for (int t = 0; t < kAChunks; ++t) {
+      int row, kc;
+      chunk_pos(tid + t * 128, row, kc);
+      const int off = (kc >> 1) * (kBM * 32) + (row >> 3) * 256 + (kc & 1) * 128 + (row & 7) * 16;
+      *reinterpret_cast<uint4*>(sA[s] + off) = ra[t];
+    }
+#pragma unroll
+    for (int t = 0; t < kBChunks; ++t) {
+      int row, kc;
+      chunk_pos(tid + t * 128, row, kc);
+      const int off = (kc >> 1) * (BN * 32) + (row >> 3) * 256 + (kc & 1) * 128 + (row & 7) * 16;
+      *reinterpret_cast<uint4*>(sB[s] + off) = rb[t];
+    }
+  };
+
   bool ok = true;
-  int kb_last = 0;
-  const int nk = K / kBK;
+  load_slice(0);
   for (int kb = 0; kb < nk; ++kb) {
-    // A tile: 128 rows x 8 chunks of 8 elements (16 bytes)
-    for (int c = tid; c < kBM * 8; c += 128) {
-      const int m = c >> 3, kc = c & 7;
-      const uint4 v = *reinterpret_cast<const uint4*>(A + (size_t)(m0 + m) * lda + kb * kBK + kc * 8);
-      const int off = (kc >> 1) * (kBM * 32) + (m >> 3) * 256 + (kc & 1) * 128 + (m & 7) * 16;
-      *reinterpret_cast<uint4*>(sA + off) = v;
+    const int s = kb & 1;
+    if (kb >= 2) {  // stage s is free once the MMAs of slice kb-2 completed
+      const int got = mbar_wait(smem_u32(&bar[s]), (uint32_t)(((kb - 2) >> 1) & 1)) ? 1 : 0;
+      if (!__syncthreads_and(got)) {
+        ok = false;
+        break;
+      }
     }
-    for (int c = tid; c < kBN * 8; c += 128) {
-      const int n = c >> 3, kc = c & 7;
-      const uint4 v = *reinterpret_cast<const uint4*>(B + (size_t)(n0 + n) * ldb + kb * kBK + kc * 8);
-      const int off = (kc >> 1) * (kBN * 32) + (n >> 3) * 256 + (kc & 1) * 128 + (n & 7) * 16;
-      *reinterpret_cast<uint4*>(sB + off) = v;
-    }
-    // make the generic-proxy stores visible to the tensor core
+    store_slice(s);
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     __syncthreads();
+    if (kb + 1 < nk) load_slice(kb + 1);
     if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
 #pragma unroll
-      for (int s = 0; s < kBK / 16; ++s) {
-        const uint64_t ad = smem_desc(smem_u32(sA + s * kBM * 32), 128, 256);
-        const uint64_t bd = smem_desc(smem_u32(sB + s * kBN * 32), 128, 256);
-        const uint32_t acc = (kb > 0 || s > 0) ? 1u : 0u;
+      for (int k16 = 0; k16 < kBK / 16; ++k16) {
+        const uint64_t ad = smem_desc(smem_u32(sA[s] + k16 * kBM * 32), 128, 256);
+        const uint64_t bd = smem_desc(smem_u32(sB[s] + k16 * BN * 32), 128, 256);
+        const uint32_t acc = (kb > 0 || k16 > 0) ? 1u : 0u;
         asm volatile(
             "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
             " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
@@ -148,48 +195,63 @@ __global__ void __launch_bounds__(128)
       }
       asm volatile(
           "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
-              bar_a)
+              smem_u32(&bar[s]))
           : "memory");
     }
-    // shared memory is reused only after the MMAs that read it completed;
-    // the outcome of the bounded wait is made block-uniform
-    kb_last = kb;
-    const int got = mbar_wait(bar_a, (uint32_t)(kb & 1)) ? 1 : 0;
-    if (!__syncthreads_and(got)) {
-      ok = false;
-      break;
-    }
+  }
+  if (ok && nk > 0) {  // the last commit covers every earlier MMA
+    const int last = nk - 1;
+    const int got =
+        mbar_wait(smem_u32(&bar[last & 1]), (uint32_t)((last >> 1) & 1)) ? 1 : 0;
+    ok = __syncthreads_and(got) != 0;
   }
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   if (!ok) {
     if (tid == 0) atomicExch(error, 1);
-    // give outstanding MMAs one more bounded wait before the TMEM is freed
-    mbar_wait(bar_a, (uint32_t)(kb_last & 1));
+    // one more bounded wait on both stages before the TMEM is freed
+    mbar_wait(smem_u32(&bar[0]), 0u);
+    mbar_wait(smem_u32(&bar[1]), 0u);
   } else {
-    const int row = m0 + warp * 32 + (tid & 31);
+    const int row = m0 + warp * 32 + lane;
+    float* dst = partial ? partial + (size_t)blockIdx.z * M * N + (size_t)row * N + n0
+                         : C + (size_t)row * ldc + n0;
+    const bool acc = partial == nullptr && accumulate;
 #pragma unroll
-    for (int c0 = 0; c0 < kBN; c0 += 16) {
+    for (int c0 = 0; c0 < BN; c0 += 16) {
       float v[16];
       tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-      if (row < M) {
-        float* dst = C + (size_t)row * ldc + n0 + c0;
 #pragma unroll
-        for (int i = 0; i < 16; ++i) dst[i] = accumulate ? dst[i] + v[i] : v[i];
-      }
+      for (int i = 0; i < 16; ++i) dst[c0 + i] = acc ? dst[c0 + i] + v[i] : v[i];
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();
   if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem),
-                 "r"(kTmemCols));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(BN));
+}
+
+// C (+)= sum_z partial[z] in z order.
+__global__ void k_gemm_reduce(int splits, long long MN, int M, int N, int ldc,
+                              const float* __restrict__ partial, float* __restrict__ C,
+                              int accumulate) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= MN) return;
+  const int m = (int)(t / N), n = (int)(t - (long long)m * N);
+  float acc = accumulate ? C[(size_t)m * ldc + n] : 0.0f;
+  for (int z = 0; z < splits; ++z) acc += partial[(size_t)z * MN + t];
+  C[(size_t)m * ldc + n] = acc;
 }
 
 }  // namespace
 
+extern "C" int64_t cvlbm_gemm_bf16_workspace(int32_t M, int32_t N, int32_t K) {
+  return (int64_t)16 * M * N * (int64_t)sizeof(float);  // up to 16 K splits
+}
+
 extern "C" int cvlbm_gemm_bf16(const void* A, const void* B, float* C, int32_t M, int32_t N,
                                int32_t K, int32_t lda, int32_t ldb, int32_t ldc,
-                               int32_t accumulate, int32_t* error, void* stream) {
+                               int32_t accumulate, int32_t* error, void* workspace,
+                               int64_t workspace_bytes, void* stream) {
   if (!A || !B || !C || !error) return fail(CVLBM_ERR_INVALID_ARG, "cvlbm_gemm_bf16: null pointer");
   if (M <= 0 || N <= 0 || K <= 0 || M % kBM || N % kBN || K % kBK)
     return fail(CVLBM_ERR_INVALID_ARG,
@@ -198,10 +260,38 @@ extern "C" int cvlbm_gemm_bf16(const void* A, const void* B, float* C, int32_t M
     return fail(CVLBM_ERR_INVALID_ARG, "cvlbm_gemm_bf16: bad leading dimensions");
   if ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B)) & 15)
     return fail(CVLBM_ERR_INVALID_ARG, "cvlbm_gemm_bf16: A and B must be 16-byte aligned");
-  dim3 grid(M / kBM, N / kBN);
-  k_gemm_bf16<<<grid, 128, 0, (cudaStream_t)stream>>>(
-      static_cast<const __nv_bfloat16*>(A), static_cast<const __nv_bfloat16*>(B), C, M, N, K,
-      lda, ldb, ldc, accumulate, error);
+  cudaStream_t s = (cudaStream_t)stream;
+  const int bn = (N % 128 == 0) ? 128 : 64;
+  const int tiles = (M / kBM) * (N / bn);
+  // split K until about two CTAs per SM, keeping at least 4 slices per split
+  int splits = 1;
+  const long long nkb = K / kBK;
+  while (splits < 16 && tiles * splits < 296 && nkb % (2 * splits) == 0 &&
+         nkb / (2 * splits) >= 4 &&
+         (long long)(2 * splits) * M * N * (long long)sizeof(float) <= workspace_bytes)
+    splits *= 2;
+  float* part = splits > 1 ? static_cast<float*>(workspace) : nullptr;
+  dim3 grid(M / kBM, N / bn, splits);
+  const int kchunk = K / splits;
+  if (bn == 128) {
+    const size_t smem = 2 * (kBM + 128) * kBK * 2;
+    cudaFuncSetAttribute(k_gemm_bf16<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_gemm_bf16<128><<<grid, 128, smem, s>>>(static_cast<const __nv_bfloat16*>(A),
+                                             static_cast<const __nv_bfloat16*>(B), C, part, M, N,
+                                             kchunk, lda, ldb, ldc, accumulate, error);
+  } else {
+    const size_t smem = 2 * (kBM + 64) * kBK * 2;
+    cudaFuncSetAttribute(k_gemm_bf16<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_gemm_bf16<64><<<grid, 128, smem, s>>>(static_cast<const __nv_bfloat16*>(A),
+                                            static_cast<const __nv_bfloat16*>(B), C, part, M, N,
+                                            kchunk, lda, ldb, ldc, accumulate, error);
+  }
   cv::count_launches(1);
+  if (splits > 1) {
+    const long long MN = (long long)M * N;
+    k_gemm_reduce<<<(unsigned)((MN + 255) / 256), 256, 0, s>>>(splits, MN, M, N, ldc, part, C,
+                                                               accumulate);
+    cv::count_launches(1);
+  }
   return check_launch("cvlbm_gemm_bf16");
 }

@@ -120,6 +120,7 @@ EXPORTED = (
     "cvlbm2d_batch_launch_grid",
     "cvlbm2d_batch_destroy",
     "cvlbm_gemm_bf16",
+    "cvlbm_gemm_bf16_workspace",
     "cvlbm_fno_pointwise_fwd",
     "cvlbm_fno_gelu_bwd",
     "cvlbm_fno_pointwise_bwd",
@@ -179,7 +180,9 @@ def load(require_cuda: bool = True):
                                        C.POINTER(f64), C.POINTER(f64), pI]),
         "cvlbm2d_batch_launch_grid": (i32, [pI, C.POINTER(i32), C.POINTER(i32)]),
         "cvlbm2d_batch_destroy": (None, [pI]),
-        "cvlbm_gemm_bf16": (i32, [pI, pI, pI, i32, i32, i32, i32, i32, i32, i32, pI, pI]),
+        "cvlbm_gemm_bf16": (i32, [pI, pI, pI, i32, i32, i32, i32, i32, i32, i32, pI, pI, i64,
+                                  pI]),
+        "cvlbm_gemm_bf16_workspace": (i64, [i32, i32, i32]),
         "cvlbm_fno_pointwise_fwd": (i32, [i32, i32, i32, i32, pI, pI, pI, pI, i32, pI, pI, pI]),
         "cvlbm_fno_gelu_bwd": (i32, [i64, pI, pI, pI, pI]),
         "cvlbm_fno_pointwise_bwd": (i32, [i32, i32, i32, i32, pI, pI, pI, pI, i32, pI, pI, pI,

@@ -99,6 +99,9 @@ class FNO:
         n_scr = max(int(self._lib.cvlbm_fno_pointwise_scratch(self.B, self.G, ci, co))
                     for ci, co in ((C_IN, C), (C, C), (C, C_OUT)))
         self._scratch = torch.empty(n_scr, dtype=torch.float32, device=self.dev)
+        ws = max(int(self._lib.cvlbm_gemm_bf16_workspace(self.B * self.C, self.M, self.G)),
+                 int(self._lib.cvlbm_gemm_bf16_workspace(self.B * self.C, self.G, self.M)))
+        self._ws = torch.empty(ws // 4, dtype=torch.float32, device=self.dev)
 
     # -- native plumbing --------------------------------------------------------
     def _s(self):
@@ -109,8 +112,9 @@ class FNO:
         N = Bm.shape[0]
         _native.check(self._lib.cvlbm_gemm_bf16(_native.ptr(A), _native.ptr(Bm), _native.ptr(C),
                                                 M, N, K, A.stride(0), Bm.stride(0), C.stride(0),
-                                                accumulate, _native.ptr(self._err), self._s()),
-                      "cvlbm_gemm_bf16")
+                                                accumulate, _native.ptr(self._err),
+                                                _native.ptr(self._ws), self._ws.numel() * 4,
+                                                self._s()), "cvlbm_gemm_bf16")
 
     def _bf16(self, x):
         import torch

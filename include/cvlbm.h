@@ -348,13 +348,16 @@ void cvlbm_graph_destroy(cvlbm_graph *g);
 /* C[M x N] (fp32, row-major, ldc) = A[M x K] . B[N x K]^T, plus the old C when
  * accumulate != 0.  A and B are bf16 (uint16 storage), K-major, 16-byte
  * aligned; M % 128 == 0, N % 64 == 0, K % 64 == 0, lda and ldb multiples of 8.
- * sm_100a tcgen05.mma with fp32 accumulation in tensor memory.  `error` is a
- * device int32 set to 1 if a CTA's MMAs did not complete in time (bounded
- * wait; that CTA's C tile is then not written).  No counterpart in the
- * reference, which has no learned components. */
+ * sm_100a tcgen05.mma with fp32 accumulation in tensor memory.  A device
+ * workspace of cvlbm_gemm_bf16_workspace() bytes (may be NULL / smaller)
+ * lets long-K, few-tile products split K over more CTAs (fp32 partials summed
+ * in a fixed order).  `error` is a device int32 set to 1 if a CTA's MMAs did
+ * not complete in time (bounded wait; that CTA's tile is then not written).
+ * No counterpart in the reference, which has no learned components. */
 int cvlbm_gemm_bf16(const void *A, const void *B, float *C, int32_t M, int32_t N, int32_t K,
                     int32_t lda, int32_t ldb, int32_t ldc, int32_t accumulate, int32_t *error,
-                    void *stream);
+                    void *workspace, int64_t workspace_bytes, void *stream);
+int64_t cvlbm_gemm_bf16_workspace(int32_t M, int32_t N, int32_t K);
 
 /* ------------------------------------------------------------------------ */
 /* Warm-start surrogate (Fourier neural operator): CUDA-core kernels          */
