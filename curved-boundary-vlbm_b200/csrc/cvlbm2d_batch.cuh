@@ -76,7 +76,7 @@ __global__ void __launch_bounds__(kTX * TY, MINB)
   }
 }
 
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 4)
     k_batch_links2(const Inst2* __restrict__ inst, const InstState2* __restrict__ st,
                    const int2* __restrict__ work, int n_work) {
   __shared__ LinkShared2 sh[128 / kLG];

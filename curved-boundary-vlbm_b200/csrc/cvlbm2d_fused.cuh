@@ -619,7 +619,7 @@ __device__ __forceinline__ void link2_group(
   }
 }
 
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 4)
     k_links2g(Ctx2 c, const double* __restrict__ fpost, double* __restrict__ fout,
               const double* __restrict__ U, const double* __restrict__ u, const double* clock,
               double t_host, double offset, int fused, const double* __restrict__ scratch,

@@ -35,6 +35,7 @@ namespace {
 
 constexpr int kBM = 128, kBN = 64, kBK = 64;
 constexpr long long kWaitCycles = 2000000000LL;  // about one second at 2 GHz
+constexpr int kMaxSplits = 64;                    // K splits of one product
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -245,7 +246,7 @@ __global__ void k_gemm_reduce(int splits, long long MN, int M, int N, int ldc,
 }  // namespace
 
 extern "C" int64_t cvlbm_gemm_bf16_workspace(int32_t M, int32_t N, int32_t K) {
-  return (int64_t)16 * M * N * (int64_t)sizeof(float);  // up to 16 K splits
+  return (int64_t)kMaxSplits * M * N * (int64_t)sizeof(float);
 }
 
 extern "C" int cvlbm_gemm_bf16(const void* A, const void* B, float* C, int32_t M, int32_t N,
@@ -266,7 +267,7 @@ extern "C" int cvlbm_gemm_bf16(const void* A, const void* B, float* C, int32_t M
   // split K until about two CTAs per SM, keeping at least 4 slices per split
   int splits = 1;
   const long long nkb = K / kBK;
-  while (splits < 16 && tiles * splits < 296 && nkb % (2 * splits) == 0 &&
+  while (splits < kMaxSplits && tiles * splits < 296 && nkb % (2 * splits) == 0 &&
          nkb / (2 * splits) >= 4 &&
          (long long)(2 * splits) * M * N * (long long)sizeof(float) <= workspace_bytes)
     splits *= 2;
