@@ -42,7 +42,7 @@ def test_two_gloo_ranks_reduce_like_the_bench():
     import torch.multiprocessing as mp
 
     port = _free_port()
-    with mp.Manager() as mgr:
+    with mp.get_context("spawn").Manager() as mgr:
         out = mgr.dict()
         mp.spawn(_worker, args=(2, port, out), nprocs=2, join=True)
         res = dict(out)
