@@ -591,15 +591,12 @@ extern "C" int cvlbm3d_run(const cvlbm3d_problem* p, cvlbm3d_fields* f, double t
           k3_sweep<<<blocks(N, 256), 256, 0, s>>>(c, f->U, f->u_next, f->u, f->u_star, clock, t);
           cv::count_launches(1);
         }
-        k3_prep<<<blocks(N, 128), 128, 0, s>>>(c, fz, f->U, f->u, f->repair_scratch, repair);
+        k3_prep<<<blocks(N, 128), 128, 0, s>>>(c, fz, f->U, f->u, f->repair_scratch, repair,
+                                               k == nsteps - 1);
         cv::count_launches(1);
         k3_collide<<<blocks(N, kCN), kQ3 * kCN, 0, s>>>(c, fz, f->f0, f->f1, f->U,
                                                         f->repair_scratch);
         cv::count_launches(1);
-        if (k == nsteps - 1 && repair) {
-          k3_store_F<<<blocks(N, 256), 256, 0, s>>>(N, f->U, f->repair_scratch);
-          cv::count_launches(1);
-        }
       }
       timer_end(tk, s);
       if (L > 0) {

@@ -7,9 +7,9 @@
 //   k3_sweep     u_swept -> u and the trapezoidal u* update, from U and ucol
 //                of the node and its six neighbours plus cut-point anchors
 //   k3_prep      F repair preparation from U and the swept u (+-2 star
-//                stencil): P(F), and where the repair applies the repaired F
-//                and the change of P; the post-step U of nodes that links
-//                read goes to U_need, one 96-byte row each
+//                stencil): P(F), and where the repair applies the deltas of
+//                P and F; the post-step U of nodes that links read goes to
+//                U_need, one 96-byte row each
 //   k3_collide   f0 again (six warps per 32 nodes, one per direction, no
 //                barriers): BGK collision with damping/source and the repair
 //                delta, push streaming to f1; a population whose neighbour is
@@ -172,13 +172,12 @@ __global__ void __launch_bounds__(256) k3_sweep(Ctx3 c, const double* __restrict
 // F repair preparation (three_d/curved_boundary_warp3d.py:2543-2672), one
 // thread per node, from U (the moments k3_moments stored) and the swept u:
 // P(F), and where the repair applies (det of the repaired F above the floor)
-// P(F_repaired) - P(F) and F_repaired.  rs holds Po[9][N], dP[9][N],
-// Fr[9][N] followed by one flag byte per node.  Also writes the U_need row.
-// U itself keeps the moments until k3_collide has read them; k3_store_F
-// writes the repaired F into U on the last step of a run.
+// P(F_repaired) - P(F) and F_repaired - F.  rs holds Po[9][N], dP[9][N],
+// dF[9][N] followed by one flag byte per node.  Also writes the U_need row
+// and, on the last step of a run, the repaired F into U.
 __global__ void __launch_bounds__(128)
-    k3_prep(Ctx3 c, Fused3 fz, const double* __restrict__ U, const double* __restrict__ u,
-            double* __restrict__ rs, int do_repair) {
+    k3_prep(Ctx3 c, Fused3 fz, double* __restrict__ U, const double* __restrict__ u,
+            double* __restrict__ rs, int do_repair, int store_all) {
   const int N = c.N;
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= N) return;
@@ -190,7 +189,7 @@ __global__ void __launch_bounds__(128)
   const M3 Po = piola3(F, m);
   double* Pog = rs;
   double* dPg = rs + 9 * (size_t)N;
-  double* Frg = rs + 18 * (size_t)N;
+  double* dFg = rs + 18 * (size_t)N;
   uint8_t* flag = reinterpret_cast<uint8_t*>(rs + 27 * (size_t)N);
 #pragma unroll
   for (int k = 0; k < 9; ++k) Pog[(size_t)k * N + n] = Po.v[k];
@@ -213,7 +212,11 @@ __global__ void __launch_bounds__(128)
 #pragma unroll
       for (int k = 0; k < 9; ++k) {
         dPg[(size_t)k * N + n] = Pn.v[k] - Po.v[k];
-        Frg[(size_t)k * N + n] = nn[k];
+        dFg[(size_t)k * N + n] = nn[k] - F[k];
+      }
+      if (store_all) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) U[(size_t)(3 + k) * N + n] = nn[k];
       }
     }
   }
@@ -227,16 +230,6 @@ __global__ void __launch_bounds__(128)
 #pragma unroll
     for (int k = 0; k < 9; ++k) row[3 + k] = repaired ? nn[k] : F[k];
   }
-}
-
-// The repaired F into U (last step of a run, after k3_collide read the
-// moments), so that getters see the reference's post-step U.
-__global__ void __launch_bounds__(256)
-    k3_store_F(int N, double* __restrict__ U, const double* __restrict__ rs) {
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= N || reinterpret_cast<const uint8_t*>(rs + 27 * (size_t)N)[n] == 0) return;
-#pragma unroll
-  for (int k = 0; k < 9; ++k) U[(size_t)(3 + k) * N + n] = rs[(size_t)(18 + k) * N + n];
 }
 
 // Collision + repair delta + push streaming (three_d/curved_boundary_warp3d.py
@@ -276,7 +269,7 @@ __global__ void __launch_bounds__(kQ3 * kCN)
   const double ff = 0.5 / p.c;
   const double sx = (double)dx3(q), sy = (double)dy3(q), sz = (double)dz3(q);
   const double* dP = rs + 9 * (size_t)N;
-  const double* Fr = rs + 18 * (size_t)N;
+  const double* dF = rs + 18 * (size_t)N;
 #pragma unroll
   for (int a = 0; a < kC3; ++a) {
     const double old = v[a];
@@ -287,7 +280,7 @@ __global__ void __launch_bounds__(kQ3 * kCN)
         val = val - ff * (sx * dP[(size_t)(3 * a) * N + n] + sy * dP[(size_t)(3 * a + 1) * N + n] +
                           sz * dP[(size_t)(3 * a + 2) * N + n]);
       else
-        val = val + sixth * (Fr[(size_t)(a - 3) * N + n] - S[a]);
+        val = val + sixth * dF[(size_t)(a - 3) * N + n];
     }
     if (nq >= 0)
       f1[(size_t)(q * kC3 + a) * N + nq] = val;

@@ -280,9 +280,8 @@ typedef struct cvlbm3d_fields {
                                leaving through each cut link */
   double *U_need;           /* [n_need*12] fused step: post-step U of the nodes cut
                                links read, one 96-byte row per node */
-  double *repair_scratch;   /* [28*n_active] fused step: P(F), the repair's change of P
-                               and repaired F (27 x n_active doubles), a flag byte
-                               per node */
+  double *repair_scratch;   /* [28*n_active] fused step: P(F), the repair deltas of P
+                               and F (27 x n_active doubles) and a flag byte per node */
 } cvlbm3d_fields;
 
 /* Replaces WarpSparseCurvedBoundaryLBM3D.step
