@@ -542,7 +542,7 @@ int check_problem(const cvlbm3d_problem* p, const cvlbm3d_fields* f) {
 // The fused pipeline needs its link tables and scratch, and one sweep per
 // due step (several sweeps per step take the per-phase pipeline).
 bool fused_ok3(const cvlbm3d_problem* p, const cvlbm3d_fields* f) {
-  if (!p->need_slot || !f->repair_scratch || p->disp_sweeps > 1) return false;
+  if (!p->need_slot || p->disp_sweeps > 1) return false;
   if (p->n_links > 0) {
     if (!p->link_partner || !f->link_scratch || !f->U_need || p->n_need <= 0 ||
         !f->link_kind || !f->link_comp_kind || !f->link_bv || !f->link_Fb || !f->link_Pb)
@@ -591,11 +591,8 @@ extern "C" int cvlbm3d_run(const cvlbm3d_problem* p, cvlbm3d_fields* f, double t
           k3_sweep<<<blocks(N, 256), 256, 0, s>>>(c, f->U, f->u_next, f->u, f->u_star, clock, t);
           cv::count_launches(1);
         }
-        k3_prep<<<blocks(N, 128), 128, 0, s>>>(c, fz, f->U, f->u, f->repair_scratch, repair,
-                                               k == nsteps - 1);
-        cv::count_launches(1);
-        k3_collide<<<blocks(N, kCN), kQ3 * kCN, 0, s>>>(c, fz, f->f0, f->f1, f->U,
-                                                        f->repair_scratch);
+        k3_collide<<<blocks(N, kCN), kQ3 * kCN, 0, s>>>(c, fz, f->f0, f->f1, f->U, f->u, repair,
+                                                        k == nsteps - 1);
         cv::count_launches(1);
       }
       timer_end(tk, s);

@@ -6,20 +6,17 @@
 //                (u_next), invalid flag; when no sweep is due, u and u* too
 //   k3_sweep     u_swept -> u and the trapezoidal u* update, from U and ucol
 //                of the node and its six neighbours plus cut-point anchors
-//   k3_prep      F repair preparation from U and the swept u (+-2 star
-//                stencil): P(F), and where the repair applies the deltas of
-//                P and F; the post-step U of nodes that links read goes to
-//                U_need, one 96-byte row each
-//   k3_collide   f0 again (six warps per 32 nodes, one per direction, no
-//                barriers): BGK collision with damping/source and the repair
-//                delta, push streaming to f1; a population whose neighbour is
-//                not active leaves through a cut link and is kept per link
-//                (link_scratch) for the link kernels
+//   k3_collide   f0 again (six warps per 32 nodes, one per direction):
+//                moments, F repair from the swept u (+-2 star stencil), BGK
+//                collision with damping/source, repair delta and push
+//                streaming to f1; a population whose neighbour is not active
+//                leaves through a cut link and is kept per link
+//                (link_scratch) for the link kernels; the post-step U of
+//                nodes that links read goes to U_need, one 96-byte row each
 // Per active node this reads f0 twice and writes f1 once (the f0 re-read of
 // k3_collide is what a single-pass 3-D fusion would save; its 3-deep halo
-// does not fit shared memory), plus U, u, u* and the 27 repair doubles:
-// about 2.8 KB per node against the algorithmic 1.2 KB, every kernel a
-// stream of independent coalesced loads.
+// does not fit shared memory), plus U, u and u* (about 2.1 KB per node
+// against the algorithmic 1.2 KB).
 //
 // Link kernels (the four phases of apply_boundary_reconstruction,
 // three_d/curved_boundary_warp3d.py:4339-4399):
@@ -169,94 +166,189 @@ __global__ void __launch_bounds__(256) k3_sweep(Ctx3 c, const double* __restrict
   }
 }
 
-// F repair preparation (three_d/curved_boundary_warp3d.py:2543-2672), one
-// thread per node, from U (the moments k3_moments stored) and the swept u:
-// P(F), and where the repair applies (det of the repaired F above the floor)
-// P(F_repaired) - P(F) and F_repaired - F.  rs holds Po[9][N], dP[9][N],
-// dF[9][N] followed by one flag byte per node.  Also writes the U_need row
-// and, on the last step of a run, the repaired F into U.
-__global__ void __launch_bounds__(128)
-    k3_prep(Ctx3 c, Fused3 fz, double* __restrict__ U, const double* __restrict__ u,
-            double* __restrict__ rs, int do_repair, int store_all) {
+// Collision + F repair + push streaming (three_d/curved_boundary_warp3d.py
+// :2192-2330, 2543-2672).  `u` is the swept displacement of every node.
+//
+// A block takes 32 consecutive active nodes with six warps, warp q owning
+// direction q (lane = node), so every population load and store is one
+// coalesced 256-byte row:
+//   1  warp q loads f0[q][0..11] of its 32 nodes (kept in registers, copied
+//      to shared memory for the moments)
+//   2  moments (summed over q in order) and the nine targets of I + grad u
+//      (+-2 star stencil of the swept u), spread over the block
+//   3  P(F) and P(F_repaired), one row per warp (six rows), U / U_need rows
+//   4  warp q: collision, repair delta and push of direction q
+constexpr int kCN = 32;  // nodes per collide block (one per lane)
+
+struct CollideSmem3 {
+  double f[kQ3][kC3][kCN];
+  double un[kQ3][3][kCN];  // swept u of the neighbour in direction q
+  double u0[3][kCN];       // swept u of the node
+  int nb[kQ3][kCN];        // neighbour in direction q, -1 if not active
+  double S[kC3][kCN];
+  double T[9][kCN];   // I + grad u
+  double Po[9][kCN];  // P(F)
+  double Pn[9][kCN];  // P(F_repaired)
+  double dF[9][kCN];  // F_repaired - F
+  int rep[kCN];
+};
+
+// feq of (q, a) with the moments and P(F) of lane `l` in shared memory; the
+// same operations as feq3 (zero-weight axes included).
+__device__ __forceinline__ double feq3_smem(int q, int a, const CollideSmem3& sm, int l,
+                                            double three_over_c, double sixth) {
+  const double sx = (double)dx3(q), sy = (double)dy3(q), sz = (double)dz3(q);
+  double f0, f1, f2;
+  if (a < 3) {
+    f0 = -sm.Po[3 * a][l];
+    f1 = -sm.Po[3 * a + 1][l];
+    f2 = -sm.Po[3 * a + 2][l];
+  } else {
+    const int r = a - 3, ax = r % 3;
+    const double v = -sm.S[r / 3][l];
+    f0 = ax == 0 ? v : 0.0;
+    f1 = ax == 1 ? v : 0.0;
+    f2 = ax == 2 ? v : 0.0;
+  }
+  return sixth * (sm.S[a][l] + three_over_c * (sx * f0 + sy * f1 + sz * f2));
+}
+
+__global__ void __launch_bounds__(kQ3 * kCN, 4)
+    k3_collide(Ctx3 c, Fused3 fz, const double* __restrict__ f0, double* __restrict__ f1,
+               double* __restrict__ U, const double* __restrict__ u, int do_repair,
+               int store_all) {
+  __shared__ CollideSmem3 sm;
   const int N = c.N;
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= N) return;
   const cvlbm3d_problem& p = c.p;
   const Mat& m = c.m;
-  double F[9];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int n0 = blockIdx.x * kCN;
+  const int n = n0 + lane;
+  const bool live = n < N;
+
+  // 1: populations of direction `warp`, its neighbour and (for the repair)
+  // the neighbour's swept u
+  double v[kC3];
+  const int q = warp;
 #pragma unroll
-  for (int k = 0; k < 9; ++k) F[k] = U[(size_t)(3 + k) * N + n];
-  const M3 Po = piola3(F, m);
-  double* Pog = rs;
-  double* dPg = rs + 9 * (size_t)N;
-  double* dFg = rs + 18 * (size_t)N;
-  uint8_t* flag = reinterpret_cast<uint8_t*>(rs + 27 * (size_t)N);
-#pragma unroll
-  for (int k = 0; k < 9; ++k) Pog[(size_t)k * N + n] = Po.v[k];
-  bool repaired = false;
-  double nn[9];
+  for (int a = 0; a < kC3; ++a) v[a] = live ? f0[(size_t)(q * kC3 + a) * N + n] : 0.0;
+  const int nq = live ? p.neighbor[(size_t)q * N + n] : -1;
   if (do_repair) {
-    const double beta = fmax(0.0, fmin(1.0, p.blend));
-    const double h[3] = {p.dx, p.dy, p.dz};
 #pragma unroll
     for (int comp = 0; comp < 3; ++comp)
+      sm.un[q][comp][lane] = nq >= 0 ? u[(size_t)comp * N + nq] : 0.0;
+    if (warp < 3) sm.u0[warp][lane] = live ? u[(size_t)warp * N + n] : 0.0;
+  }
 #pragma unroll
-      for (int ax = 0; ax < 3; ++ax) {
-        const double g = du_axis3(u + (size_t)comp * N, p.neighbor, N, n, ax, ax + 3, h[ax]);
-        const double t = comp == ax ? 1.0 + g : g;
-        nn[3 * comp + ax] = F[3 * comp + ax] + beta * (t - F[3 * comp + ax]);
+  for (int a = 0; a < kC3; ++a) sm.f[q][a][lane] = v[a];
+  sm.nb[q][lane] = nq;
+  __syncthreads();
+
+  // 2: moments (12 x 32 sums) and I + grad u (9 x 32 targets)
+  const double hdt = 0.5 * p.dt;
+  for (int t = threadIdx.x; t < kC3 * kCN; t += blockDim.x) {
+    const int a = t / kCN, l = t % kCN;
+    double sacc = 0.0;
+#pragma unroll
+    for (int qq = 0; qq < kQ3; ++qq) sacc += sm.f[qq][a][l];
+    if (p.source_mode == kSrcConstant) {
+      sacc += hdt * p.source[a];
+    } else if (p.source_mode == kSrcDamping && a < 3) {
+      const double den = 1.0 + hdt * p.source[0];
+      sacc = sacc / den;
+    }
+    sm.S[a][l] = sacc;
+  }
+  if (do_repair) {
+    // derivative of the swept u along each axis, as du_axis3: centred with
+    // both neighbours, second-order one-sided with two on one side, first
+    // order with one, zero with none
+    const double h[3] = {p.dx, p.dy, p.dz};
+    for (int t = threadIdx.x; t < 9 * kCN; t += blockDim.x) {
+      const int k = t / kCN, l = t % kCN, comp = k / 3, ax = k % 3;
+      const int pp = sm.nb[ax][l], pm = sm.nb[ax + 3][l];
+      const double* uc = u + (size_t)comp * N;
+      const double hh = h[ax];
+      double g = 0.0;
+      if (n0 + l < N) {
+        if (pp >= 0 && pm >= 0) {
+          g = (sm.un[ax][comp][l] - sm.un[ax + 3][comp][l]) / (2.0 * hh);
+        } else if (pp >= 0) {
+          const int pp2 = p.neighbor[(size_t)ax * N + pp];
+          if (pp2 >= 0)
+            g = (-3.0 * sm.u0[comp][l] + 4.0 * sm.un[ax][comp][l] - uc[pp2]) / (2.0 * hh);
+          else
+            g = (sm.un[ax][comp][l] - sm.u0[comp][l]) / hh;
+        } else if (pm >= 0) {
+          const int pm2 = p.neighbor[(size_t)(ax + 3) * N + pm];
+          if (pm2 >= 0)
+            g = (3.0 * sm.u0[comp][l] - 4.0 * sm.un[ax + 3][comp][l] + uc[pm2]) / (2.0 * hh);
+          else
+            g = (sm.u0[comp][l] - sm.un[ax + 3][comp][l]) / hh;
+        }
       }
-    if (det3v(nn) > m.jf) {
-      repaired = true;
-      const M3 Pn = piola3(nn, m);
+      sm.T[k][l] = comp == ax ? 1.0 + g : g;
+    }
+  }
+  __syncthreads();
+
+  // 3: P(F) and P(F_repaired), one row of each per warp: warps 0-2 row
+  // `warp` of P(F), warps 3-5 row `warp - 3` of the repaired F and its Piola;
+  // warp 3 also writes the repaired flag and the U / U_need rows
+  {
+    const int row = warp < 3 ? warp : warp - 3;
+    double F[9];
 #pragma unroll
-      for (int k = 0; k < 9; ++k) {
-        dPg[(size_t)k * N + n] = Pn.v[k] - Po.v[k];
-        dFg[(size_t)k * N + n] = nn[k] - F[k];
+    for (int k = 0; k < 9; ++k) F[k] = sm.S[3 + k][lane];
+    if (warp < 3) {
+      double Pr[3];
+      piola3_row(F, m, row, Pr);
+#pragma unroll
+      for (int c2 = 0; c2 < 3; ++c2) sm.Po[3 * row + c2][lane] = Pr[c2];
+    } else {
+      bool repaired = false;
+      double nn[9];
+      if (do_repair) {
+        const double beta = fmax(0.0, fmin(1.0, p.blend));
+#pragma unroll
+        for (int k = 0; k < 9; ++k) nn[k] = F[k] + beta * (sm.T[k][lane] - F[k]);
+        if (det3v(nn) > m.jf) {
+          repaired = true;
+          double Pr[3];
+          piola3_row(nn, m, row, Pr);
+#pragma unroll
+          for (int c2 = 0; c2 < 3; ++c2) {
+            sm.Pn[3 * row + c2][lane] = Pr[c2];
+            sm.dF[3 * row + c2][lane] = nn[3 * row + c2] - F[3 * row + c2];
+          }
+        }
       }
-      if (store_all) {
+      if (warp == 3) {
+        sm.rep[lane] = repaired ? 1 : 0;
+        if (repaired && store_all && live) {
 #pragma unroll
-        for (int k = 0; k < 9; ++k) U[(size_t)(3 + k) * N + n] = nn[k];
+          for (int k = 0; k < 9; ++k) U[(size_t)(3 + k) * N + n] = nn[k];
+        }
+        const int slot = live ? fz.need_slot[n] : -1;
+        if (slot >= 0) {
+          double* rowp = fz.Uneed + (size_t)slot * kC3;
+          rowp[0] = sm.S[0][lane];
+          rowp[1] = sm.S[1][lane];
+          rowp[2] = sm.S[2][lane];
+#pragma unroll
+          for (int k = 0; k < 9; ++k) rowp[3 + k] = repaired ? nn[k] : F[k];
+        }
       }
     }
   }
-  flag[n] = repaired ? 1 : 0;
-  const int slot = fz.need_slot[n];
-  if (slot >= 0) {
-    double* row = fz.Uneed + (size_t)slot * kC3;
-    row[0] = U[n];
-    row[1] = U[(size_t)N + n];
-    row[2] = U[2 * (size_t)N + n];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) row[3 + k] = repaired ? nn[k] : F[k];
-  }
-}
+  __syncthreads();
+  if (!live) return;
 
-// Collision + repair delta + push streaming (three_d/curved_boundary_warp3d.py
-// :2192-2330).  32 consecutive nodes x 6 warps, warp q = direction q (lane =
-// node), so every population load and store is a coalesced 256-byte row; the
-// moments come from U (bitwise the sums k3_moments stored), P(F) and the
-// repair deltas from k3_prep.  No shared memory and no block barrier.
-constexpr int kCN = 32;  // nodes per collide block (one per lane)
-
-__global__ void __launch_bounds__(kQ3 * kCN)
-    k3_collide(Ctx3 c, Fused3 fz, const double* __restrict__ f0, double* __restrict__ f1,
-               const double* __restrict__ U, const double* __restrict__ rs) {
-  const int N = c.N;
-  const cvlbm3d_problem& p = c.p;
-  const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
-  const int n = blockIdx.x * kCN + lane;
-  if (n >= N) return;
-  double v[kC3], S[kC3];
-#pragma unroll
-  for (int a = 0; a < kC3; ++a) v[a] = f0[(size_t)(q * kC3 + a) * N + n];
-#pragma unroll
-  for (int a = 0; a < kC3; ++a) S[a] = U[(size_t)a * N + n];
-  const int nq = p.neighbor[(size_t)q * N + n];
-  const bool repaired = reinterpret_cast<const uint8_t*>(rs + 27 * (size_t)N)[n] != 0;
-  M3 Po;
-#pragma unroll
-  for (int k = 0; k < 9; ++k) Po.v[k] = rs[(size_t)k * N + n];
+  // 4: collision, repair delta, push of direction q
+  const double k3c = 3.0 / p.c, sixth = 1.0 / 6.0, om = p.omega;
+  const double sw = p.dt * (2.0 - om) * (1.0 / 12.0);
+  const double ff = 0.5 / p.c;
+  const bool repaired = sm.rep[lane] != 0;
   int ell = -1;
   if (nq < 0) {
     for (int k = p.node_link_start[n]; k < p.node_link_start[n + 1]; ++k) {
@@ -264,23 +356,20 @@ __global__ void __launch_bounds__(kQ3 * kCN)
       if (p.link_q[e] == q) ell = e;
     }
   }
-  const double k3c = 3.0 / p.c, sixth = 1.0 / 6.0, om = p.omega;
-  const double sw = p.dt * (2.0 - om) * (1.0 / 12.0);
-  const double ff = 0.5 / p.c;
   const double sx = (double)dx3(q), sy = (double)dy3(q), sz = (double)dz3(q);
-  const double* dP = rs + 9 * (size_t)N;
-  const double* dF = rs + 18 * (size_t)N;
+  const double vel[3] = {sm.S[0][lane], sm.S[1][lane], sm.S[2][lane]};
 #pragma unroll
   for (int a = 0; a < kC3; ++a) {
     const double old = v[a];
-    const double fe = feq3(q, a, S, Po, k3c, sixth);
-    double val = old + om * (fe - old) + sw * source_comp3(a, p.source_mode, p.source, S);
+    const double fe = feq3_smem(q, a, sm, lane, k3c, sixth);
+    double val = old + om * (fe - old) + sw * source_comp3(a, p.source_mode, p.source, vel);
     if (repaired) {
       if (a < 3)
-        val = val - ff * (sx * dP[(size_t)(3 * a) * N + n] + sy * dP[(size_t)(3 * a + 1) * N + n] +
-                          sz * dP[(size_t)(3 * a + 2) * N + n]);
+        val = val - ff * (sx * (sm.Pn[3 * a][lane] - sm.Po[3 * a][lane]) +
+                          sy * (sm.Pn[3 * a + 1][lane] - sm.Po[3 * a + 1][lane]) +
+                          sz * (sm.Pn[3 * a + 2][lane] - sm.Po[3 * a + 2][lane]));
       else
-        val = val + sixth * dF[(size_t)(a - 3) * N + n];
+        val = val + sixth * sm.dF[a - 3][lane];
     }
     if (nq >= 0)
       f1[(size_t)(q * kC3 + a) * N + nq] = val;

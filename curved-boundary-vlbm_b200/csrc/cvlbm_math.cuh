@@ -255,6 +255,40 @@ CV_DEV M3 piola3(const double* F, const Mat& m) {
   return P;
 }
 
+// Row r (entries 3r..3r+2) of piola3(F, m), with the same operations for the
+// neo-Hooke law (cofactor / J per entry); other laws evaluate the full tensor.
+CV_DEV void piola3_row(const double* F, const Mat& m, int r, double* out) {
+  if (m.model != kMatNeoHooke) {
+    const M3 P = piola3(F, m);
+    out[0] = P.v[3 * r];
+    out[1] = P.v[3 * r + 1];
+    out[2] = P.v[3 * r + 2];
+    return;
+  }
+  const double F11 = F[0], F12 = F[1], F13 = F[2], F21 = F[3], F22 = F[4], F23 = F[5],
+               F31 = F[6], F32 = F[7], F33 = F[8];
+  const double J = clamp_j(det3(F11, F12, F13, F21, F22, F23, F31, F32, F33), m.jf);
+  double c0, c1, c2;
+  if (r == 0) {
+    c0 = F22 * F33 - F23 * F32;
+    c1 = F23 * F31 - F21 * F33;
+    c2 = F21 * F32 - F22 * F31;
+  } else if (r == 1) {
+    c0 = F13 * F32 - F12 * F33;
+    c1 = F11 * F33 - F13 * F31;
+    c2 = F12 * F31 - F11 * F32;
+  } else {
+    c0 = F12 * F23 - F13 * F22;
+    c1 = F13 * F21 - F11 * F23;
+    c2 = F11 * F22 - F12 * F21;
+  }
+  const double h0 = c0 / J, h1 = c1 / J, h2 = c2 / J;
+  const double vol = 0.5 * m.lam * (J * J - 1.0);
+  out[0] = m.mu * (F[3 * r] - h0) + vol * h0;
+  out[1] = m.mu * (F[3 * r + 1] - h1) + vol * h1;
+  out[2] = m.mu * (F[3 * r + 2] - h2) + vol * h2;
+}
+
 // ---------------------------------------------------------------------------
 // Lattice helpers.
 // ---------------------------------------------------------------------------

@@ -87,7 +87,7 @@ class Fields3D(C.Structure):
     _fields_ = [(name, pI) for name in
                 ("f0", "f1", "U", "u", "u_next", "u_star", "link_kind", "link_comp_kind",
                  "link_bv", "link_Fb", "link_Pb", "char_state", "invalid", "clock",
-                 "link_scratch", "U_need", "repair_scratch")]
+                 "link_scratch", "U_need")]
 
 
 EXPORTED = (

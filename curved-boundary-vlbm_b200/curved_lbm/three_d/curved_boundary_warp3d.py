@@ -398,7 +398,6 @@ class WarpSparseCurvedBoundaryLBM3D:
         self._clock = torch.zeros(1, dtype=f64, device=dev)
         self.link_scratch = torch.zeros(max(1, 12 * nl), dtype=f64, device=dev)
         self.U_need = torch.zeros(max(1, 12 * self._n_need), dtype=f64, device=dev)
-        self.repair_scratch = torch.zeros(28 * max(1, self.n_active), dtype=f64, device=dev)
         self.source_params_wp = self.source_params.copy()
         self._problem = self._make_problem()
         self.initialize_identity()
@@ -445,8 +444,7 @@ class WarpSparseCurvedBoundaryLBM3D:
                              ("link_Pb", self.link_Pb),
                              ("char_state", self.char_state if has_char else None),
                              ("invalid", self.invalid), ("clock", self._clock),
-                             ("link_scratch", self.link_scratch), ("U_need", self.U_need),
-                             ("repair_scratch", self.repair_scratch)):
+                             ("link_scratch", self.link_scratch), ("U_need", self.U_need)):
             setattr(fl, name, _native.ptr(tensor))
         return fl
 

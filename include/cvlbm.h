@@ -252,8 +252,7 @@ typedef struct cvlbm3d_problem {
   const int32_t *dyn_enabled;                     /* [n_links] */
   const double *dyn_traction;                     /* [3*n_links] */
   /* fused step (optional; need_slot, link_partner and fields->link_scratch,
-     fields->U_need, fields->repair_scratch all set enable it when
-     disp_sweeps <= 1) */
+     fields->U_need all set enable it when disp_sweeps <= 1) */
   const int32_t *need_slot;                       /* [n_active] row of U_need holding the
                                                      node's post-step U, or -1 */
   int32_t n_need;                                 /* rows of U_need */
@@ -280,8 +279,6 @@ typedef struct cvlbm3d_fields {
                                leaving through each cut link */
   double *U_need;           /* [n_need*12] fused step: post-step U of the nodes cut
                                links read, one 96-byte row per node */
-  double *repair_scratch;   /* [28*n_active] fused step: P(F), the repair deltas of P
-                               and F (27 x n_active doubles) and a flag byte per node */
 } cvlbm3d_fields;
 
 /* Replaces WarpSparseCurvedBoundaryLBM3D.step
