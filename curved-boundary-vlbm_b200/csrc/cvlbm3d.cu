@@ -578,20 +578,6 @@ extern "C" int cvlbm3d_run(const cvlbm3d_problem* p, cvlbm3d_fields* f, double t
     Fused3 fz{p->need_slot, p->char_slot, p->link_partner, p->link_order, f->link_scratch,
               f->U_need};
     const int L = p->n_links;
-    using CollideFn = void (*)(Ctx3, Fused3, const double*, double*, double*, const double*,
-                               int, int);
-    const CollideFn collide =
-        p->mat.model == kMatNeoHooke ? (CollideFn)k3_collide<true> : (CollideFn)k3_collide<false>;
-    cudaFuncSetAttribute(collide, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)sizeof(CollideSmem3));
-    int dev = 0, sms = 148, per_sm = 1;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, collide, kQ3 * kCN,
-                                                  sizeof(CollideSmem3));
-    const int groups = (N + kCN - 1) / kCN;
-    int collide_grid = sms * (per_sm > 0 ? per_sm : 1);
-    if (collide_grid > groups) collide_grid = groups > 0 ? groups : 1;
     for (int k = 0; k < nsteps; ++k) {
       const long long step = step0 + k;
       const int sweep = N > 0 && due(p->disp_interval, step);
@@ -605,8 +591,8 @@ extern "C" int cvlbm3d_run(const cvlbm3d_problem* p, cvlbm3d_fields* f, double t
           k3_sweep<<<blocks(N, 256), 256, 0, s>>>(c, f->U, f->u_next, f->u, f->u_star, clock, t);
           cv::count_launches(1);
         }
-        collide<<<collide_grid, kQ3 * kCN, sizeof(CollideSmem3), s>>>(
-            c, fz, f->f0, f->f1, f->U, f->u, repair, k == nsteps - 1);
+        k3_collide<<<blocks(N, kCN), kQ3 * kCN, 0, s>>>(c, fz, f->f0, f->f1, f->U, f->u, repair,
+                                                        k == nsteps - 1);
         cv::count_launches(1);
       }
       timer_end(tk, s);

@@ -172,9 +172,8 @@ __global__ void __launch_bounds__(256) k3_sweep(Ctx3 c, const double* __restrict
 // A block takes 32 consecutive active nodes with six warps, warp q owning
 // direction q (lane = node), so every population load and store is one
 // coalesced 256-byte row:
-//   1  warp q takes f0[q][0..11] of its 32 nodes from the shared-memory
-//      buffer the previous iteration filled (cp.async) and starts the copy of
-//      the next group's populations into the other buffer
+//   1  warp q loads f0[q][0..11] of its 32 nodes (kept in registers, copied
+//      to shared memory for the moments)
 //   2  moments (summed over q in order) and the nine targets of I + grad u
 //      (+-2 star stencil of the swept u), spread over the block
 //   3  P(F) and P(F_repaired), one row per warp (six rows), U / U_need rows
@@ -182,10 +181,10 @@ __global__ void __launch_bounds__(256) k3_sweep(Ctx3 c, const double* __restrict
 constexpr int kCN = 32;  // nodes per collide block (one per lane)
 
 struct CollideSmem3 {
-  double fb[2][kQ3][kC3][kCN];  // populations of the current / next node group
-  int nbb[2][kQ3][kCN];         // neighbour in direction q, -1 if not active
+  double f[kQ3][kC3][kCN];
   double un[kQ3][3][kCN];  // swept u of the neighbour in direction q
   double u0[3][kCN];       // swept u of the node
+  int nb[kQ3][kCN];        // neighbour in direction q, -1 if not active
   double S[kC3][kCN];
   double T[9][kCN];   // I + grad u
   double Po[9][kCN];  // P(F)
@@ -214,75 +213,35 @@ __device__ __forceinline__ double feq3_smem(int q, int a, const CollideSmem3& sm
   return sixth * (sm.S[a][l] + three_over_c * (sx * f0 + sy * f1 + sz * f2));
 }
 
-// cp.async of the populations and neighbour ids of node group g (32 nodes)
-// into buffer b: warp q copies direction q.
-__device__ __forceinline__ void collide_prefetch(CollideSmem3& sm, int b, int g, int q, int lane,
-                                                 const double* __restrict__ f0,
-                                                 const int32_t* __restrict__ nbr, int N) {
-  const int n = g * kCN + lane;
-  if (n < N) {
-#pragma unroll
-    for (int a = 0; a < kC3; ++a) {
-      const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&sm.fb[b][q][a][lane]);
-      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst),
-                   "l"(f0 + (size_t)(q * kC3 + a) * N + n)
-                   : "memory");
-    }
-    const uint32_t dn = (uint32_t)__cvta_generic_to_shared(&sm.nbb[b][q][lane]);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dn),
-                 "l"(nbr + (size_t)q * N + n)
-                 : "memory");
-  } else {
-#pragma unroll
-    for (int a = 0; a < kC3; ++a) sm.fb[b][q][a][lane] = 0.0;
-    sm.nbb[b][q][lane] = -1;
-  }
-  asm volatile("cp.async.commit_group;\n" ::: "memory");
-}
-
-// Persistent: block b takes node groups b, b + gridDim.x, ...; while one
-// group is processed the populations of the next are copied into the other
-// shared-memory buffer (cp.async), so the loads overlap the arithmetic.
-// NH: compiled for the neo-Hooke law only (its Piola rows need no other
-// branch), the production material; other laws take NH = false.
-template <bool NH>
 __global__ void __launch_bounds__(kQ3 * kCN, 4)
     k3_collide(Ctx3 c, Fused3 fz, const double* __restrict__ f0, double* __restrict__ f1,
                double* __restrict__ U, const double* __restrict__ u, int do_repair,
                int store_all) {
-  extern __shared__ __align__(16) uint8_t smem3[];
-  CollideSmem3& sm = *reinterpret_cast<CollideSmem3*>(smem3);
+  __shared__ CollideSmem3 sm;
   const int N = c.N;
   const cvlbm3d_problem& p = c.p;
   const Mat& m = c.m;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int q = warp;
-  const int ngroups = (N + kCN - 1) / kCN;
-  int cur = 0;
-  if ((int)blockIdx.x < ngroups) collide_prefetch(sm, 0, blockIdx.x, q, lane, f0, p.neighbor, N);
-  for (int g = blockIdx.x; g < ngroups; g += gridDim.x) {
-    asm volatile("cp.async.wait_all;\n" ::: "memory");
-    __syncthreads();
-    const int n0 = g * kCN;
-    const int n = n0 + lane;
-    const bool live = n < N;
-    double(*fcur)[kC3][kCN] = sm.fb[cur];
-    int(*nbcur)[kCN] = sm.nbb[cur];
+  const int n0 = blockIdx.x * kCN;
+  const int n = n0 + lane;
+  const bool live = n < N;
 
-  // 1: populations of direction `warp` (prefetched), its neighbour and (for
-  // the repair) the neighbour's swept u
+  // 1: populations of direction `warp`, its neighbour and (for the repair)
+  // the neighbour's swept u
   double v[kC3];
+  const int q = warp;
 #pragma unroll
-  for (int a = 0; a < kC3; ++a) v[a] = fcur[q][a][lane];
-  const int nq = nbcur[q][lane];
+  for (int a = 0; a < kC3; ++a) v[a] = live ? f0[(size_t)(q * kC3 + a) * N + n] : 0.0;
+  const int nq = live ? p.neighbor[(size_t)q * N + n] : -1;
   if (do_repair) {
 #pragma unroll
     for (int comp = 0; comp < 3; ++comp)
       sm.un[q][comp][lane] = nq >= 0 ? u[(size_t)comp * N + nq] : 0.0;
     if (warp < 3) sm.u0[warp][lane] = live ? u[(size_t)warp * N + n] : 0.0;
   }
-  if (g + (int)gridDim.x < ngroups)
-    collide_prefetch(sm, cur ^ 1, g + gridDim.x, q, lane, f0, p.neighbor, N);
+#pragma unroll
+  for (int a = 0; a < kC3; ++a) sm.f[q][a][lane] = v[a];
+  sm.nb[q][lane] = nq;
   __syncthreads();
 
   // 2: moments (12 x 32 sums) and I + grad u (9 x 32 targets)
@@ -291,7 +250,7 @@ __global__ void __launch_bounds__(kQ3 * kCN, 4)
     const int a = t / kCN, l = t % kCN;
     double sacc = 0.0;
 #pragma unroll
-    for (int qq = 0; qq < kQ3; ++qq) sacc += fcur[qq][a][l];
+    for (int qq = 0; qq < kQ3; ++qq) sacc += sm.f[qq][a][l];
     if (p.source_mode == kSrcConstant) {
       sacc += hdt * p.source[a];
     } else if (p.source_mode == kSrcDamping && a < 3) {
@@ -307,7 +266,7 @@ __global__ void __launch_bounds__(kQ3 * kCN, 4)
     const double h[3] = {p.dx, p.dy, p.dz};
     for (int t = threadIdx.x; t < 9 * kCN; t += blockDim.x) {
       const int k = t / kCN, l = t % kCN, comp = k / 3, ax = k % 3;
-      const int pp = nbcur[ax][l], pm = nbcur[ax + 3][l];
+      const int pp = sm.nb[ax][l], pm = sm.nb[ax + 3][l];
       const double* uc = u + (size_t)comp * N;
       const double hh = h[ax];
       double g = 0.0;
@@ -343,7 +302,7 @@ __global__ void __launch_bounds__(kQ3 * kCN, 4)
     for (int k = 0; k < 9; ++k) F[k] = sm.S[3 + k][lane];
     if (warp < 3) {
       double Pr[3];
-      piola3_row<NH>(F, m, row, Pr);
+      piola3_row(F, m, row, Pr);
 #pragma unroll
       for (int c2 = 0; c2 < 3; ++c2) sm.Po[3 * row + c2][lane] = Pr[c2];
     } else {
@@ -356,7 +315,7 @@ __global__ void __launch_bounds__(kQ3 * kCN, 4)
         if (det3v(nn) > m.jf) {
           repaired = true;
           double Pr[3];
-          piola3_row<NH>(nn, m, row, Pr);
+          piola3_row(nn, m, row, Pr);
 #pragma unroll
           for (int c2 = 0; c2 < 3; ++c2) {
             sm.Pn[3 * row + c2][lane] = Pr[c2];
@@ -383,7 +342,7 @@ __global__ void __launch_bounds__(kQ3 * kCN, 4)
     }
   }
   __syncthreads();
-  if (live) {
+  if (!live) return;
 
   // 4: collision, repair delta, push of direction q
   const double k3c = 3.0 / p.c, sixth = 1.0 / 6.0, om = p.omega;
@@ -416,9 +375,6 @@ __global__ void __launch_bounds__(kQ3 * kCN, 4)
       f1[(size_t)(q * kC3 + a) * N + nq] = val;
     else if (ell >= 0)
       fz.scratch[(size_t)ell * kC3 + a] = val;
-  }
-  }
-    cur ^= 1;
   }
 }
 

@@ -257,9 +257,8 @@ CV_DEV M3 piola3(const double* F, const Mat& m) {
 
 // Row r (entries 3r..3r+2) of piola3(F, m), with the same operations for the
 // neo-Hooke law (cofactor / J per entry); other laws evaluate the full tensor.
-template <bool kNeoHookeOnly = false>
 CV_DEV void piola3_row(const double* F, const Mat& m, int r, double* out) {
-  if (!kNeoHookeOnly && m.model != kMatNeoHooke) {
+  if (m.model != kMatNeoHooke) {
     const M3 P = piola3(F, m);
     out[0] = P.v[3 * r];
     out[1] = P.v[3 * r + 1];
