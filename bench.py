@@ -268,14 +268,16 @@ def measured_peaks():
 
 
 def ncu_traffic(workload: str):
-    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
+    """(DRAM bytes per launch of the bracketed node kernels, where they come from),
+    read from the committed ncu summary figures."""
     path = ROOT / "profiles" / "traffic.json"
     if not path.exists():
-        return None
+        return None, None
     try:
-        return json.loads(path.read_text()).get(workload)
+        ent = json.loads(path.read_text()).get(workload) or {}
+        return ent.get("bytes"), ent.get("source")
     except Exception:
-        return None
+        return None, None
 
 
 def cpu_baseline(workload: str, seconds: float, threads: int):
@@ -482,11 +484,12 @@ def main():
     avg_kern_s = kern_ms * 1e-3 / max(kern_n, 1)
     algo_bytes = n_active * BYTES_PER_UPDATE[args.workload]
     achieved = algo_bytes / avg_kern_s / 1e9 if kern_n else None
+    traffic, traffic_src = ncu_traffic(args.workload)
     roofline = {"bound": "hbm", "kernel": "bulk node kernel (bracketed per lattice step)",
                 "achieved": achieved, "peak": peaks.get("hbm_gbs", HBM_FALLBACK_GBS),
                 "peak_kind": peak_kind, "unit": "GB/s",
                 "frac": (achieved / peaks.get("hbm_gbs", HBM_FALLBACK_GBS)) if achieved else None,
-                "traffic": ncu_traffic(args.workload),
+                "traffic": traffic, "traffic_source": traffic_src,
                 "algorithmic_bytes_per_launch": algo_bytes,
                 "avg_launch_ms": avg_kern_s * 1e3,
                 "step_frac": (kern_ms / total_ms) if total_ms else None,
