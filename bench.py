@@ -356,7 +356,7 @@ def main():
                     help="CPU time of the oracle sample (CPU baseline and reference arm)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tile-variant", type=int, default=-1,
-                    help="fused 2-D tile shape; -1 = autotune on the workload")
+                    help="fused 2-D tile shape or 3-D collide variant; -1 = autotune")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.inner % 2:
@@ -512,6 +512,7 @@ def main():
                    "l2": "flushed between bench steps (256 MB write)",
                    "parallelism": f"replicas x{world}",
                    "tile_variant": getattr(solver, "tile_variant", None),
+                   "node_variant": getattr(solver, "node_variant", None),
                    "autotune_us_per_step": {str(k): round(v, 2) for k, v in tuned.items()}},
         "e2e": e2e, "roofline": roofline, "cpu_baseline": base,
         "clocks": clocks.summary(),

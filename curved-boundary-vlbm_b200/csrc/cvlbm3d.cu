@@ -591,8 +591,15 @@ extern "C" int cvlbm3d_run(const cvlbm3d_problem* p, cvlbm3d_fields* f, double t
           k3_sweep<<<blocks(N, 256), 256, 0, s>>>(c, f->U, f->u_next, f->u, f->u_star, clock, t);
           cv::count_launches(1);
         }
-        k3_collide<<<blocks(N, kCN), kQ3 * kCN, 0, s>>>(c, fz, f->f0, f->f1, f->U, f->u, repair,
-                                                        k == nsteps - 1);
+        if (p->node_variant == 1)
+          k3_collide<<<blocks(N, kCN), kQ3 * kCN, 0, s>>>(c, fz, f->f0, f->f1, f->U, f->u,
+                                                          repair, k == nsteps - 1);
+        else if (p->node_variant == 2)
+          k3_collide_node<3><<<blocks(N, 128), 128, 0, s>>>(c, fz, f->f0, f->f1, f->U, f->u,
+                                                            repair, k == nsteps - 1);
+        else
+          k3_collide_node<4><<<blocks(N, 128), 128, 0, s>>>(c, fz, f->f0, f->f1, f->U, f->u,
+                                                            repair, k == nsteps - 1);
         cv::count_launches(1);
       }
       timer_end(tk, s);

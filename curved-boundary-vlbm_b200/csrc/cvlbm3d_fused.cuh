@@ -117,6 +117,7 @@ __global__ void __launch_bounds__(256) k3_sweep(Ctx3 c, const double* __restrict
     const double dbz = z - ((double)p.active_k[n] + 0.5) * p.dz;
     const int mode = p.bc_mode[bid];
     const double* pp = p.bc_params + bid * 16;
+#pragma unroll
     for (int comp = 0; comp < 3; ++comp) {
       if (!(force_all || p.bc_comp_kind[comp * kMaxIds3 + bid] == kDirichlet)) continue;
       const double ub = disp3(mode, pp, comp, x, y, z, time);
@@ -376,6 +377,179 @@ __global__ void __launch_bounds__(kQ3 * kCN, 4)
     else if (ell >= 0)
       fz.scratch[(size_t)ell * kC3 + a] = val;
   }
+}
+
+// Collision + F repair + push streaming, one thread per node.
+//
+// The moments come from U, which k3_moments wrote this step with the same
+// sums (so they equal the shared-memory sums of k3_collide bit for bit), and
+// P(F), P(F_repaired) are evaluated once per node.  Each direction is then 12
+// coalesced loads of f0 and 12 stores to f1 at the neighbour, with the
+// direction a compile-time constant: of the three terms s_x f_x + s_y f_y +
+// s_z f_z of the equilibrium flux only the one on the direction's axis is
+// formed (the others are products with an exact zero, which change no finite
+// sum), so the arithmetic is that of k3_collide without its 0 * x products.
+struct NodeState3 {
+  double S[kC3];
+  double Po[9];  // P(F)
+  double dP[9];  // P(F_repaired) - P(F)
+  double dF[9];  // F_repaired - F
+  int nb[kQ3];
+  bool repaired;
+};
+
+// Moments, neighbours, P(F), the F repair and its Piola difference; the U
+// and U_need rows of the node.
+__device__ __forceinline__ void node_prologue3(const Ctx3& c, const Fused3& fz,
+                                               double* __restrict__ U,
+                                               const double* __restrict__ u, int do_repair,
+                                               int store_all, int n, NodeState3& st) {
+  const int N = c.N;
+  const cvlbm3d_problem& p = c.p;
+  const Mat& m = c.m;
+#pragma unroll
+  for (int a = 0; a < kC3; ++a) st.S[a] = U[(size_t)a * N + n];
+#pragma unroll
+  for (int q = 0; q < kQ3; ++q) st.nb[q] = p.neighbor[(size_t)q * N + n];
+  const double* F = st.S + 3;
+#pragma unroll
+  for (int r = 0; r < 3; ++r) piola3_row(F, m, r, st.Po + 3 * r);
+
+  st.repaired = false;
+  double nn[9];
+  if (do_repair) {
+    // I + grad u of the swept u, as du_axis3: centred with both neighbours,
+    // second-order one-sided with two on one side, first order with one,
+    // zero with none
+    const double h[3] = {p.dx, p.dy, p.dz};
+    double T[9];
+#pragma unroll
+    for (int comp = 0; comp < 3; ++comp) {
+      const double* uc = u + (size_t)comp * N;
+      const double u0 = uc[n];
+#pragma unroll
+      for (int ax = 0; ax < 3; ++ax) {
+        const int pp = st.nb[ax], pm = st.nb[ax + 3];
+        const double hh = h[ax];
+        double g = 0.0;
+        if (pp >= 0 && pm >= 0) {
+          g = (uc[pp] - uc[pm]) / (2.0 * hh);
+        } else if (pp >= 0) {
+          const int pp2 = p.neighbor[(size_t)ax * N + pp];
+          if (pp2 >= 0)
+            g = (-3.0 * u0 + 4.0 * uc[pp] - uc[pp2]) / (2.0 * hh);
+          else
+            g = (uc[pp] - u0) / hh;
+        } else if (pm >= 0) {
+          const int pm2 = p.neighbor[(size_t)(ax + 3) * N + pm];
+          if (pm2 >= 0)
+            g = (3.0 * u0 - 4.0 * uc[pm] + uc[pm2]) / (2.0 * hh);
+          else
+            g = (u0 - uc[pm]) / hh;
+        }
+        T[3 * comp + ax] = comp == ax ? 1.0 + g : g;
+      }
+    }
+    const double beta = fmax(0.0, fmin(1.0, p.blend));
+#pragma unroll
+    for (int k = 0; k < 9; ++k) nn[k] = F[k] + beta * (T[k] - F[k]);
+    if (det3v(nn) > m.jf) {
+      st.repaired = true;
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        double Pr[3];
+        piola3_row(nn, m, r, Pr);
+#pragma unroll
+        for (int c2 = 0; c2 < 3; ++c2) st.dP[3 * r + c2] = Pr[c2] - st.Po[3 * r + c2];
+      }
+#pragma unroll
+      for (int k = 0; k < 9; ++k) st.dF[k] = nn[k] - F[k];
+    }
+  }
+  if (st.repaired && store_all) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) U[(size_t)(3 + k) * N + n] = nn[k];
+  }
+  const int slot = fz.need_slot[n];
+  if (slot >= 0) {
+    double* rowp = fz.Uneed + (size_t)slot * kC3;
+    rowp[0] = st.S[0];
+    rowp[1] = st.S[1];
+    rowp[2] = st.S[2];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) rowp[3 + k] = st.repaired ? nn[k] : F[k];
+  }
+}
+
+template <int Q>
+__device__ __forceinline__ void collide_dir3(const cvlbm3d_problem& p, const Fused3& fz,
+                                             const NodeState3& st,
+                                             const double* __restrict__ f0,
+                                             double* __restrict__ f1, int N, int n) {
+  constexpr int ax = Q % 3;
+  constexpr double s = Q < 3 ? 1.0 : -1.0;
+  const double k3c = 3.0 / p.c, sixth = 1.0 / 6.0, om = p.omega;
+  const double sw = p.dt * (2.0 - om) * (1.0 / 12.0);
+  const double ff = 0.5 / p.c;
+  const int nq = st.nb[Q];
+  double* dst;
+  size_t stride;
+  if (nq >= 0) {
+    dst = f1 + (size_t)(Q * kC3) * N + nq;
+    stride = (size_t)N;
+  } else {
+    int ell = -1;
+    for (int k = p.node_link_start[n]; k < p.node_link_start[n + 1]; ++k) {
+      const int e = p.node_link_list[k];
+      if (p.link_q[e] == Q) ell = e;
+    }
+    if (ell < 0) return;
+    dst = fz.scratch + (size_t)ell * kC3;
+    stride = 1;
+  }
+  double old[kC3];
+#pragma unroll
+  for (int a = 0; a < kC3; ++a) old[a] = f0[(size_t)(Q * kC3 + a) * N + n];
+#pragma unroll
+  for (int a = 0; a < kC3; ++a) {
+    double fe;
+    if (a < 3) {
+      fe = sixth * (st.S[a] + k3c * (s * -st.Po[3 * a + ax]));
+    } else if ((a - 3) % 3 == ax) {
+      fe = sixth * (st.S[a] + k3c * (s * -st.S[(a - 3) / 3]));
+    } else {
+      fe = sixth * st.S[a];
+    }
+    double val = old[a] + om * (fe - old[a]) + sw * source_comp3(a, p.source_mode, p.source, st.S);
+    if (st.repaired) {
+      if (a < 3)
+        val = val - ff * (s * st.dP[3 * a + ax]);
+      else
+        val = val + sixth * st.dF[a - 3];
+    }
+    dst[a * stride] = val;
+  }
+}
+
+// MINB resident blocks of 128 threads per SM bound the registers per thread
+// (4: 128 registers, 3: 168).
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB)
+    k3_collide_node(Ctx3 c, Fused3 fz, const double* __restrict__ f0, double* __restrict__ f1,
+                    double* __restrict__ U, const double* __restrict__ u, int do_repair,
+                    int store_all) {
+  const int N = c.N;
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  NodeState3 st;
+  node_prologue3(c, fz, U, u, do_repair, store_all, n, st);
+  const cvlbm3d_problem& p = c.p;
+  collide_dir3<0>(p, fz, st, f0, f1, N, n);
+  collide_dir3<1>(p, fz, st, f0, f1, N, n);
+  collide_dir3<2>(p, fz, st, f0, f1, N, n);
+  collide_dir3<3>(p, fz, st, f0, f1, N, n);
+  collide_dir3<4>(p, fz, st, f0, f1, N, n);
+  collide_dir3<5>(p, fz, st, f0, f1, N, n);
 }
 
 // -- link kernels -------------------------------------------------------------

@@ -78,7 +78,7 @@ class Problem3D(C.Structure):
         ("node_link_start", pI), ("node_link_list", pI),
         ("bc_kind", pI), ("bc_mode", pI), ("bc_comp_kind", pI), ("bc_params", pI),
         ("dyn_enabled", pI), ("dyn_traction", pI),
-        ("need_slot", pI), ("n_need", i32), ("reserved3", i32), ("char_slot", pI),
+        ("need_slot", pI), ("n_need", i32), ("node_variant", i32), ("char_slot", pI),
         ("link_partner", pI), ("link_order", pI),
     ]
 

@@ -643,6 +643,48 @@ class WarpSparseCurvedBoundaryLBM3D:
             self.time += self.dt
         self.steps += nsteps
 
+    # fused collide kernel: 0 one thread per node (128 registers), 1 six warps
+    # per 32 nodes (shared memory), 2 one thread per node (168 registers)
+    NODE_VARIANTS = (0, 1, 2)
+
+    @property
+    def node_variant(self) -> int:
+        return int(self._problem.node_variant)
+
+    def _select_variant(self, variant: int) -> None:
+        """Pick the fused collide kernel (results are identical; speed differs)."""
+        if int(variant) not in self.NODE_VARIANTS:
+            raise ValueError(f"fused collide variant {variant} does not exist")
+        self._problem.node_variant = int(variant)
+
+    def autotune(self, steps: int = 10, variants=None) -> dict:
+        """Time every fused collide variant on this problem; keep the fastest.
+
+        Runs on a copy of the state that is restored afterwards, so the
+        solution is unchanged.  Returns {variant: us/step}.
+        """
+        import torch
+
+        saved = (self.f0.clone(), self.f1.clone(), self.u_star.clone(), self.U.clone(),
+                 self.u.clone(), self.u_local_next.clone(), self.time, self.steps)
+        times = {}
+        for v in (variants if variants is not None else self.NODE_VARIANTS):
+            self._select_variant(v)
+            self.run(2)
+            torch.cuda.synchronize(self._tdev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            self.run(steps)
+            e1.record()
+            e1.synchronize()
+            times[v] = e0.elapsed_time(e1) * 1e3 / steps
+            for dst, src in zip((self.f0, self.f1, self.u_star, self.U, self.u,
+                                 self.u_local_next), saved[:6]):
+                dst.copy_(src)
+            self.time, self.steps = saved[6], saved[7]
+        self._select_variant(min(times, key=times.get))
+        return times
+
     def step(self):
         """Reference :4549-4589."""
         self.run(1)

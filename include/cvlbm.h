@@ -256,7 +256,11 @@ typedef struct cvlbm3d_problem {
   const int32_t *need_slot;                       /* [n_active] row of U_need holding the
                                                      node's post-step U, or -1 */
   int32_t n_need;                                 /* rows of U_need */
-  int32_t reserved3;
+  int32_t node_variant;                           /* fused collide kernel: 0 one thread per
+                                                     node within 128 registers, 1 six warps
+                                                     per 32 nodes (shared memory), 2 one
+                                                     thread per node within 168 registers;
+                                                     results are identical */
   const int32_t *char_slot;                       /* [64*n_links] char_idx mapped to
                                                      U_need rows (-1 unused) */
   const int32_t *link_partner;                    /* [n_links] link at the same node in the

@@ -84,26 +84,66 @@ def test_annulus_tile_variants_match_oracle(variant):
         close_rel(k, s.numpy_field(k), ref[k])
 
 
-def test_shell_200_steps_match_oracle():
+def _oracle_shell(n, steps):
+    key = ("shell", n, steps)
+    if key not in _cache:
+        from curved_lbm import workloads
+        from oracle.oracle import Oracle3D, available
+
+        if not available():
+            pytest.skip("oracle library not built")
+        geom, mat, spec, kw = workloads.shell(n)
+        o = Oracle3D(geom, material=mat, boundary=spec, threads=8, **kw)
+        o.initialize_identity()
+        o.run(steps)
+        ref = {"f0": np.array(o.f0), "u_star": np.array(o.u_star)}
+        o.refresh()
+        ref["U"], ref["u"] = np.array(o.U), np.array(o.u)
+        _cache[key] = ref
+    return _cache[key]
+
+
+def _gpu_shell(n, variant):
     from curved_lbm import workloads
     from curved_lbm.three_d import curved_boundary_warp3d as c3
-    from oracle.oracle import Oracle3D, available
 
-    if not available():
-        pytest.skip("oracle library not built")
-    geom, mat, spec, kw = workloads.shell(40)
-    o = Oracle3D(geom, material=mat, boundary=spec, threads=8, **kw)
-    o.initialize_identity()
-    o.run(200)
+    geom, mat, spec, kw = workloads.shell(n)
     s = c3.WarpSparseCurvedBoundaryLBM3D(geom, material=mat, boundary=spec, **kw)
+    s._select_variant(variant)
     s.initialize_identity()
+    return s
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2])
+def test_shell_200_steps_match_oracle(variant):
+    ref = _oracle_shell(40, 200)
+    s = _gpu_shell(40, variant)
     s.run(200)
-    close_rel("f0", s.active_populations(), o.f0)
-    close_rel("u_star", s.active_ustar(), o.u_star)
+    close_rel("f0", s.active_populations(), ref["f0"])
+    close_rel("u_star", s.active_ustar(), ref["u_star"])
     s.refresh_current()
-    o.refresh()
-    close_rel("U", s.active_system_state(), o.U)
-    close_rel("u", s.active_displacement(), o.u)
+    close_rel("U", s.active_system_state(), ref["U"])
+    close_rel("u", s.active_displacement(), ref["u"])
+
+
+def test_shell96_collide_variants_bitwise_equal():
+    import torch
+
+    want = None
+    for v in (0, 1, 2):
+        s = _gpu_shell(96, v)
+        s.run(30)
+        got = [s.active_populations(), s.active_ustar()]
+        s.refresh_current()
+        got += [s.active_system_state(), s.active_displacement()]
+        assert np.isfinite(got[0]).all()
+        if want is None:
+            want = got
+        else:
+            for k, g, w in zip(("f0", "u_star", "U", "u"), got, want):
+                np.testing.assert_array_equal(g, w, err_msg=f"variant {v} {k}")
+        del s
+        torch.cuda.empty_cache()
 
 
 def test_annulus512_fused_variants_bitwise_equal_per_phase():
