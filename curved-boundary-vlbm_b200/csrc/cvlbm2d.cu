@@ -16,6 +16,7 @@
 // order, the order in which the reference's serial atomics add them.
 #include <cuda_runtime.h>
 
+#include <map>
 #include <mutex>
 #include <string>
 
@@ -469,15 +470,64 @@ Ctx2 make_ctx(const cvlbm2d_problem* p) {
   return c;
 }
 
+// The link kernel is a set of long dependent chains (one per link) that
+// gates the next step: it is launched at the device's highest priority, so
+// that with the inner tiles of the next step in flight on another stream its
+// blocks are placed first (graphs keep the priority, see capture_graph).
+int link_priority() {
+  static int prio = [] {
+    int least = 0, greatest = 0;
+    if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess) return 0;
+    return greatest;
+  }();
+  return prio;
+}
+
 void launch_links(const Ctx2& c, const double* src, double* dst, const double* U,
                   const double* u, const double* clock, double t, double offset,
                   cudaStream_t s, int fused = 0, const double* scratch = nullptr,
                   const int32_t* partner = nullptr, double* clock_next = nullptr) {
   if (c.p.n_links <= 0) return;
   const int per = 128 / kLG;
-  k_links2g<<<blocks(c.p.n_links, per), 128, 0, s>>>(c, src, dst, U, u, clock, t, offset, fused,
-                                                      scratch, partner, clock_next);
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(blocks(c.p.n_links, per));
+  cfg.blockDim = dim3(128);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributePriority;
+  attr[0].val.priority = link_priority();
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, k_links2g, c, src, dst, U, u, clock, t, offset, fused, scratch, partner,
+                     clock_next);
   cv::count_launches(1);
+}
+
+// Second stream and the two events of the overlapped fused step, one set per
+// caller stream (runs on one stream are ordered, so they can share a set;
+// runs on different streams get different sets), created on first use and
+// kept for the life of the process.
+struct Overlap2 {
+  cudaStream_t inner;          // inner tiles
+  cudaEvent_t inner_done;      // last inner-tile launch issued
+  cudaEvent_t boundary_done;   // last boundary-tile launch issued
+};
+std::mutex g_overlap_mu;
+std::map<cudaStream_t, Overlap2> g_overlap;
+
+Overlap2* overlap_resources(cudaStream_t s) {
+  std::lock_guard<std::mutex> lock(g_overlap_mu);
+  auto it = g_overlap.find(s);
+  if (it != g_overlap.end()) return &it->second;
+  Overlap2 o{};
+  if (cudaStreamCreateWithFlags(&o.inner, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+  if (cudaEventCreateWithFlags(&o.inner_done, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&o.boundary_done, cudaEventDisableTiming) != cudaSuccess) {
+    cudaStreamDestroy(o.inner);
+    return nullptr;
+  }
+  return &(g_overlap[s] = o);
 }
 
 using FusedFn2 = void (*)(Ctx2, Fused2, const double*, double*, double*, double*, const double*,
@@ -533,6 +583,15 @@ extern "C" int cvlbm2d_run(const cvlbm2d_problem* p, cvlbm2d_fields* f, double t
   // between u_star and u_next; an odd count ends with one copy back
   double* us_cur = f->u_star;
   double* us_nxt = f->u_next;
+  Overlap2* ov = nullptr;
+  if (fused && !split && p->overlap && p->n_tiles_inner > 0 && p->n_tiles_inner < p->n_tiles &&
+      nsteps > 0) {
+    ov = overlap_resources(s);
+    if (ov) {
+      cudaEventRecord(ov->boundary_done, s);  // the inner stream starts after prior work
+      cudaStreamWaitEvent(ov->inner, ov->boundary_done, 0);
+    }
+  }
   for (int k = 0; k < nsteps; ++k) {
     const long long step = step0 + k;
     const int sweep = due(p->disp_interval, step), repair = due(p->rep_interval, step);
@@ -553,6 +612,35 @@ extern "C" int cvlbm2d_run(const cvlbm2d_problem* p, cvlbm2d_fields* f, double t
                                                  f->link_scratch, repair, k == nsteps - 1);
       cv::count_launches(1);
       timer_end(tk, s);
+      launch_links(c, f->f1, f->f1, f->U, f->u, clock, t, 0.5 * p->dt, s, 1, f->link_scratch,
+                   p->link_partner, clock_next);
+    } else if (ov) {
+      // step k: boundary tiles after the links of step k-1 (stream order) and
+      // the inner tiles of step k-1; inner tiles after the boundary tiles of
+      // step k-1 only, so they run while the link kernel of step k-1 does.
+      // The inner tiles hold no cut-link node in their halo and no node a
+      // link reads, so neither kernel touches what the other one reads.
+      const int n_in = p->n_tiles_inner, n_bd = p->n_tiles - n_in;
+      Fused2 fz_in{p->tiles, n_in, p->tiles_j, p->need_fields, p->link_partner,
+                   f->link_scratch, k == nsteps - 1};
+      Fused2 fz_bd{p->tiles + n_in, n_bd, p->tiles_j, p->need_fields, p->link_partner,
+                   f->link_scratch, k == nsteps - 1};
+      if (k > 0) {
+        cudaStreamWaitEvent(s, ov->inner_done, 0);
+        cudaStreamWaitEvent(ov->inner, ov->boundary_done, 0);
+      }
+      fl.fn<<<n_bd, fl.threads, fl.smem, s>>>(c, fz_bd, f->f0, f->f1, f->U, f->u, us_cur,
+                                              us_nxt, f->invalid, clock, t, sweep, repair);
+      cudaEventRecord(ov->boundary_done, s);
+      // inner tiles read no time (they have no cut-point anchors)
+      fl.fn<<<n_in, fl.threads, fl.smem, ov->inner>>>(c, fz_in, f->f0, f->f1, f->U, f->u, us_cur,
+                                                      us_nxt, f->invalid, nullptr, t, sweep,
+                                                      repair);
+      cudaEventRecord(ov->inner_done, ov->inner);
+      cv::count_launches(2);
+      double* us = us_cur;
+      us_cur = us_nxt;
+      us_nxt = us;
       launch_links(c, f->f1, f->f1, f->U, f->u, clock, t, 0.5 * p->dt, s, 1, f->link_scratch,
                    p->link_partner, clock_next);
     } else if (fused) {
@@ -601,6 +689,7 @@ extern "C" int cvlbm2d_run(const cvlbm2d_problem* p, cvlbm2d_fields* f, double t
     f->f1 = tmp;
     t += p->dt;
   }
+  if (ov) cudaStreamWaitEvent(s, ov->inner_done, 0);  // join: the run ends on `s`
   if (us_cur != f->u_star)
     cudaMemcpyAsync(f->u_star, us_cur, sizeof(double) * 2 * (size_t)N, cudaMemcpyDeviceToDevice, s);
   return check_launch("cvlbm2d_run");
@@ -737,7 +826,10 @@ extern "C" int cvlbm2d_run_static_scratch(const cvlbm2d_problem* p, cvlbm2d_fiel
   if (rc) return rc;
   cvlbm2d_fields local = *f;
   local.link_scratch = scratch;
-  rc = cvlbm2d_run(p, &local, time0, step0, nsteps, 0, stream);
+  // the serial step: no second stream or events are created for this call
+  cvlbm2d_problem serial = *p;
+  serial.overlap = 0;
+  rc = cvlbm2d_run(&serial, &local, time0, step0, nsteps, 0, stream);
   // hand back the f0/f1 exchange cvlbm2d_run made, keep the caller's scratch field
   f->f0 = local.f0;
   f->f1 = local.f1;

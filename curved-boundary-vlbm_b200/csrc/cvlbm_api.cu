@@ -73,6 +73,16 @@ extern "C" int cvlbm_timer_attach(cvlbm_timer* t) { return cv::attach_timer(t); 
 
 extern "C" int cvlbm_version(void) { return 10000; }
 
+extern "C" int64_t cvlbm_struct_size(int32_t which) {
+  switch (which) {
+    case 0: return (int64_t)sizeof(cvlbm2d_problem);
+    case 1: return (int64_t)sizeof(cvlbm2d_fields);
+    case 2: return (int64_t)sizeof(cvlbm3d_problem);
+    case 3: return (int64_t)sizeof(cvlbm3d_fields);
+    default: return -1;
+  }
+}
+
 extern "C" const char* cvlbm_last_error(void) { return cv::g_last_error.c_str(); }
 
 extern "C" int cvlbm_graph_launch(cvlbm_graph* g, void* stream) {

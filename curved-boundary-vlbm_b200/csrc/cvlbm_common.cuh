@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <map>
+#include <mutex>
 #include <string>
 
 #include "cvlbm.h"
@@ -60,27 +62,44 @@ inline int check_launch(const char* where) {
   return CVLBM_OK;
 }
 
+// Captures run one at a time on one persistent stream per device, so that
+// per-stream resources the captured code keys on that stream (the second
+// stream of an overlapped step) are reused from capture to capture.
+inline std::mutex& capture_mutex() {
+  static std::mutex mu;
+  return mu;
+}
+inline cudaStream_t capture_stream() {
+  static std::map<int, cudaStream_t> streams;
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  auto it = streams.find(dev);
+  if (it != streams.end()) return it->second;
+  cudaStream_t s = nullptr;
+  if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+  streams[dev] = s;
+  return s;
+}
+
 template <class F>
 int capture_graph(F&& body, cvlbm_graph** out) {
-  cudaStream_t s;
-  if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess)
-    return fail(CVLBM_ERR_CUDA, "graph capture: stream creation failed");
+  std::lock_guard<std::mutex> lock(capture_mutex());
+  cudaStream_t s = capture_stream();
+  if (!s) return fail(CVLBM_ERR_CUDA, "graph capture: stream creation failed");
   int rc = CVLBM_OK;
   cudaGraph_t g = nullptr;
-  if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
-    cudaStreamDestroy(s);
+  if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
     return fail(CVLBM_ERR_CUDA, "graph capture: begin failed");
-  }
   rc = body(s);
   cudaError_t e = cudaStreamEndCapture(s, &g);
-  cudaStreamDestroy(s);
   if (rc != CVLBM_OK) {
     if (g) cudaGraphDestroy(g);
     return rc;
   }
   if (e != cudaSuccess || !g) return fail(CVLBM_ERR_CUDA, "graph capture: end failed");
   cudaGraphExec_t ex;
-  if (cudaGraphInstantiate(&ex, g, 0) != cudaSuccess) {
+  // kernels launched with a priority attribute keep it when replayed
+  if (cudaGraphInstantiate(&ex, g, cudaGraphInstantiateFlagUseNodePriority) != cudaSuccess) {
     cudaGraphDestroy(g);
     return fail(CVLBM_ERR_CUDA, "graph capture: instantiate failed");
   }

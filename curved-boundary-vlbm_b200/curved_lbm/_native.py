@@ -48,7 +48,7 @@ class Problem2D(C.Structure):
         ("traction_x", pI), ("traction_y", pI),
         ("tiles", pI), ("n_tiles", i32), ("tiles_j", i32), ("need_fields", pI),
         ("link_partner", pI), ("lsq_node", pI), ("link_order", pI),
-        ("tile_variant", i32), ("tile_i", i32),
+        ("tile_variant", i32), ("tile_i", i32), ("n_tiles_inner", i32), ("overlap", i32),
     ]
 
 
@@ -104,6 +104,7 @@ EXPORTED = (
     "cvlbm_graph_launch",
     "cvlbm_graph_destroy",
     "cvlbm_version",
+    "cvlbm_struct_size",
     "cvlbm_last_error",
     "cvlbm_timer_create",
     "cvlbm_timer_destroy",
@@ -163,6 +164,7 @@ def load(require_cuda: bool = True):
         "cvlbm_graph_launch": (i32, [pI, pI]),
         "cvlbm_graph_destroy": (None, [pI]),
         "cvlbm_version": (i32, []),
+        "cvlbm_struct_size": (C.c_int64, [i32]),
         "cvlbm_timer_create": (i32, [i32, C.POINTER(pI)]),
         "cvlbm_timer_destroy": (None, [pI]),
         "cvlbm_timer_reset": (i32, [pI]),

@@ -229,6 +229,37 @@ def _tile_list(active: np.ndarray, tile_i: int):
     return np.flatnonzero(occupied.reshape(-1)).astype(np.int32), tj
 
 
+def _split_tiles(tiles: np.ndarray, tiles_j: int, tile_i: int, link_node: np.ndarray,
+                 need: np.ndarray, halo: int = 3):
+    """Tiles reordered inner first, and the inner count.
+
+    A tile is inner when no cut-link node lies in the tile or its `halo`-node
+    margin (the region the fused kernel reads populations from) and no node a
+    link reads (`need`) lies in the tile.  Inner tiles of one step neither
+    read what the link kernel of the previous step writes nor write what it
+    reads, so the two can run at the same time.
+    """
+    nx, ny = link_node.shape
+
+    def box_sums(mask):
+        c = np.zeros((nx + 1, ny + 1), dtype=np.int64)
+        c[1:, 1:] = mask.astype(np.int64).cumsum(0).cumsum(1)
+        return c
+
+    def count(c, i0, i1, j0, j1):
+        i0, j0 = np.clip(i0, 0, nx), np.clip(j0, 0, ny)
+        i1, j1 = np.clip(i1, 0, nx), np.clip(j1, 0, ny)
+        return c[i1, j1] - c[i0, j1] - c[i1, j0] + c[i0, j0]
+
+    cl, cn = box_sums(link_node), box_sums(need)
+    t = np.asarray(tiles, dtype=np.int64)
+    i0, j0 = (t // tiles_j) * tile_i, (t % tiles_j) * TILE_J
+    inner = ((count(cl, i0 - halo, i0 + tile_i + halo, j0 - halo, j0 + TILE_J + halo) == 0)
+             & (count(cn, i0, i0 + tile_i, j0, j0 + TILE_J) == 0))
+    order = np.concatenate([t[inner], t[~inner]]).astype(np.int32)
+    return order, int(inner.sum())
+
+
 def _fused_tables(geometry, lsq_i, lsq_j, lsq_valid):
     """Tables of the fused step: link-stencil nodes and link partners.
 
@@ -444,8 +475,10 @@ class WarpCurvedBoundaryLBM2D:
         t["node_link_start"], t["node_link_list"] = dev_i(start), dev_i(order)
         t["bc_kind"], t["bc_mode"], t["bc_params"] = dev_i(kind), dev_i(mode), dev_f(params)
         fused = _fused_tables(geometry, np.asarray(lsq_i), np.asarray(lsq_j), lsq_valid)
+        self._need_np = None
         if fused is not None:
             need, partner = fused
+            self._need_np = need
             t["need_fields"] = torch.as_tensor(need, device=dev)
             t["link_partner"] = dev_i(partner)
         self._tile_lists: dict = {}
@@ -481,6 +514,16 @@ class WarpCurvedBoundaryLBM2D:
         self.initialize_identity(init_order=1)
 
     # -- native plumbing ---------------------------------------------------
+    @property
+    def overlap_links(self) -> bool:
+        """Run the next step's inner tiles on a second stream while the cut-link
+        kernel runs (fused step only; results are identical either way)."""
+        return bool(self._problem.overlap)
+
+    @overlap_links.setter
+    def overlap_links(self, on: bool) -> None:
+        self._problem.overlap = int(bool(on))
+
     def _select_variant(self, variant: int) -> None:
         """Point the problem at the tile list of fused-kernel variant `variant`."""
         import torch
@@ -490,13 +533,21 @@ class WarpCurvedBoundaryLBM2D:
             raise ValueError(f"fused-kernel variant {variant} is not compiled")
         if tile_i not in self._tile_lists:
             tiles, tj = _tile_list(self.active_np.astype(bool), tile_i)
-            self._tile_lists[tile_i] = (torch.as_tensor(tiles, device=self._tdev), tj)
-        tiles, tj = self._tile_lists[tile_i]
+            n_inner = 0
+            if self._need_np is not None:
+                link_node = np.zeros((self.nx, self.ny), dtype=bool)
+                link_node[self.geometry.link_i, self.geometry.link_j] = True
+                tiles, n_inner = _split_tiles(
+                    tiles, tj, tile_i, link_node,
+                    np.asarray(self._need_np).reshape(self.nx, self.ny).astype(bool))
+            self._tile_lists[tile_i] = (torch.as_tensor(tiles, device=self._tdev), tj, n_inner)
+        tiles, tj, n_inner = self._tile_lists[tile_i]
         self._tables["tiles"] = tiles
         self.tile_variant = int(variant)
         p = self._problem
         p.tile_variant, p.tile_i = int(variant), tile_i
         p.n_tiles, p.tiles_j = int(tiles.numel()), int(tj)
+        p.n_tiles_inner = int(n_inner)
         p.tiles = _native.ptr(tiles) if self._fused_possible else None
 
     def autotune(self, steps: int = 40, variants=None) -> dict:
@@ -557,6 +608,7 @@ class WarpCurvedBoundaryLBM2D:
             setattr(p, name, _native.ptr(tensor))
         p.traction_x = _native.ptr(self.link_traction_x)
         p.traction_y = _native.ptr(self.link_traction_y)
+        p.overlap = 1
         return p
 
     def _set_fused(self, enabled: bool) -> None:

@@ -105,6 +105,13 @@ typedef struct cvlbm2d_problem {
   int32_t tile_variant;                       /* compiled fused-kernel variant, see
                                                  cvlbm2d_tile_variant() */
   int32_t tile_i;                             /* tile rows the tile list was built for */
+  int32_t n_tiles_inner;                      /* the first n_tiles_inner entries of `tiles`
+                                                 are inner tiles: no cut-link node within
+                                                 the tile's 3-node halo and no link-stencil
+                                                 node in the tile; the rest are boundary
+                                                 tiles (0: not classified) */
+  int32_t overlap;                            /* nonzero: the next step's inner tiles run on
+                                                 a second stream while the link kernel runs */
 } cvlbm2d_problem;
 
 /* Tile rows (i extent, tiles are 32 nodes wide in j) of fused-kernel variant
@@ -397,6 +404,11 @@ int cvlbm_fno_mse(int32_t B, int32_t C, int32_t G, const float *y, const float *
 /* Adam step, bias correction folded into lr. */
 int cvlbm_fno_adam(int64_t n, float *p, const float *g, float *m, float *v, float lr, float b1,
                    float b2, float eps, void *stream);
+
+/* sizeof of the ABI structs as this library was compiled: which = 0
+ * cvlbm2d_problem, 1 cvlbm2d_fields, 2 cvlbm3d_problem, 3 cvlbm3d_fields;
+ * -1 for anything else.  Bindings compare it with their own layout. */
+int64_t cvlbm_struct_size(int32_t which);
 
 /* Library version (major*10000 + minor*100 + patch) and last error text. */
 int cvlbm_version(void);

@@ -48,3 +48,21 @@ def test_cpu_device_is_rejected():
 
     with pytest.raises(ValueError):
         _native.torch_device("cpu")
+
+
+def test_struct_layouts_match_the_library():
+    """The ctypes mirrors of the ABI structs have the library's sizes."""
+    from curved_lbm import _build, _native
+
+    if not _native.lib_path().exists():
+        try:
+            _build.build()
+        except Exception as exc:  # pragma: no cover - toolchain missing
+            pytest.skip(f"cannot build libcvlbm.so here: {exc}")
+    lib = ctypes.CDLL(str(_native.lib_path()))
+    lib.cvlbm_struct_size.restype = ctypes.c_int64
+    lib.cvlbm_struct_size.argtypes = [ctypes.c_int32]
+    mirrors = (_native.Problem2D, _native.Fields2D, _native.Problem3D, _native.Fields3D)
+    for which, cls in enumerate(mirrors):
+        assert lib.cvlbm_struct_size(which) == ctypes.sizeof(cls), cls.__name__
+    assert lib.cvlbm_struct_size(7) == -1

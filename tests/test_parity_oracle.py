@@ -162,6 +162,35 @@ def test_annulus512_fused_variants_bitwise_equal_per_phase():
         torch.cuda.empty_cache()
 
 
+def test_annulus512_overlapped_links_bitwise_equal():
+    """Inner tiles of the next step on a second stream while the link kernel
+    runs: the same state as the serial step, every tile shape, eager and
+    replayed from a graph."""
+    import torch
+
+    keys = ("f0", "u_star", "U", "u")
+    for v in range(5):
+        a = _gpu_annulus(512, variant=v)
+        a.overlap_links = False
+        a.run(30)
+        want = [a.numpy_field(k) for k in keys]
+        b = _gpu_annulus(512, variant=v)
+        assert b.overlap_links and b._problem.n_tiles_inner > 0
+        b.run(30)
+        for k, w in zip(keys, want):
+            np.testing.assert_array_equal(b.numpy_field(k), w, err_msg=f"variant {v} {k}")
+        if v == 2:
+            c = _gpu_annulus(512, variant=v)
+            g = c.capture_graph(10)
+            for _ in range(3):
+                g.launch()
+            for k, w in zip(keys, want):
+                np.testing.assert_array_equal(c.numpy_field(k), w, err_msg=f"graph {k}")
+            del g, c
+        del a, b
+        torch.cuda.empty_cache()
+
+
 def test_annulus512_graph_equals_run():
     a = _gpu_annulus(512)
     b = _gpu_annulus(512)
