@@ -342,9 +342,9 @@ def main():
     ap.add_argument("--workload", default="annulus512",
                     choices=sorted(BUILDERS) + ["batch256", "tube_warmstart"])
     ap.add_argument("--tube-nxy", type=int, default=32, help="tube_warmstart: lattice nx = ny")
-    ap.add_argument("--train", type=int, default=128, help="tube_warmstart: training cases")
+    ap.add_argument("--train", type=int, default=256, help="tube_warmstart: training cases")
     ap.add_argument("--test", type=int, default=4, help="tube_warmstart: held-out cases")
-    ap.add_argument("--epochs", type=int, default=200, help="tube_warmstart: training epochs")
+    ap.add_argument("--epochs", type=int, default=300, help="tube_warmstart: training epochs")
     ap.add_argument("--instances", type=int, default=256, help="batch256: instance count")
     ap.add_argument("--tol", type=float, default=1e-8, help="batch256: residual tolerance")
     ap.add_argument("--max-replays", type=int, default=100000, help="batch256: replay cap")
@@ -355,6 +355,8 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=12.0,
                     help="CPU time of the oracle sample (CPU baseline and reference arm)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--overlap", default="default", choices=["default", "on", "off"],
+                    help="link-kernel overlap of the fused step (default: the solver's)")
     ap.add_argument("--tile-variant", type=int, default=-1,
                     help="fused 2-D tile shape or 3-D collide variant; -1 = autotune")
     args = ap.parse_args()
@@ -395,6 +397,8 @@ def main():
         return rc
     size_kw = {"n": args.size} if args.size > 0 else {}
     solver, n_active = BUILDERS[args.workload](device=str(dev), **size_kw)
+    if args.overlap != "default" and hasattr(solver, "overlap_links"):
+        solver.overlap_links = args.overlap == "on"
     tuned = {}
     if hasattr(solver, "autotune"):
         if args.tile_variant >= 0:

@@ -15,6 +15,9 @@
 //             _sparse_apply_links, _sparse_apply_characteristic)
 #include <cuda_runtime.h>
 
+#include <map>
+#include <mutex>
+
 #include "cvlbm_common.cuh"
 #include "cvlbm_math.cuh"
 
@@ -552,6 +555,30 @@ bool fused_ok3(const cvlbm3d_problem* p, const cvlbm3d_fields* f) {
   return true;
 }
 
+// Second stream and two events of the overlapped fused step, one set per
+// caller stream, created on first use and kept for the life of the process.
+struct Overlap3 {
+  cudaStream_t inner;         // moments of the nodes without a cut link
+  cudaEvent_t inner_done;     // last such launch issued
+  cudaEvent_t collide_done;   // last collide launch issued
+};
+std::mutex g_overlap3_mu;
+std::map<cudaStream_t, Overlap3> g_overlap3;
+
+Overlap3* overlap3_resources(cudaStream_t s) {
+  std::lock_guard<std::mutex> lock(g_overlap3_mu);
+  auto it = g_overlap3.find(s);
+  if (it != g_overlap3.end()) return &it->second;
+  Overlap3 o{};
+  if (cudaStreamCreateWithFlags(&o.inner, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+  if (cudaEventCreateWithFlags(&o.inner_done, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&o.collide_done, cudaEventDisableTiming) != cudaSuccess) {
+    cudaStreamDestroy(o.inner);
+    return nullptr;
+  }
+  return &(g_overlap3[s] = o);
+}
+
 Ctx3 make_ctx(const cvlbm3d_problem* p) {
   Ctx3 c;
   c.p = *p;
@@ -578,15 +605,31 @@ extern "C" int cvlbm3d_run(const cvlbm3d_problem* p, cvlbm3d_fields* f, double t
     Fused3 fz{p->need_slot, p->char_slot, p->link_partner, p->link_order, f->link_scratch,
               f->U_need};
     const int L = p->n_links;
+    // Overlap: the links of step k read f1 only at link nodes and their
+    // upstream nodes, and U_need, the swept u and link_scratch; the moments
+    // of step k + 1 at nodes without a cut link read f1 elsewhere and write
+    // U and u_next.  So they run on a second stream after the collide of step
+    // k, while the links do; the moments of the link nodes follow the links.
+    Overlap3* ov = nullptr;
+    if (p->overlap && p->disp_interval == 1 && N > 0 && L > 0 && p->link_nodes &&
+        p->n_link_nodes > 0 && nsteps > 1)
+      ov = overlap3_resources(s);
     for (int k = 0; k < nsteps; ++k) {
       const long long step = step0 + k;
       const int sweep = N > 0 && due(p->disp_interval, step);
       const int repair = due(p->rep_interval, step);
-      int tk = timer_begin(s);
-      if (N > 0) {
+      int tk = ov ? -1 : timer_begin(s);
+      if (N > 0 && ov && k > 0) {
+        cudaStreamWaitEvent(s, ov->inner_done, 0);
+        k3_moments_part<1><<<blocks(p->n_link_nodes, 256), 256, 0, s>>>(
+            c, f->f0, f->U, f->u_next, f->u_star, f->invalid, sweep);
+        cv::count_launches(1);
+      } else if (N > 0) {
         k3_moments<<<blocks(N, 256), 256, 0, s>>>(c, f->f0, f->U, sweep ? f->u_next : f->u,
                                                   f->u_star, f->invalid, sweep);
         cv::count_launches(1);
+      }
+      if (N > 0) {
         if (sweep) {
           k3_sweep<<<blocks(N, 256), 256, 0, s>>>(c, f->U, f->u_next, f->u, f->u_star, clock, t);
           cv::count_launches(1);
@@ -601,6 +644,15 @@ extern "C" int cvlbm3d_run(const cvlbm3d_problem* p, cvlbm3d_fields* f, double t
           k3_collide_node<4><<<blocks(N, 128), 128, 0, s>>>(c, fz, f->f0, f->f1, f->U, f->u,
                                                             repair, k == nsteps - 1);
         cv::count_launches(1);
+        if (ov && k + 1 < nsteps) {
+          // a sweep is due every step, so these moments write u_next
+          cudaEventRecord(ov->collide_done, s);
+          cudaStreamWaitEvent(ov->inner, ov->collide_done, 0);
+          k3_moments_part<0><<<blocks(N, 256), 256, 0, ov->inner>>>(
+              c, f->f1, f->U, f->u_next, f->u_star, f->invalid, 1);
+          cudaEventRecord(ov->inner_done, ov->inner);
+          cv::count_launches(1);
+        }
       }
       timer_end(tk, s);
       if (L > 0) {

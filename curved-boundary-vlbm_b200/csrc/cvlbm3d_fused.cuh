@@ -65,14 +65,51 @@ __device__ __forceinline__ void moments3(const cvlbm3d_problem& p, const double*
   }
 }
 
+__device__ __forceinline__ void moments_node3(const Ctx3& c, const double* __restrict__ f0,
+                                              double* __restrict__ U,
+                                              double* __restrict__ ucol,
+                                              double* __restrict__ ustar,
+                                              int* __restrict__ invalid, int sweep_due, int n);
+
 __global__ void __launch_bounds__(256) k3_moments(Ctx3 c, const double* __restrict__ f0,
                                                   double* __restrict__ U,
                                                   double* __restrict__ ucol,
                                                   double* __restrict__ ustar,
                                                   int* __restrict__ invalid, int sweep_due) {
-  const int N = c.N;
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= N) return;
+  if (n >= c.N) return;
+  moments_node3(c, f0, U, ucol, ustar, invalid, sweep_due, n);
+}
+
+// The moments of part of the nodes: LINKED = 0 the nodes without a cut link
+// (one thread per node, the others return), LINKED = 1 the nodes of
+// p.link_nodes (one thread per listed node).
+template <int LINKED>
+__global__ void __launch_bounds__(256) k3_moments_part(Ctx3 c, const double* __restrict__ f0,
+                                                       double* __restrict__ U,
+                                                       double* __restrict__ ucol,
+                                                       double* __restrict__ ustar,
+                                                       int* __restrict__ invalid,
+                                                       int sweep_due) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const cvlbm3d_problem& p = c.p;
+  int n;
+  if (LINKED) {
+    if (t >= p.n_link_nodes) return;
+    n = p.link_nodes[t];
+  } else {
+    if (t >= c.N || p.node_link_start[t + 1] > p.node_link_start[t]) return;
+    n = t;
+  }
+  moments_node3(c, f0, U, ucol, ustar, invalid, sweep_due, n);
+}
+
+__device__ __forceinline__ void moments_node3(const Ctx3& c, const double* __restrict__ f0,
+                                              double* __restrict__ U,
+                                              double* __restrict__ ucol,
+                                              double* __restrict__ ustar,
+                                              int* __restrict__ invalid, int sweep_due, int n) {
+  const int N = c.N;
   const cvlbm3d_problem& p = c.p;
   double S[kC3];
   moments3(p, f0, N, n, S);

@@ -79,7 +79,8 @@ class Problem3D(C.Structure):
         ("bc_kind", pI), ("bc_mode", pI), ("bc_comp_kind", pI), ("bc_params", pI),
         ("dyn_enabled", pI), ("dyn_traction", pI),
         ("need_slot", pI), ("n_need", i32), ("node_variant", i32), ("char_slot", pI),
-        ("link_partner", pI), ("link_order", pI),
+        ("link_partner", pI), ("link_order", pI), ("link_nodes", pI), ("n_link_nodes", i32),
+        ("overlap", i32),
     ]
 
 

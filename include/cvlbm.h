@@ -274,6 +274,15 @@ typedef struct cvlbm3d_problem {
                                                      incoming direction, or -1 */
   const int32_t *link_order;                      /* [n_links] processing order of the
                                                      one-thread-per-link kernels (optional) */
+  const int32_t *link_nodes;                      /* [n_link_nodes] ascending active ids of
+                                                     the nodes that hold a cut link */
+  int32_t n_link_nodes;
+  int32_t overlap;                                /* nonzero (fused step, a sweep every
+                                                     step): the next step's moments of the
+                                                     nodes without a cut link run on a
+                                                     second stream while the link kernels
+                                                     run (measured slower on shell192: the
+                                                     link kernels are throughput-bound) */
 } cvlbm3d_problem;
 
 typedef struct cvlbm3d_fields {

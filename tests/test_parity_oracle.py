@@ -127,12 +127,22 @@ def test_shell_200_steps_match_oracle(variant):
 
 
 def test_shell96_collide_variants_bitwise_equal():
+    """Every collide kernel, with and without the next step's moments
+    overlapping the link kernels, eager and replayed from a graph: one state."""
     import torch
 
     want = None
-    for v in (0, 1, 2):
+    for v, overlap, graph in ((1, False, False), (0, False, False), (2, False, False),
+                              (0, True, False), (0, True, True)):
         s = _gpu_shell(96, v)
-        s.run(30)
+        s.overlap_links = overlap
+        if graph:
+            g = s.capture_graph(10)
+            for _ in range(3):
+                g.launch()
+            del g
+        else:
+            s.run(30)
         got = [s.active_populations(), s.active_ustar()]
         s.refresh_current()
         got += [s.active_system_state(), s.active_displacement()]
@@ -141,7 +151,7 @@ def test_shell96_collide_variants_bitwise_equal():
             want = got
         else:
             for k, g, w in zip(("f0", "u_star", "U", "u"), got, want):
-                np.testing.assert_array_equal(g, w, err_msg=f"variant {v} {k}")
+                np.testing.assert_array_equal(g, w, err_msg=f"{v} {overlap} {graph} {k}")
         del s
         torch.cuda.empty_cache()
 
