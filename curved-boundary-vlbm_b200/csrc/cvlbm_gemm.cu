@@ -22,10 +22,14 @@
 // Every wait is bounded: a CTA whose MMAs do not complete within about a
 // second raises the error word, waits once more (bounded), frees its TMEM and
 // returns.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <cstdint>
+#include <cstdlib>
+#include <cstring>
 
 #include "cvlbm_common.cuh"
 
@@ -231,6 +235,162 @@ __global__ void __launch_bounds__(128)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(BN));
 }
 
+// -- TMA-fed form ------------------------------------------------------------
+// The same product with the operand tiles brought in by the tensor memory
+// accelerator: a 2-D tensor map per operand (K innermost, box 64 x rows,
+// 128-byte swizzle), so every 64-wide K slice of a 128-row tile is one
+// cp.async.bulk.tensor that lands in the canonical SWIZZLE_128B K-major
+// layout of the tensor core (rows of 128 bytes, 8-row atoms of 1024 bytes,
+// 16-byte chunks permuted by row).  Three stages: one thread issues the TMA
+// loads of slice k + 2 while another has the MMAs of slice k in flight;
+// stage s is refilled once the MMAs that read it have committed to empty[s].
+constexpr int kStagesT = 3;
+
+// Shared-memory descriptor of a SWIZZLE_128B K-major tile: start address,
+// stride between 8-row atoms 1024 bytes, leading offset unused (1), version
+// 1, layout type 2 (128-byte swizzle).  The K step of 16 elements advances
+// the start address by 32 bytes inside the atom.
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFF);
+  d |= (uint64_t)1 << 16;
+  d |= (uint64_t)(1024 >> 4) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)2 << 61;
+  return d;
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y,
+                                            uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];\n" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar)
+      : "memory");
+}
+
+// One CTA computes a 128 x BN tile of C over the K range of blockIdx.z (as
+// k_gemm_bf16).  Thread 0 issues the TMA loads, thread 32 the MMAs; every
+// wait is bounded, and a CTA that gives up raises the error word, waits
+// (bounded) for the copies and MMAs it started, frees its TMEM and returns.
+template <int BN>
+__global__ void __launch_bounds__(128)
+    k_gemm_tma(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+               float* __restrict__ C, float* __restrict__ partial, int M, int N, int kchunk,
+               int ldc, int accumulate, int* __restrict__ error) {
+  extern __shared__ uint8_t smem_t[];
+  constexpr uint32_t kATile = kBM * kBK * 2, kBTile = BN * kBK * 2;
+  __shared__ __align__(8) uint64_t full[kStagesT], empty[kStagesT], done;
+  __shared__ uint32_t tmem_slot;
+  __shared__ int s_fail, s_issued, s_consumed;
+  const uint32_t base = (smem_u32(smem_t) + 1023u) & ~1023u;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * BN;
+  const int kbeg = blockIdx.z * kchunk, nk = kchunk / kBK;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     smem_u32(&tmem_slot)),
+                 "r"(BN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+  }
+  if (tid == 32) {
+    for (int s = 0; s < kStagesT; ++s) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&full[s])));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&empty[s])));
+    }
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&done)));
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    s_fail = 0;
+    s_issued = 0;
+    s_consumed = 0;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = tmem_slot;
+  const uint32_t idesc = instr_desc_bf16(kBM, BN);
+
+  if (tid == 0) {
+    int kb = 0;
+    for (; kb < nk; ++kb) {
+      const int s = kb % kStagesT, j = kb / kStagesT;
+      if (kb >= kStagesT && !mbar_wait(smem_u32(&empty[s]), (uint32_t)((j - 1) & 1))) {
+        s_fail = 1;
+        break;
+      }
+      const uint32_t a = base + (uint32_t)s * (kATile + kBTile);
+      mbar_expect(smem_u32(&full[s]), kATile + kBTile);
+      tma_load_2d(a, &mapA, kbeg + kb * kBK, m0, smem_u32(&full[s]));
+      tma_load_2d(a + kATile, &mapB, kbeg + kb * kBK, n0, smem_u32(&full[s]));
+    }
+    s_issued = kb;
+  } else if (tid == 32) {
+    int kb = 0;
+    for (; kb < nk; ++kb) {
+      const int s = kb % kStagesT, j = kb / kStagesT;
+      if (!mbar_wait(smem_u32(&full[s]), (uint32_t)(j & 1))) {
+        s_fail = 1;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      const uint32_t a = base + (uint32_t)s * (kATile + kBTile);
+#pragma unroll
+      for (int k16 = 0; k16 < kBK / 16; ++k16) {
+        const uint64_t ad = smem_desc_sw128(a + k16 * 32);
+        const uint64_t bd = smem_desc_sw128(a + kATile + k16 * 32);
+        const uint32_t acc = (kb > 0 || k16 > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+            "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+      }
+      mma_commit(smem_u32(&empty[s]));
+    }
+    s_consumed = kb;
+    mma_commit(smem_u32(&done));  // tracks every MMA issued, also after a failure
+  }
+  __syncthreads();
+  const int got = mbar_wait(smem_u32(&done), 0u) ? 1 : 0;
+  const bool ok = __syncthreads_and(got && s_fail == 0) != 0;
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  if (!ok) {
+    if (tid == 0) {
+      atomicExch(error, 1);
+      // loads issued but not consumed still target this CTA's shared memory
+      for (int kb = s_consumed; kb < s_issued; ++kb)
+        mbar_wait(smem_u32(&full[kb % kStagesT]), (uint32_t)((kb / kStagesT) & 1));
+    }
+  } else {
+    const int row = m0 + warp * 32 + lane;
+    float* dst = partial ? partial + (size_t)blockIdx.z * M * N + (size_t)row * N + n0
+                         : C + (size_t)row * ldc + n0;
+    const bool acc = partial == nullptr && accumulate;
+#pragma unroll
+    for (int c0 = 0; c0 < BN; c0 += 16) {
+      float v[16];
+      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) dst[c0 + i] = acc ? dst[c0 + i] + v[i] : v[i];
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(BN));
+}
+
 // C (+)= sum_z partial[z] in z order.
 __global__ void k_gemm_reduce(int splits, long long MN, int M, int N, int ldc,
                               const float* __restrict__ partial, float* __restrict__ C,
@@ -241,6 +401,41 @@ __global__ void k_gemm_reduce(int splits, long long MN, int M, int N, int ldc,
   float acc = accumulate ? C[(size_t)m * ldc + n] : 0.0f;
   for (int z = 0; z < splits; ++z) acc += partial[(size_t)z * MN + t];
   C[(size_t)m * ldc + n] = acc;
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the
+// library does not link the driver API); null if unavailable.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return (PFN_cuTensorMapEncodeTiled_v12000) nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+// Tensor map of a K-major bf16 operand (rows x K, leading dimension ld):
+// boxes of 64 K-elements (128 bytes) x box_rows rows, 128-byte swizzle.
+bool operand_map(CUtensorMap* map, const void* ptr, int rows, int K, int ld, int box_rows) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+  const cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)box_rows};
+  const cuuint32_t elem[2] = {1, 1};
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr), dims, strides, box,
+             elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// CVLBM_GEMM_LOADER=threads selects the thread-loaded kernel (comparison).
+bool tma_allowed() {
+  const char* e = std::getenv("CVLBM_GEMM_LOADER");
+  return !(e && std::strcmp(e, "threads") == 0);
 }
 
 }  // namespace
@@ -274,7 +469,22 @@ extern "C" int cvlbm_gemm_bf16(const void* A, const void* B, float* C, int32_t M
   float* part = splits > 1 ? static_cast<float*>(workspace) : nullptr;
   dim3 grid(M / kBM, N / bn, splits);
   const int kchunk = K / splits;
-  if (bn == 128) {
+  CUtensorMap mapA, mapB;
+  if (tma_allowed() && operand_map(&mapA, A, M, K, lda, kBM) &&
+      operand_map(&mapB, B, N, K, ldb, bn)) {
+    const size_t smem = (size_t)kStagesT * (kBM + bn) * kBK * 2 + 1024;
+    if (bn == 128) {
+      cudaFuncSetAttribute(k_gemm_tma<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem);
+      k_gemm_tma<128><<<grid, 128, smem, s>>>(mapA, mapB, C, part, M, N, kchunk, ldc, accumulate,
+                                              error);
+    } else {
+      cudaFuncSetAttribute(k_gemm_tma<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem);
+      k_gemm_tma<64><<<grid, 128, smem, s>>>(mapA, mapB, C, part, M, N, kchunk, ldc, accumulate,
+                                             error);
+    }
+  } else if (bn == 128) {
     const size_t smem = 2 * (kBM + 128) * kBK * 2;
     cudaFuncSetAttribute(k_gemm_bf16<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_gemm_bf16<128><<<grid, 128, smem, s>>>(static_cast<const __nv_bfloat16*>(A),

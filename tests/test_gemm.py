@@ -1,8 +1,10 @@
-"""BF16 tensor-core GEMM (tcgen05) of the warm-start surrogate against torch fp32.
+"""BF16 tensor-core GEMM (tcgen05) of the warm-start surrogate against fp64.
 
 The products of bf16 inputs are exact in fp32; only the accumulation order
-differs from the fp32 reference, so the tolerance is a few fp32 ulps of the
-row sums.
+differs from the reference, so the tolerance is a few fp32 ulps of the row
+sums.  Both operand loaders run every case: TMA tensor copies into the
+128-byte-swizzled layout (the default) and thread loads into the
+no-swizzle layout (CVLBM_GEMM_LOADER=threads).
 """
 
 from __future__ import annotations
@@ -10,6 +12,12 @@ from __future__ import annotations
 import pytest
 
 pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(params=["tma", "threads"], autouse=True)
+def loader(request, monkeypatch):
+    monkeypatch.setenv("CVLBM_GEMM_LOADER", request.param)
+    return request.param
 
 
 def _gemm(A, B, C, accumulate=0, split=True):
