@@ -6,6 +6,11 @@
 // A and B are bf16, K-major (row-major with K contiguous).  M % 128 == 0,
 // N % 64 == 0, K % 64 == 0, lda/ldb % 8 == 0 (16-byte rows of 8 elements).
 //
+// Two kernels compute the same product.  k_gemm_tma (the default, further
+// down) has the operand tiles brought in by TMA tensor copies; k_gemm_bf16,
+// described here, loads them with threads and is the fallback when no tensor
+// map can be encoded (or CVLBM_GEMM_LOADER=threads).
+//
 // One CTA (4 warps) computes a 128 x BN tile of C (BN = 128 when N allows,
 // else 64).  For every 64-wide slice of K the CTA stages the A (128 x 64) and
 // B (BN x 64) tiles in shared memory in the canonical no-swizzle K-major
