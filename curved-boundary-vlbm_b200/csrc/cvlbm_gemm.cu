@@ -382,12 +382,30 @@ __global__ void __launch_bounds__(128)
     float* dst = partial ? partial + (size_t)blockIdx.z * M * N + (size_t)row * N + n0
                          : C + (size_t)row * ldc + n0;
     const bool acc = partial == nullptr && accumulate;
+    // 16-byte stores when the row start allows them (partials always do)
+    const bool vec = (reinterpret_cast<uintptr_t>(dst) & 15) == 0;
 #pragma unroll
     for (int c0 = 0; c0 < BN; c0 += 16) {
       float v[16];
       tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+      if (vec) {
+        float4* d4 = reinterpret_cast<float4*>(dst + c0);
 #pragma unroll
-      for (int i = 0; i < 16; ++i) dst[c0 + i] = acc ? dst[c0 + i] + v[i] : v[i];
+        for (int i = 0; i < 4; ++i) {
+          float4 o = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+          if (acc) {
+            const float4 c = d4[i];
+            o.x = c.x + o.x;
+            o.y = c.y + o.y;
+            o.z = c.z + o.z;
+            o.w = c.w + o.w;
+          }
+          d4[i] = o;
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) dst[c0 + i] = acc ? dst[c0 + i] + v[i] : v[i];
+      }
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
