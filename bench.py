@@ -19,6 +19,8 @@ Workloads (synthetic, seeded geometry; no external data):
   tube_warmstart  3-D tubes under end stretch and twist: solver-generated
               equilibria, surrogate training, warm vs cold time-to-residual
               (see warmstart_bench).
+  gemm_bf16   the surrogate's tcgen05 BF16 GEMM on its spectral-transform
+              shapes and two square shapes (see gemm_bench).
 
 One bench step = `--inner` lattice time steps replayed from one CUDA graph.
 L2 (126 MB) is flushed between bench steps, outside the timed events.
@@ -117,6 +119,62 @@ def warmstart_bench(args, dev):
                        "epochs": args.epochs, "tol": args.tol},
             "report": rep}
     print(json.dumps(line, default=float), flush=True)
+    return 0
+
+
+GEMM_SHAPES = ((128, 768, 65536), (128, 65536, 768), (1024, 1024, 8192), (4096, 4096, 4096))
+
+
+def gemm_bench(args, dev):
+    """gemm_bf16: the tcgen05 BF16 GEMM of the surrogate on the two FNO
+    spectral-transform shapes of the 32 x 32 x 64 tube (128 rows, 768 modes,
+    65,536 nodes) and two square shapes; CUDA events around 20 calls after 3
+    warm-ups, inputs resident.  `value` is the 4096^3 rate.  The loader is
+    the library's default (TMA); CVLBM_GEMM_LOADER=threads selects the
+    thread-loaded kernel."""
+    import torch
+
+    from curved_lbm import _native
+
+    lib = _native.load()
+    peaks, peak_kind = measured_peaks()
+    out = {}
+    for M, N, K in GEMM_SHAPES:
+        g = torch.Generator(device=dev).manual_seed(M + N + K)
+        A = torch.randn(M, K, device=dev, generator=g).to(torch.bfloat16)
+        B = torch.randn(N, K, device=dev, generator=g).to(torch.bfloat16)
+        C = torch.empty(M, N, device=dev)
+        err = torch.zeros(1, dtype=torch.int32, device=dev)
+        ws = torch.empty(int(lib.cvlbm_gemm_bf16_workspace(M, N, K)) // 4, device=dev)
+
+        def call():
+            _native.check(lib.cvlbm_gemm_bf16(
+                _native.ptr(A), _native.ptr(B), _native.ptr(C), M, N, K, K, K, N, 0,
+                _native.ptr(err), _native.ptr(ws), ws.numel() * 4, _native.stream_ptr(dev)),
+                "cvlbm_gemm_bf16")
+
+        for _ in range(3):
+            call()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(20):
+            call()
+        e1.record()
+        e1.synchronize()
+        us = e0.elapsed_time(e1) * 1e3 / 20
+        out[f"{M}x{N}x{K}"] = {"us": round(us, 1), "tflops": round(2.0 * M * N * K / us / 1e6, 1),
+                               "error_flag": int(err.item())}
+    top = out["4096x4096x4096"]["tflops"]
+    line = {"metric": "bf16 GEMM TFLOP/s (tcgen05, fp32 accumulate)", "value": top,
+            "unit": "TFLOP/s", "higher_is_better": True, "n_gpus": 1, "dtype": "bf16",
+            "data": "synthetic", "loader": os.environ.get("CVLBM_GEMM_LOADER", "tma"),
+            "config": {"workload": "gemm_bf16", "shapes": out},
+            "roofline": {"bound": "tensor", "achieved": top,
+                         "peak": peaks.get("bf16_tflops"), "peak_kind": peak_kind,
+                         "unit": "TFLOP/s",
+                         "frac": top / peaks["bf16_tflops"] if peaks.get("bf16_tflops") else None}}
+    print(json.dumps(line), flush=True)
     return 0
 
 
@@ -340,7 +398,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="annulus512",
-                    choices=sorted(BUILDERS) + ["batch256", "tube_warmstart"])
+                    choices=sorted(BUILDERS) + ["batch256", "tube_warmstart", "gemm_bf16"])
     ap.add_argument("--tube-nxy", type=int, default=32, help="tube_warmstart: lattice nx = ny")
     ap.add_argument("--train", type=int, default=256, help="tube_warmstart: training cases")
     ap.add_argument("--test", type=int, default=4, help="tube_warmstart: held-out cases")
@@ -379,6 +437,13 @@ def main():
     dev = torch.device(f"cuda:{local}")
     torch.cuda.set_device(dev)
     args.local, args.world, args.rank = local, world, rank
+    if args.workload == "gemm_bf16":
+        rc = gemm_bench(args, dev) if rank == 0 else 0
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+        return rc
     if args.workload == "tube_warmstart":
         rc = warmstart_bench(args, dev) if rank == 0 else 0
         if world > 1:
