@@ -383,8 +383,30 @@ def generate_equilibria(params: list[dict], nxy: int, tol: float, device="cuda:0
     return out
 
 
+def output_scale(t_all: np.ndarray, m_all: np.ndarray, device="cpu") -> np.ndarray:
+    """Per-channel RMS of the masked training targets [n, C_OUT, G] over the
+    training set of every rank (each rank passes its own share)."""
+    import torch
+
+    from . import replicas
+
+    w = m_all[:, None, :]
+    num = torch.as_tensor((t_all ** 2 * w).sum(axis=(0, 2)), dtype=torch.float64, device=device)
+    den = torch.as_tensor(np.broadcast_to(w.sum(axis=(0, 2)), num.shape).copy(),
+                          dtype=torch.float64, device=device)
+    replicas.allreduce_([num, den])
+    std = np.sqrt(num.cpu().numpy() / np.maximum(den.cpu().numpy(), 1))
+    return np.maximum(std, 1e-6).astype(np.float32)
+
+
 class Surrogate:
-    """FNO plus the per-channel output scaling of the training set."""
+    """FNO plus the per-channel output scaling of the training set.
+
+    Under an open process group `fit` trains data-parallel: every rank holds
+    its own share of the equilibria, draws the same number of batches per
+    epoch, and the gradients are averaged over the ranks (one flat
+    all-reduce) before each Adam step, so every rank keeps the same weights.
+    """
 
     def __init__(self, nxy: int, *, modes=(4, 4, 8), batch: int = 4, device="cuda:0",
                  seed: int = 0):
@@ -396,42 +418,55 @@ class Surrogate:
         self.scale = np.ones(C_OUT, dtype=np.float32)
         self.history: list[float] = []
 
-    def _batches(self, data, rng):
+    def _batches(self, data, rng, n: int | None = None):
+        """Shuffled batches of B cases, padded by resampling to n cases (at
+        least len(data)) and to a multiple of B."""
         B = self.net.B
         idx = rng.permutation(len(data))
-        if len(idx) % B:
-            idx = np.concatenate([idx, rng.choice(len(data), B - len(idx) % B)])
+        n = max(len(data), n or 0)
+        n = -(-n // B) * B
+        if len(idx) < n:
+            idx = np.concatenate([idx, rng.choice(len(data), n - len(idx))])
         return idx.reshape(-1, B)
 
     def fit(self, data, *, epochs: int = 100, lr: float = 2e-3, seed: int = 0) -> list[float]:
         import torch
 
+        from . import replicas
+
         net = self.net
         dev = net.dev
+        world, rank = replicas.world_and_rank()
         t_all = np.stack([d["target"] for d in data])
         m_all = np.stack([d["mask"] for d in data])
-        w = m_all[:, None, :]
-        std = np.sqrt((t_all ** 2 * w).sum(axis=(0, 2)) / np.maximum(w.sum(axis=(0, 2)), 1))
-        self.scale = np.maximum(std, 1e-6).astype(np.float32)
+        self.scale = output_scale(t_all, m_all, dev)
         X = torch.as_tensor(np.stack([d["x"] for d in data]), device=dev)
         T = torch.as_tensor((t_all / self.scale[None, :, None]).astype(np.float32), device=dev)
         Mk = torch.as_tensor(m_all.astype(np.float32), device=dev)
         wch = torch.ones(C_OUT, dtype=torch.float32, device=dev)
-        rng = np.random.default_rng(seed)
+        rng = np.random.default_rng(seed + 1000 * rank)
+        n_max = torch.tensor([float(len(data))], dtype=torch.float64, device=dev)
+        replicas.allreduce_([n_max], op="max")  # equal batch counts on every rank
+        n_max = int(n_max.item())
+        grads = list(net.grads.values())
         hist = []
-        n_batches = 0
         for ep in range(epochs):
             lr_e = lr * 0.5 * (1 + math.cos(math.pi * ep / epochs))
-            tot = torch.zeros((), dtype=torch.float64, device=dev)
-            for b in self._batches(data, rng):
+            tot = torch.zeros(1, dtype=torch.float64, device=dev)
+            batches = self._batches(data, rng, n_max)
+            for b in batches:
                 bi = torch.as_tensor(b, device=dev)
                 y = net.forward(X[bi].contiguous())
                 part, dy = net.loss_grad(y, T[bi].contiguous(), Mk[bi].contiguous(), wch)
                 net.backward(dy)
+                if world > 1:
+                    replicas.allreduce_(grads)
+                    for g in grads:
+                        g.mul_(1.0 / world)
                 net.adam_step(lr=lr_e)
                 tot += part.sum().double()
-                n_batches += 1
-            hist.append(float(tot.item()) / len(self._batches(data, np.random.default_rng(0))))
+            replicas.allreduce_([tot])
+            hist.append(float(tot.item()) / (len(batches) * world))
         if not net.gemm_ok():
             raise RuntimeError("tensor-core GEMM reported incomplete MMAs during training")
         self.history = hist
@@ -467,17 +502,23 @@ def train_and_compare(*, nxy: int = 32, n_train: int = 64, n_test: int = 4, epoc
     once) both run to `tol`; the cold run then continues to tol/100, whose
     field is the converged reference both final errors are measured against.
     """
-    from . import workloads
+    from . import replicas, workloads
 
+    world, rank = replicas.world_and_rank()
     dx = workloads.tube_lattice(nxy)[3]
     params = workloads.tube_params(n_train + n_test, seed, min_wall=4.0 * dx)
     t0 = _time.perf_counter()
-    train = generate_equilibria(params[:n_train], nxy, tol, device)
+    # under a process group every rank solves its own share of the cases
+    train = generate_equilibria(replicas.deal(params[:n_train], rank, world), nxy, tol, device)
     gen_s = _time.perf_counter() - t0
     sur = Surrogate(nxy, modes=modes, device=device, seed=seed)
     t0 = _time.perf_counter()
     hist = sur.fit(train, epochs=epochs, lr=lr, seed=seed)
     fit_s = _time.perf_counter() - t0
+    (gen_s, fit_s), (steps_sum, n_done) = replicas.reduce_times_and_counts(
+        [gen_s, fit_s], [sum(d["steps"] for d in train), len(train)], device=device)
+    if rank != 0:  # the held-out comparison runs on one GPU
+        return {"rank": rank, "n_train_local": len(train)}
     cases = []
     for prm in params[n_train:]:
         x, mask = tube_features(prm, nxy)
@@ -507,7 +548,7 @@ def train_and_compare(*, nxy: int = 32, n_train: int = 64, n_test: int = 4, epoc
     return {"nxy": nxy, "dx": dx, "min_wall": 4.0 * dx, "n_train": n_train, "n_test": n_test, "epochs": epochs, "tol": tol,
             "modes": list(modes), "generate_s": gen_s, "fit_s": fit_s,
             "train_loss_first": hist[0], "train_loss_last": hist[-1],
-            "train_steps_mean": float(np.mean([d["steps"] for d in train])),
+            "train_steps_mean": steps_sum / max(n_done, 1), "ranks": world,
             "cases": cases, "cold_wall_s": cold_w, "warm_wall_s": warm_w,
             "speedup_wall": cold_w / max(warm_w, 1e-12),
             "speedup_steps": sum(c["cold_steps"] for c in cases)
