@@ -16,6 +16,7 @@
 // order, the order in which the reference's serial atomics add them.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <map>
 #include <mutex>
 #include <string>

@@ -275,6 +275,8 @@ extern "C" int cvlbm2d_batch_create(int32_t n_inst, const cvlbm2d_problem* probl
             cudaSuccess)
       return fail(CVLBM_ERR_CUDA, "cvlbm2d_batch_create: reading a tile list failed");
     work_start[i] = (int)work.size();
+    // raster order (a solver's list may hold its inner tiles first)
+    std::sort(tiles.begin(), tiles.end());
     for (int t : tiles) work.push_back(make_int2(i, t));
     for (int l = 0; l < p->n_links; l += 128 / kLG) lwork.push_back(make_int2(i, l));
   }
