@@ -509,6 +509,7 @@ class WarpCurvedBoundaryLBM2D:
         self._clock = torch.zeros(2, dtype=f64, device=dev)
         self._stress_current = True
         self._graphs: dict = {}
+        self.use_graphs = True
         self._problem = self._make_problem()
         self._select_variant(self.tile_variant)
         self.initialize_identity(init_order=1)
@@ -565,6 +566,7 @@ class WarpCurvedBoundaryLBM2D:
         cand = [v for v in (variants if variants is not None else range(8))
                 if int(self._lib.cvlbm2d_tile_variant(int(v))) > 0]
         times = {}
+        use_graphs, self.use_graphs = self.use_graphs, False  # time launches, not captures
         for v in cand:
             self._select_variant(v)
             self.run(4)
@@ -578,6 +580,7 @@ class WarpCurvedBoundaryLBM2D:
             self.f0.copy_(saved[0]); self.f1.copy_(saved[1]); self.u_star.copy_(saved[2])
             self.U.copy_(saved[3]); self.u.copy_(saved[4])
             self.time, self.steps = saved[5], saved[6]
+        self.use_graphs = use_graphs
         best = min(times, key=times.get)
         self._select_variant(best)
         return times
@@ -724,10 +727,39 @@ class WarpCurvedBoundaryLBM2D:
         return self.local_displacement_interval > 0 and self.steps % self.local_displacement_interval == 0
 
     # -- time stepping -----------------------------------------------------
+    GRAPH_MIN_STEPS = 8   # run() replays a cached CUDA graph for even counts from here on
+    GRAPH_CACHE = 8       # graphs kept per solver
+
+    def _cached_graph(self, nsteps: int):
+        """The CUDA graph of `nsteps` steps for the current buffers, settings
+        and kinematic phase (captured on first use), or None when run() takes
+        the plain launch path (odd or short counts, graphs switched off)."""
+        import ctypes
+
+        if not self.use_graphs or nsteps < self.GRAPH_MIN_STEPS or nsteps % 2:
+            return None
+        phase = tuple(self.steps % iv for iv in (self.local_displacement_interval,
+                                                 self.local_compatibility_interval) if iv > 0)
+        key = (nsteps, phase, ctypes.string_at(ctypes.addressof(self._problem),
+                                               ctypes.sizeof(self._problem)),
+               bytes(self._fields()))
+        g = self._graphs.get(key)
+        if g is None:
+            if len(self._graphs) >= self.GRAPH_CACHE:
+                self._graphs.pop(next(iter(self._graphs)))
+            g = self._graphs[key] = _Graph2D(self, nsteps)
+        return g
+
     def run(self, nsteps: int) -> None:
-        """Advance ``nsteps`` steps in one native call (no host sync)."""
+        """Advance ``nsteps`` steps (no host sync).  Even counts of at least
+        GRAPH_MIN_STEPS replay a cached CUDA graph of the same launches (same
+        results); other counts make one native call."""
         nsteps = int(nsteps)
         if nsteps <= 0:
+            return
+        g = self._cached_graph(nsteps)
+        if g is not None:
+            g.launch()
             return
         fl = self._fields()
         _native.check(self._lib.cvlbm2d_run(self._problem, fl, float(self.time), int(self.steps),

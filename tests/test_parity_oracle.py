@@ -52,12 +52,13 @@ def _oracle_annulus(n, steps):
     return _cache[key]
 
 
-def _gpu_annulus(n, variant=None, fused=True):
+def _gpu_annulus(n, variant=None, fused=True, graphs=False):
     from curved_lbm import workloads
     from curved_lbm.two_d import curved_boundary_warp as c2
 
     geom, mat, spec, kw = workloads.annulus(n)
     s = c2.WarpCurvedBoundaryLBM2D(geom, material=mat, boundary=spec, **kw)
+    s.use_graphs = graphs  # run() on the plain launch path unless asked
     if variant is not None:
         s._select_variant(variant)
     s._set_fused(fused)
@@ -199,6 +200,24 @@ def test_annulus512_overlapped_links_bitwise_equal():
             del g, c
         del a, b
         torch.cuda.empty_cache()
+
+
+def test_annulus512_run_through_cached_graphs_equals_plain_run():
+    """run() replays cached CUDA graphs for long even counts (recaptured when
+    the buffers, settings or phase change); mixing graph and plain calls,
+    odd counts and a variant switch gives the plain path's state."""
+    a = _gpu_annulus(512)
+    b = _gpu_annulus(512, graphs=True)
+    for n in (40, 7, 40, 3, 16):
+        a.run(n)
+        b.run(n)
+    b._select_variant(4)
+    a._select_variant(4)
+    a.run(24)
+    b.run(24)
+    assert len(b._graphs) >= 3 and a.steps == b.steps and a.time == b.time
+    for k in ("f0", "u_star", "U", "u"):
+        np.testing.assert_array_equal(a.numpy_field(k), b.numpy_field(k))
 
 
 def test_annulus512_graph_equals_run():
