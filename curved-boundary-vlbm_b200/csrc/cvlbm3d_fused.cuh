@@ -6,15 +6,18 @@
 //                (u_next), invalid flag; when no sweep is due, u and u* too
 //   k3_sweep     u_swept -> u and the trapezoidal u* update, from U and ucol
 //                of the node and its six neighbours plus cut-point anchors
-//   k3_collide   f0 again (six warps per 32 nodes, one per direction):
-//                moments, F repair from the swept u (+-2 star stencil), BGK
+//   k3_collide_node (default; one thread per node) or k3_collide (six
+//                warps per 32 nodes, one per direction; shared memory):
+//                f0 again, F repair from the swept u (+-2 star stencil), BGK
 //                collision with damping/source, repair delta and push
 //                streaming to f1; a population whose neighbour is not active
 //                leaves through a cut link and is kept per link
 //                (link_scratch) for the link kernels; the post-step U of
 //                nodes that links read goes to U_need, one 96-byte row each
+//   k3_moments_part  the moments of the nodes without / with a cut link,
+//                for the optional overlap of the next step with the links
 // Per active node this reads f0 twice and writes f1 once (the f0 re-read of
-// k3_collide is what a single-pass 3-D fusion would save; its 3-deep halo
+// the collide is what a single-pass 3-D fusion would save; its 3-deep halo
 // does not fit shared memory), plus U, u and u* (about 2.1 KB per node
 // against the algorithmic 1.2 KB).
 //
