@@ -379,18 +379,50 @@ def init_dist():
 
 
 def reference_arm(args, world, rank):
+    """`--impl reference`: the reference's kernels on the host cores (the
+    oracle, a C port pinned to the reference's own outputs; Warp cannot be
+    installed here).  Rank 0 alone runs: `--warmup` untimed and `--steps`
+    timed bench steps, each a bounded sample of `chunk` lattice steps of the
+    same workload, sized to about `--ref-step-seconds` of host time."""
     if rank != 0:
         return 0
+    if args.workload not in BUILDERS:
+        print(json.dumps({"impl": "reference", "unavailable":
+                          f"no host implementation of the {args.workload} workload"}), flush=True)
+        return 0
+    from oracle import oracle as orc
+
+    orc.load()
     threads = os.cpu_count() or 1
-    base = cpu_baseline(args.workload, args.ref_seconds, threads)
+    s, n_active = BUILDERS[args.workload](oracle=True, threads=threads)
+    s.step()  # page cache and OpenMP pool
+    t0 = time.perf_counter()
+    s.step()
+    one = time.perf_counter() - t0
+    chunk = max(1, min(args.inner, int(round(args.ref_step_seconds / max(one, 1e-9)))))
+    for _ in range(args.warmup):
+        for _ in range(chunk):
+            s.step()
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        for _ in range(chunk):
+            s.step()
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = n_active * chunk * args.steps / total / 1e6
+    sample = (f"{args.steps} bench steps of {chunk} lattice time steps of {args.workload} "
+              f"({n_active} active nodes), oracle/cvlbm_oracle.c, OpenMP {threads} threads, "
+              f"{total:.1f} s")
     line = {
-        "impl": "reference", "metric": "MLUPS FP64", "value": base["value"], "unit": "MLUPS",
+        "impl": "reference", "metric": "MLUPS FP64", "value": value, "unit": "MLUPS",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "lbm_steps_per_bench_step": args.inner},
-        "cpu_baseline": base,
-        "e2e": {"value": base["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0,
+        "ms_per_step": total / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "lbm_steps_per_bench_step": chunk},
+        "cpu_baseline": {"value": value, "unit": "MLUPS", "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "MLUPS", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
         "note": "reference Warp 1.10.1 is not installable here (no wheel, no network); the "
                 "reference arm times oracle/cvlbm_oracle.c, a C port of its kernels pinned "
@@ -419,6 +451,8 @@ def main():
     ap.add_argument("--size", type=int, default=0,
                     help="lattice nodes per axis (0 = the workload's own size; smaller sizes "
                          "are for profiler captures, not bench lines)")
+    ap.add_argument("--ref-step-seconds", type=float, default=0.5,
+                    help="--impl reference: host time of one bench step (sizes the sample)")
     ap.add_argument("--ref-seconds", type=float, default=12.0,
                     help="CPU time of the oracle sample (CPU baseline and reference arm)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
