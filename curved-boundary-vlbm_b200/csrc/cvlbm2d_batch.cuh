@@ -25,6 +25,8 @@
 // has taken inside the batch.
 #pragma once
 
+#include <cstdlib>
+#include <cstring>
 #include <vector>
 
 namespace {
@@ -93,9 +95,11 @@ __global__ void __launch_bounds__(128, 4)
   }
 }
 
-__global__ void k_batch_tick2(const Inst2* __restrict__ inst, InstState2* __restrict__ st, int n) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n || !st[i].active) return;
+// Instances [i0, i1).
+__global__ void k_batch_tick2(const Inst2* __restrict__ inst, InstState2* __restrict__ st, int i0,
+                              int i1) {
+  const int i = i0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= i1 || !st[i].active) return;
   st[i].clock = st[i].clock + inst[i].c.p.dt;
   st[i].step = st[i].step + 1;
   if (*inst[i].invalid) {  // non-positive Jacobian: stop this instance, keep the others
@@ -200,6 +204,11 @@ struct cvlbm2d_batch {
   int* d_work_start = nullptr;
   double* d_uprev = nullptr;
   double2* d_partial = nullptr;
+  // two instance groups on two streams (see batch_run_grouped)
+  int groups = 1;
+  int inst_split = 0, work_split = 0, lwork_split = 0;
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_a = nullptr, ev_b = nullptr;
 };
 
 namespace {
@@ -213,22 +222,87 @@ void batch_free(cvlbm2d_batch* b) {
   cudaFree(b->d_work_start);
   cudaFree(b->d_partial);
   cudaFree(b->d_uprev);
+  if (b->ev_a) cudaEventDestroy(b->ev_a);
+  if (b->ev_b) cudaEventDestroy(b->ev_b);
+  if (b->side) cudaStreamDestroy(b->side);
   delete b;
 }
 
-void batch_step(cvlbm2d_batch* b, int store_all, cudaStream_t s) {
+// Node work items [w0, w1), link items [l0, l1), instances [i0, i1).
+void batch_nodes(cvlbm2d_batch* b, int w0, int w1, int store_all, cudaStream_t s) {
+  if (w1 <= w0) return;
   const BatchVariant2 v = batch_variant(b->variant);
-  if (b->n_work > 0) {
-    v.nodes<<<b->node_grid, v.threads, v.smem, s>>>(b->d_inst, b->d_state, b->d_work, b->n_work,
-                                                    store_all);
-    cv::count_launches(1);
-  }
-  if (b->n_lwork > 0) {
-    k_batch_links2<<<b->link_grid, 128, 0, s>>>(b->d_inst, b->d_state, b->d_lwork, b->n_lwork);
-    cv::count_launches(1);
-  }
-  k_batch_tick2<<<blocks(b->n_inst, 128), 128, 0, s>>>(b->d_inst, b->d_state, b->n_inst);
+  const int grid = b->node_grid < w1 - w0 ? b->node_grid : w1 - w0;
+  v.nodes<<<grid, v.threads, v.smem, s>>>(b->d_inst, b->d_state, b->d_work + w0, w1 - w0,
+                                          store_all);
   cv::count_launches(1);
+}
+
+void batch_links_tick(cvlbm2d_batch* b, int l0, int l1, int i0, int i1, cudaStream_t s) {
+  if (l1 > l0) {
+    const int grid = b->link_grid < l1 - l0 ? b->link_grid : l1 - l0;
+    k_batch_links2<<<grid, 128, 0, s>>>(b->d_inst, b->d_state, b->d_lwork + l0, l1 - l0);
+    cv::count_launches(1);
+  }
+  if (i1 > i0) {
+    k_batch_tick2<<<blocks(i1 - i0, 128), 128, 0, s>>>(b->d_inst, b->d_state, i0, i1);
+    cv::count_launches(1);
+  }
+}
+
+void batch_step(cvlbm2d_batch* b, int store_all, cudaStream_t s) {
+  batch_nodes(b, 0, b->n_work, store_all, s);
+  batch_links_tick(b, 0, b->n_lwork, 0, b->n_inst, s);
+}
+
+void batch_check(cvlbm2d_batch* b, int check_every, double tol, double t_min, cudaStream_t s) {
+  const BatchVariant2 v = batch_variant(b->variant);
+  if (b->n_work <= 0) return;
+  v.partial<<<b->node_grid, v.threads, 0, s>>>(b->d_inst, b->d_state, b->d_work, b->n_work,
+                                               b->d_partial);
+  cv::count_launches(1);
+  k_batch_residual2<<<blocks(b->n_inst, 128), 128, 0, s>>>(b->d_inst, b->d_state,
+                                                           b->d_work_start, b->d_partial,
+                                                           b->n_inst, tol, t_min, check_every);
+  cv::count_launches(1);
+}
+
+// Two instance groups, each advanced by its own node / link / tick launches
+// on its own stream (group A on the caller's stream, group B on `side`).
+// The groups share no buffer and no state entry, so every instance takes
+// exactly its serial sequence of launches; group B's node kernel of a step
+// starts once group A's has finished, so that it runs while A's link kernel
+// (a set of long per-link chains) does, and the offset carries on from step
+// to step.  At residual-check steps the groups join for the check over all
+// instances.
+void batch_run_grouped(cvlbm2d_batch* b, int nsteps, int check_every, double tol, double t_min,
+                       cudaStream_t s) {
+  const int ia = b->inst_split, wa = b->work_split, la = b->lwork_split;
+  cudaEventRecord(b->ev_b, s);  // the side stream starts after prior work
+  cudaStreamWaitEvent(b->side, b->ev_b, 0);
+  bool offset = true;
+  for (int k = 0; k < nsteps; ++k) {
+    const bool check = check_every > 0 && (k + 1) % check_every == 0;
+    batch_nodes(b, 0, wa, check ? 1 : 0, s);
+    if (offset) {
+      cudaEventRecord(b->ev_a, s);
+      cudaStreamWaitEvent(b->side, b->ev_a, 0);
+      offset = false;
+    }
+    batch_links_tick(b, 0, la, 0, ia, s);
+    batch_nodes(b, wa, b->n_work, check ? 1 : 0, b->side);
+    batch_links_tick(b, la, b->n_lwork, ia, b->n_inst, b->side);
+    if (check) {
+      cudaEventRecord(b->ev_b, b->side);
+      cudaStreamWaitEvent(s, b->ev_b, 0);
+      batch_check(b, check_every, tol, t_min, s);
+      cudaEventRecord(b->ev_b, s);
+      cudaStreamWaitEvent(b->side, b->ev_b, 0);
+      offset = true;
+    }
+  }
+  cudaEventRecord(b->ev_b, b->side);  // join: the run ends on the caller's stream
+  cudaStreamWaitEvent(s, b->ev_b, 0);
 }
 
 }  // namespace
@@ -332,6 +406,22 @@ extern "C" int cvlbm2d_batch_create(int32_t n_inst, const cvlbm2d_problem* probl
     batch_free(b);
     return fail(CVLBM_ERR_CUDA, "cvlbm2d_batch_create: device allocation or upload failed");
   }
+  // two instance groups of about equal node work (CVLBM_BATCH_GROUPS=1: one)
+  const char* ge = std::getenv("CVLBM_BATCH_GROUPS");
+  if (!(ge && std::strcmp(ge, "1") == 0) && n_inst > 1) {
+    int split = 1;
+    while (split < n_inst - 1 && work_start[split] < b->n_work / 2) ++split;
+    int lsplit = 0;
+    while (lsplit < b->n_lwork && lwork[lsplit].x < split) ++lsplit;
+    if (cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) == cudaSuccess &&
+        cudaEventCreateWithFlags(&b->ev_a, cudaEventDisableTiming) == cudaSuccess &&
+        cudaEventCreateWithFlags(&b->ev_b, cudaEventDisableTiming) == cudaSuccess) {
+      b->groups = 2;
+      b->inst_split = split;
+      b->work_split = work_start[split];
+      b->lwork_split = lsplit;
+    }
+  }
   *out = b;
   return CVLBM_OK;
 }
@@ -341,21 +431,16 @@ extern "C" int cvlbm2d_batch_run(cvlbm2d_batch* b, int32_t nsteps, int32_t check
   if (!b) return fail(CVLBM_ERR_INVALID_ARG, "null batch");
   if (nsteps < 0) return fail(CVLBM_ERR_INVALID_ARG, "negative step count");
   cudaStream_t s = (cudaStream_t)stream;
-  const BatchVariant2 v = batch_variant(b->variant);
+  if (b->groups == 2) {
+    batch_run_grouped(b, nsteps, check_every, tol, t_min, s);
+    return check_launch("cvlbm2d_batch_run");
+  }
   for (int k = 0; k < nsteps; ++k) {
     const bool check = check_every > 0 && (k + 1) % check_every == 0;
     int tk = timer_begin(s);
     batch_step(b, check ? 1 : 0, s);
     timer_end(tk, s);
-    if (check && b->n_work > 0) {
-      v.partial<<<b->node_grid, v.threads, 0, s>>>(b->d_inst, b->d_state, b->d_work, b->n_work,
-                                                   b->d_partial);
-      cv::count_launches(1);
-      k_batch_residual2<<<blocks(b->n_inst, 128), 128, 0, s>>>(
-          b->d_inst, b->d_state, b->d_work_start, b->d_partial, b->n_inst, tol, t_min,
-          check_every);
-      cv::count_launches(1);
-    }
+    if (check) batch_check(b, check_every, tol, t_min, s);
   }
   return check_launch("cvlbm2d_batch_run");
 }
