@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <map>
 #include <mutex>
+#include <utility>
 #include <string>
 
 #include "cvlbm_common.cuh"
@@ -506,20 +507,23 @@ void launch_links(const Ctx2& c, const double* src, double* dst, const double* U
 }
 
 // Second stream and the two events of the overlapped fused step, one set per
-// caller stream (runs on one stream are ordered, so they can share a set;
-// runs on different streams get different sets), created on first use and
-// kept for the life of the process.
+// device and caller stream (runs on one stream are ordered, so they can share
+// a set; runs on different streams get different sets), created on first use
+// and kept for the life of the process.
 struct Overlap2 {
   cudaStream_t inner;          // inner tiles
   cudaEvent_t inner_done;      // last inner-tile launch issued
   cudaEvent_t boundary_done;   // last boundary-tile launch issued
 };
 std::mutex g_overlap_mu;
-std::map<cudaStream_t, Overlap2> g_overlap;
+std::map<std::pair<int, cudaStream_t>, Overlap2> g_overlap;  // (device, caller stream)
 
 Overlap2* overlap_resources(cudaStream_t s) {
   std::lock_guard<std::mutex> lock(g_overlap_mu);
-  auto it = g_overlap.find(s);
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  const auto key = std::make_pair(dev, s);  // the default stream's handle is shared by devices
+  auto it = g_overlap.find(key);
   if (it != g_overlap.end()) return &it->second;
   Overlap2 o{};
   if (cudaStreamCreateWithFlags(&o.inner, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
@@ -528,7 +532,7 @@ Overlap2* overlap_resources(cudaStream_t s) {
     cudaStreamDestroy(o.inner);
     return nullptr;
   }
-  return &(g_overlap[s] = o);
+  return &(g_overlap[key] = o);
 }
 
 using FusedFn2 = void (*)(Ctx2, Fused2, const double*, double*, double*, double*, const double*,

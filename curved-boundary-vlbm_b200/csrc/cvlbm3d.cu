@@ -17,6 +17,7 @@
 
 #include <map>
 #include <mutex>
+#include <utility>
 
 #include "cvlbm_common.cuh"
 #include "cvlbm_math.cuh"
@@ -556,18 +557,22 @@ bool fused_ok3(const cvlbm3d_problem* p, const cvlbm3d_fields* f) {
 }
 
 // Second stream and two events of the overlapped fused step, one set per
-// caller stream, created on first use and kept for the life of the process.
+// device and caller stream, created on first use and kept for the life of the
+// process.
 struct Overlap3 {
   cudaStream_t inner;         // moments of the nodes without a cut link
   cudaEvent_t inner_done;     // last such launch issued
   cudaEvent_t collide_done;   // last collide launch issued
 };
 std::mutex g_overlap3_mu;
-std::map<cudaStream_t, Overlap3> g_overlap3;
+std::map<std::pair<int, cudaStream_t>, Overlap3> g_overlap3;  // (device, caller stream)
 
 Overlap3* overlap3_resources(cudaStream_t s) {
   std::lock_guard<std::mutex> lock(g_overlap3_mu);
-  auto it = g_overlap3.find(s);
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  const auto key = std::make_pair(dev, s);  // the default stream's handle is shared by devices
+  auto it = g_overlap3.find(key);
   if (it != g_overlap3.end()) return &it->second;
   Overlap3 o{};
   if (cudaStreamCreateWithFlags(&o.inner, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
@@ -576,7 +581,7 @@ Overlap3* overlap3_resources(cudaStream_t s) {
     cudaStreamDestroy(o.inner);
     return nullptr;
   }
-  return &(g_overlap3[s] = o);
+  return &(g_overlap3[key] = o);
 }
 
 Ctx3 make_ctx(const cvlbm3d_problem* p) {
