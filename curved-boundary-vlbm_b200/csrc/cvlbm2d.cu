@@ -765,7 +765,7 @@ extern "C" int cvlbm2d_graph_create(const cvlbm2d_problem* p, const cvlbm2d_fiel
 // scratch lives here instead, in a static device array sized for
 // CVLBM2D_STATIC_SCRATCH_MAX_LINKS cut links (6 * 16384 doubles = 768 KiB per
 // device).  Nothing is allocated on any call: the array's address is looked
-// up once per device (cudaGetSymbolAddress) and cached.
+// up once per device context (cudaGetSymbolAddress) and cached.
 //
 // Contents: no element has to start at zero.  Within every step the node
 // kernel writes the entry of each cut link before the link kernel reads it.
@@ -777,24 +777,47 @@ namespace {
 
 static __device__ __align__(256) double g_static_link_scratch[6 * CVLBM2D_STATIC_SCRATCH_MAX_LINKS];
 
+// The current context, through the runtime's driver entry point (the library
+// does not link the driver API); null when that entry point is unavailable.
+typedef int (*CtxGetCurrentFn)(void**);
+void* current_context() {
+  static CtxGetCurrentFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return (CtxGetCurrentFn) nullptr;
+    return reinterpret_cast<CtxGetCurrentFn>(p);
+  }();
+  void* ctx = nullptr;
+  if (fn && fn(&ctx) != 0) ctx = nullptr;
+  return ctx;
+}
+
 constexpr int kMaxDevices = 64;
 std::mutex g_static_mu;
 double* g_static_ptr[kMaxDevices] = {};
+void* g_static_ctx[kMaxDevices] = {};
 
-// Address of g_static_link_scratch on the current device (set up on first use).
+// Address of g_static_link_scratch on the current device.  It is looked up
+// (cudaGetSymbolAddress) on the first call on a device and kept for that
+// device's context; a new context (after cudaDeviceReset the runtime creates
+// one and loads the module again) gets a fresh lookup.
 int static_scratch(double** out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail(CVLBM_ERR_CUDA, (std::string("cudaGetDevice: ") + cudaGetErrorString(e)).c_str());
   if (dev < 0 || dev >= kMaxDevices) return fail(CVLBM_ERR_UNSUPPORTED, "device ordinal out of range");
   std::lock_guard<std::mutex> lock(g_static_mu);
-  if (!g_static_ptr[dev]) {
+  void* ctx = current_context();
+  if (!g_static_ptr[dev] || !ctx || ctx != g_static_ctx[dev]) {
     void* addr = nullptr;
     e = cudaGetSymbolAddress(&addr, g_static_link_scratch);
     if (e != cudaSuccess || !addr)
       return fail(CVLBM_ERR_CUDA, (std::string("cudaGetSymbolAddress(static link scratch): ") +
                                    cudaGetErrorString(e)).c_str());
     g_static_ptr[dev] = static_cast<double*>(addr);
+    g_static_ctx[dev] = current_context();  // the lookup made the context current
   }
   *out = g_static_ptr[dev];
   return CVLBM_OK;

@@ -19,7 +19,7 @@ from typing import Literal
 
 import numpy as np
 
-from .. import _native
+from .. import _native, _stamp
 from .characteristic_stencil3d import MAX_CHARACTERISTIC_SAMPLES, build_characteristic_weights
 from .geometry3d import (
     BOUNDARY_ID_INNER,
@@ -858,12 +858,16 @@ class WarpSparseCurvedBoundaryLBM3D:
 
     # -- exact checkpoint / restart (no counterpart in the reference) --------
     def _checkpoint_stamp(self) -> str:
-        return json.dumps({"nx": self.nx, "ny": self.ny, "nz": self.nz,
-                           "n_active": int(self.n_active),
-                           "n_links": int(self.geometry.n_links), "dt": self.dt,
-                           "omega": self.collision_omega, "c": self.lattice_speed,
-                           "material": [self.material.model, self.material.lam,
-                                        self.material.mu]}, sort_keys=True)
+        g = self.geometry
+        cs = self.characteristic_stencil
+        arrays = [self.active_i, self.active_j, self.active_k]
+        arrays += [getattr(g, k) for k in ("link_i", "link_j", "link_k", "link_q",
+                                            "link_boundary_id", "link_eta", "link_xb", "link_yb",
+                                            "link_zb", "link_nx", "link_ny", "link_nz")]
+        arrays += [None] if cs is None else [np.asarray(a) for a in cs]
+        return _stamp.config_stamp(
+            self, geometry_arrays=arrays,
+            boundary_tables=(self.kind_by_id, self.mode_by_id, self.params_by_id))
 
     def checkpoint(self, path):
         """Write the complete stepping state (active populations, u*, U, u,

@@ -23,7 +23,7 @@ from typing import Literal
 
 import numpy as np
 
-from .. import _native
+from .. import _native, _stamp
 from .geometry import (
     BOUNDARY_ID_INNER,
     BOUNDARY_ID_OUTER,
@@ -904,11 +904,15 @@ class WarpCurvedBoundaryLBM2D:
 
     # -- exact checkpoint / restart (no counterpart in the reference) --------
     def _checkpoint_stamp(self) -> str:
-        return json.dumps({"nx": self.nx, "ny": self.ny, "n_links": int(self.geometry.n_links),
-                           "dt": self.dt, "omega": self.collision_omega,
-                           "c": self.lattice_speed, "recon": self.boundary_reconstruction_name,
-                           "material": [self.material.model, self.material.lam,
-                                        self.material.mu]}, sort_keys=True)
+        g = self.geometry
+        return _stamp.config_stamp(
+            self,
+            geometry_arrays=(self.active_np, g.link_i, g.link_j, g.link_q, g.link_boundary_id,
+                             g.link_eta, g.link_xb, g.link_yb, g.link_nx, g.link_ny,
+                             self.lsq_wb_np, self.lsq_wt_np, self.lsq_wx_np, self.lsq_wy_np,
+                             self.lsq_valid_np),
+            boundary_tables=(self.boundary_kind_by_id_np, self.boundary_mode_by_id_np,
+                             self.boundary_params_by_id_np))
 
     def checkpoint(self, path: str | Path) -> None:
         """Write the complete stepping state (populations, u*, U, u, time and

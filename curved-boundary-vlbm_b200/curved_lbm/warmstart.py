@@ -437,6 +437,8 @@ class Surrogate:
         net = self.net
         dev = net.dev
         world, rank = replicas.world_and_rank()
+        if not data:
+            raise ValueError("Surrogate.fit needs at least one training case on every rank")
         t_all = np.stack([d["target"] for d in data])
         m_all = np.stack([d["mask"] for d in data])
         self.scale = output_scale(t_all, m_all, dev)
@@ -505,6 +507,10 @@ def train_and_compare(*, nxy: int = 32, n_train: int = 64, n_test: int = 4, epoc
     from . import replicas, workloads
 
     world, rank = replicas.world_and_rank()
+    if n_train < world:
+        # every rank must hold training cases: a rank with none would fail
+        # before its first gradient all-reduce and leave the others waiting
+        raise ValueError(f"n_train={n_train} is smaller than the number of ranks ({world})")
     dx = workloads.tube_lattice(nxy)[3]
     params = workloads.tube_params(n_train + n_test, seed, min_wall=4.0 * dx)
     t0 = _time.perf_counter()

@@ -1,6 +1,6 @@
 """Synthetic benchmark workloads of the curved-boundary VLBM time step.
 
-Both are the reference's production traction setups at benchmark size
+The first two are the reference's production traction setups at benchmark size
 (seeded analytic geometry, no external data):
 
 * ``annulus``: D2Q4x6 on an n x n lattice over [0, 1.1]^2, annulus r in
@@ -13,6 +13,19 @@ Both are the reference's production traction setups at benchmark size
 * ``shell``: D3Q6x12 spherical shell r in [0.5, 1.0] on an n^3 lattice over
   [0, 2.2]^3, inner sphere clamped, outer sphere under a radial traction
   ramped 0 -> 0.05 over 10000 steps (value mode 208); same physics.
+
+* ``affine_annulus``: D2Q4x6 affine Dirichlet annulus on [-0.55, 0.55]^2
+  (stored as [0, 1.1]^2 centred at (0.55, 0.55)), r in [0.25, 0.5], both
+  circles prescribing the velocity v = L X with L = [[0.01, 0.005],
+  [0, -0.01]]; the reference's affine-benchmark settings (c = 10,
+  omega = 2, compat_bfl, init_order 2, no source, no kinematics,
+  cases/affine_annulus.py:141-166, 409-445), neo-Hooke lambda = mu = 1.
+  Exact solution u = t L X, F = I + t L, v = L X (``affine_exact``).
+* ``affine_convergence``: the reference's own affine convergence case
+  (cases/affine_annulus.py:38-112): unit square, annulus r in [0.18, 0.42]
+  centred at (0.5, 0.5), affine velocity A / T with A = [[0.35, 0.18],
+  [-0.10, 0.24]], T = 0.2, neo-Hooke from Poisson ratio 0.2 and mu = 1, run
+  to t = 0.2.
 
 Each function returns ``(geometry, material, boundary_spec, solver_kwargs)``;
 the solver class is the caller's choice.
@@ -52,6 +65,117 @@ def annulus_initial_state(n: int):
     U = np.zeros((6, n, n))
     U[2] = U[5] = 1.0
     return U, np.zeros((2, n, n))
+
+
+# ---------------------------------------------------------------------------
+# Affine Dirichlet annulus (exact solution)
+# ---------------------------------------------------------------------------
+AFFINE_L = ((0.01, 0.005), (0.0, -0.01))
+AFFINE_CENTER = (0.55, 0.55)
+
+
+def _affine_spec(c2, B, center):
+    cx, cy = center
+    params = (B[0][0], B[0][1], -(B[0][0] * cx + B[0][1] * cy),
+              B[1][0], B[1][1], -(B[1][0] * cx + B[1][1] * cy), 0.0, 0.0)
+    params = tuple(float(v) for v in params)
+    return c2.CurvedBoundarySpec(
+        kind="dirichlet", value_mode=c2.CURVED_VALUE_AFFINE_VELOCITY, params=params,
+        id_kinds={c2.BOUNDARY_ID_OUTER: "dirichlet", c2.BOUNDARY_ID_INNER: "dirichlet"},
+        id_value_modes={c2.BOUNDARY_ID_OUTER: c2.CURVED_VALUE_AFFINE_VELOCITY,
+                        c2.BOUNDARY_ID_INNER: c2.CURVED_VALUE_AFFINE_VELOCITY},
+        id_params={c2.BOUNDARY_ID_OUTER: params, c2.BOUNDARY_ID_INNER: params})
+
+
+_AFFINE_SOLVER = dict(lattice_speed=10.0, collision_omega=2.0, boundary_reconstruction="compat_bfl",
+                      source_mode="none")
+
+
+def affine_annulus(n: int = 128):
+    """Affine Dirichlet annulus of the exact-solution check (module docstring)."""
+    from .two_d import curved_boundary_warp as c2
+
+    geom = c2.CurvedBoundaryGeometry.annulus(nx=n, ny=n, length_x=1.1, length_y=1.1,
+                                             center_x=AFFINE_CENTER[0], center_y=AFFINE_CENTER[1],
+                                             inner_radius=0.25, outer_radius=0.5)
+    mat = c2.WarpHyperelasticMaterial(model="neo_hooke", lam=1.0, mu=1.0)
+    return geom, mat, _affine_spec(c2, AFFINE_L, AFFINE_CENTER), dict(_AFFINE_SOLVER)
+
+
+def affine_exact(geom, t: float, L=AFFINE_L, center=AFFINE_CENTER):
+    """Exact (u, U) of the affine case at time t on the geometry's nodes:
+    u = t L X, v = L X, F = I + t L, X measured from the annulus centre."""
+    L = np.asarray(L, dtype=np.float64)
+    x = (np.arange(geom.nx) + 0.5) * geom.dx - center[0]
+    y = (np.arange(geom.ny) + 0.5) * geom.dy - center[1]
+    X, Y = np.meshgrid(x, y, indexing="ij")
+    u = np.stack([t * (L[0, 0] * X + L[0, 1] * Y), t * (L[1, 0] * X + L[1, 1] * Y)])
+    U = np.zeros((6,) + X.shape)
+    U[0] = L[0, 0] * X + L[0, 1] * Y
+    U[1] = L[1, 0] * X + L[1, 1] * Y
+    for k, (a, b) in enumerate(((0, 0), (0, 1), (1, 0), (1, 1))):
+        U[2 + k] = (1.0 if a == b else 0.0) + t * L[a, b]
+    return u, U
+
+
+def affine_initial_state(geom, L=AFFINE_L, center=AFFINE_CENTER):
+    """Start of the affine case: v = L X, F = I, u = 0 (the exact field at t = 0)."""
+    _, U = affine_exact(geom, 0.0, L, center)
+    return U, np.zeros((2, geom.nx, geom.ny))
+
+
+AFFINE_CONV_A = ((0.35, 0.18), (-0.10, 0.24))
+AFFINE_CONV_T_END = 0.20
+
+
+def affine_convergence(n: int):
+    """The reference's affine convergence case at grid n (module docstring)."""
+    from .two_d import curved_boundary_warp as c2
+
+    geom = c2.CurvedBoundaryGeometry.annulus(nx=n, ny=n, inner_radius=0.18, outer_radius=0.42,
+                                             center_x=0.5, center_y=0.5)
+    mat = c2.WarpHyperelasticMaterial.from_poisson("neo_hooke", 0.20, mu=1.0)
+    B = [[a / AFFINE_CONV_T_END for a in row] for row in AFFINE_CONV_A]
+    kw = dict(_AFFINE_SOLVER, local_compatibility_interval=0, local_compatibility_blend=0.05,
+              local_compatibility_interior_only=True)
+    return geom, mat, _affine_spec(c2, B, (0.5, 0.5)), kw
+
+
+def affine_convergence_exact(geom, t: float):
+    """Exact (u, U) of the convergence case: u = (t/T) A X, v = A X / T, F = I + (t/T) A."""
+    A = np.asarray(AFFINE_CONV_A)
+    B = A / AFFINE_CONV_T_END
+    u, U = affine_exact(geom, t, B, (0.5, 0.5))
+    return u, U
+
+
+def affine_metrics(u, U, sigma, active, u_ex, U_ex, material, relative_l2) -> dict:
+    """Relative L2 errors of the affine cases over active nodes, as the
+    reference reports them (cases/affine_annulus.py:181-227)."""
+    from .two_d.vector_nonlinear_elastic_warp import _first_piola_np
+
+    F_ex = np.array([[U_ex[2].flat[0], U_ex[3].flat[0]], [U_ex[4].flat[0], U_ex[5].flat[0]]])
+    P = _first_piola_np(F_ex, material)
+    J = float(np.linalg.det(F_ex))
+    sg = P @ F_ex.T / J
+    sig_ex = np.empty_like(sigma)
+    for k, (a, b) in enumerate(((0, 0), (0, 1), (1, 0), (1, 1))):
+        sig_ex[k] = sg[a, b]
+    F_num = U[2:6]
+    F_exf = U_ex[2:6]
+    I = np.zeros_like(F_exf)
+    I[0] = I[3] = 1.0
+    Jn = U[2] * U[5] - U[3] * U[4]
+    m = np.asarray(active, dtype=bool)
+    return {
+        "rel_l2_u": relative_l2(u - u_ex, u_ex, m),
+        "rel_l2_v": relative_l2(U[:2] - U_ex[:2], U_ex[:2], m),
+        "rel_l2_F": relative_l2(F_num - F_exf, F_exf, m),
+        "rel_l2_F_minus_I": relative_l2(F_num - F_exf, F_exf - I, m),
+        "rel_l2_sigma": relative_l2(sigma - sig_ex, sig_ex, m),
+        "min_J": float(np.min(Jn[m])),
+        "max_J": float(np.max(Jn[m])),
+    }
 
 
 def shell_geometry(n: int = 192, L: float = 2.2, ri: float = 0.5, ro: float = 1.0):

@@ -8,8 +8,7 @@
  * below replaces one of those methods; the citation in front of each names
  * the reference method (file:line inside the reference project) whose device
  * work it performs.  The Python drop-in package (curved_lbm.*) binds these
- * symbols with ctypes; INTEGRATION.md shows the binding a maintainer would
- * add to the reference.
+ * symbols with ctypes (curved_lbm/_native.py mirrors every struct below).
  *
  * Conventions
  *   - Every pointer inside a *_problem or *_fields struct is a device pointer

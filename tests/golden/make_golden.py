@@ -3,7 +3,9 @@
 
 Run in the build container, where the reference checkout is readable::
 
-    python tests/golden/make_golden.py [--ref-src /root/reference/src] [--only NAME]
+    python tests/golden/make_golden.py --ref-src <reference checkout>/src [--only NAME]
+
+(or set CVLBM_REFERENCE_SRC instead of passing --ref-src)
 
 The reference solver (``curved_lbm`` 1.0.0, Python + NVIDIA Warp 1.10.1) is
 imported from its source tree with ``_warp_standin`` installed in place of
@@ -30,6 +32,7 @@ from __future__ import annotations
 import argparse
 import json
 import math
+import os
 import shutil
 import sys
 import time
@@ -606,9 +609,12 @@ def run_geometry(c2, c3, cs3, name, case, out_dir):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref-src", default="/root/reference/src")
+    ap.add_argument("--ref-src", default=os.environ.get("CVLBM_REFERENCE_SRC"),
+                    help="src/ directory of the reference checkout (or CVLBM_REFERENCE_SRC)")
     ap.add_argument("--only", default=None)
     args = ap.parse_args()
+    if not args.ref_src:
+        ap.error("--ref-src (or CVLBM_REFERENCE_SRC) is required")
     c2, v2, c3, cs3 = _load_reference(args.ref_src)
     out_dir = HERE
     ref_fixture = Path(args.ref_src).parent / "tests" / "data" / "dirichlet_bfl_3d_reference.npz"

@@ -34,6 +34,62 @@ def _shell(n):
     return s
 
 
+def _annulus_with(n, *, traction=None, material=None, **solver_overrides):
+    from curved_lbm import workloads
+    from curved_lbm.two_d import curved_boundary_warp as c2
+
+    geom, mat, spec, kw = workloads.annulus(n)
+    if traction is not None:
+        ramp = spec.params[1]
+        spec = c2.CurvedBoundarySpec(kind="neumann", value_mode=105, params=(traction, ramp),
+                                     id_kinds={1: "neumann", 2: "dirichlet"},
+                                     id_value_modes={1: 105, 2: 0},
+                                     id_params={1: (traction, ramp), 2: ()})
+    kw.update(solver_overrides)
+    return c2.WarpCurvedBoundaryLBM2D(geom, material=material or mat, boundary=spec, **kw)
+
+
+def test_restore_refuses_other_load_material_or_schedule(tmp_path):
+    """A checkpoint only restores into a solver whose step computes the same
+    thing: another traction, material parameter, sweep relaxation or repair
+    interval is refused."""
+    from curved_lbm.two_d.vector_nonlinear_elastic_warp import WarpHyperelasticMaterial
+
+    a = _annulus(96)
+    a.run(4)
+    a.checkpoint(tmp_path / "ck.npz")
+    _annulus_with(96).restore(tmp_path / "ck.npz")  # same configuration: accepted
+    others = [
+        _annulus_with(96, traction=0.06),
+        _annulus_with(96, material=WarpHyperelasticMaterial(model="neo_hooke", lam=1.5, mu=1.0)),
+        _annulus_with(96, local_displacement_relax=0.8),
+        _annulus_with(96, local_compatibility_interval=2),
+        _annulus_with(96, damping_gamma=5.0),
+    ]
+    for s in others:
+        with pytest.raises(ValueError):
+            s.restore(tmp_path / "ck.npz")
+
+
+def test_shell_restore_refuses_other_load(tmp_path):
+    from curved_lbm import workloads
+    from curved_lbm.three_d import curved_boundary_warp3d as c3
+
+    a = _shell(24)
+    a.checkpoint(tmp_path / "ck3.npz")
+    geom, mat, spec, kw = workloads.shell(24)
+    ramp = spec.params[1]
+    other = c3.CurvedBoundarySpec3D(kind="neumann", value_mode=208, params=(0.07, ramp),
+                                    id_kinds={1: "neumann", 2: "dirichlet"},
+                                    id_value_modes={1: 208, 2: 0},
+                                    id_params={1: (0.07, ramp), 2: ()})
+    b = c3.WarpSparseCurvedBoundaryLBM3D(geom, material=mat, boundary=other, **kw)
+    with pytest.raises(ValueError):
+        b.restore(tmp_path / "ck3.npz")
+    c = c3.WarpSparseCurvedBoundaryLBM3D(geom, material=mat, boundary=spec, **kw)
+    c.restore(tmp_path / "ck3.npz")
+
+
 def test_annulus_restart_is_exact(tmp_path):
     a = _annulus(160)
     a.run(30)
