@@ -79,6 +79,7 @@ extern "C" int64_t cvlbm_struct_size(int32_t which) {
     case 1: return (int64_t)sizeof(cvlbm2d_fields);
     case 2: return (int64_t)sizeof(cvlbm3d_problem);
     case 3: return (int64_t)sizeof(cvlbm3d_fields);
+    case 4: return (int64_t)sizeof(cvlbm3d_stencil_input);
     default: return -1;
   }
 }

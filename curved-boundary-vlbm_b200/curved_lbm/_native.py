@@ -91,6 +91,13 @@ class Fields3D(C.Structure):
                  "link_scratch", "U_need")]
 
 
+class StencilInput3D(C.Structure):
+    _fields_ = [("nx", i32), ("ny", i32), ("nz", i32), ("n_links", i32), ("dx", f64),
+                ("active_id", pI)] + [(name, pI) for name in (
+                    "link_i", "link_j", "link_k", "link_q", "link_eta", "link_xb", "link_yb",
+                    "link_zb", "link_nx", "link_ny", "link_nz", "link_mask")]
+
+
 EXPORTED = (
     "cvlbm2d_run",
     "cvlbm2d_apply_boundary",
@@ -100,6 +107,7 @@ EXPORTED = (
     "cvlbm3d_apply_boundary",
     "cvlbm3d_refresh",
     "cvlbm3d_set_ustar",
+    "cvlbm3d_build_char_stencil",
     "cvlbm2d_graph_create",
     "cvlbm3d_graph_create",
     "cvlbm_graph_launch",
@@ -160,6 +168,7 @@ def load(require_cuda: bool = True):
         "cvlbm3d_apply_boundary": (i32, [P3, F3, f64, i32, pI]),
         "cvlbm3d_refresh": (i32, [P3, F3, pI]),
         "cvlbm3d_set_ustar": (i32, [P3, F3, pI, pI]),
+        "cvlbm3d_build_char_stencil": (i32, [C.POINTER(StencilInput3D), pI, pI, pI, pI, pI]),
         "cvlbm2d_graph_create": (i32, [P2, F2, i64, i32, C.POINTER(pI)]),
         "cvlbm3d_graph_create": (i32, [P3, F3, i64, i32, C.POINTER(pI)]),
         "cvlbm_graph_launch": (i32, [pI, pI]),

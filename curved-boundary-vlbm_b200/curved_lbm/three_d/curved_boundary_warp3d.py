@@ -237,7 +237,11 @@ class WarpSparseCurvedBoundaryLBM3D:
                  local_displacement_boundary_weight: float = 20.0,
                  local_displacement_boundary_id: int = -1, local_compatibility_interval: int = 0,
                  local_compatibility_blend: float = 0.1, normal_jacobian: str | None = None,
-                 neumann_solver: str | None = None):
+                 neumann_solver: str | None = None, characteristic_stencil: dict | None = None):
+        """`characteristic_stencil` (not in the reference): precomputed
+        local_f stencil tables in build_characteristic_weights' layout, used
+        instead of building them on the device (e.g. to run on the exact
+        tables of another builder)."""
         import torch
 
         self.geometry = geometry
@@ -328,8 +332,20 @@ class WarpSparseCurvedBoundaryLBM3D:
                 "normal solve) are not implemented")
         self.characteristic_stencil = None
         if self.boundary_reconstruction == BOUNDARY_RECON_LOCAL_F and self._has_neumann_cut_links:
-            self.characteristic_stencil = build_characteristic_weights(
-                geometry, tables, link_mask=np.any(ck == BC_NEUMANN, axis=0))
+            if characteristic_stencil is not None:
+                cs = characteristic_stencil
+                want = (MAX_CHARACTERISTIC_SAMPLES, int(geometry.n_links))
+                if np.shape(cs["indices"]) != want or np.shape(cs["weights"]) != (4,) + want:
+                    raise ValueError("characteristic_stencil does not match this geometry")
+                self.characteristic_stencil = {
+                    "indices": np.ascontiguousarray(cs["indices"], dtype=np.int32),
+                    "weights": np.ascontiguousarray(cs["weights"], dtype=np.float64),
+                    "probe_modes": np.asarray(cs.get("probe_modes", np.zeros(want[1])),
+                                              dtype=np.int32)}
+            else:
+                self.characteristic_stencil = build_characteristic_weights(
+                    geometry, tables, link_mask=np.any(ck == BC_NEUMANN, axis=0),
+                    device=str(device or default_device()))
         self.memory = None
 
         self.device = str(device or default_device())

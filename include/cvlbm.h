@@ -320,6 +320,37 @@ int cvlbm3d_set_ustar(const cvlbm3d_problem *p, cvlbm3d_fields *f, const double 
                       void *stream);
 
 /* ------------------------------------------------------------------------ */
+/* 3-D geometry preprocessing on the device                                  */
+/* ------------------------------------------------------------------------ */
+
+/* Geometry of the cut links whose characteristic stencil is built.  All
+ * pointers are device pointers; active_id is the dense [nx][ny][nz] map from
+ * lattice node to active id (-1: not active).  Cut points (link_xb/yb/zb)
+ * are physical coordinates of a lattice with cell-centred nodes
+ * ((i + 1/2) dx) and isotropic spacing dx. */
+typedef struct {
+  int32_t nx, ny, nz, n_links;
+  double dx;
+  const int32_t *active_id;
+  const int32_t *link_i, *link_j, *link_k, *link_q;
+  const double *link_eta, *link_xb, *link_yb, *link_zb, *link_nx, *link_ny, *link_nz;
+  const uint8_t *link_mask; /* [n_links]: nonzero = build this link; NULL = all */
+} cvlbm3d_stencil_input;
+
+/* Fixed geometry weights of the D3Q6 local_f characteristic closure for every
+ * selected cut link.  Replaces build_characteristic_weights
+ * (three_d/characteristic_stencil3d.py:18-171).  Outputs (device, caller
+ * owned): indices [64][n_links] int32 (48 gradient samples, then 16 probe
+ * samples; -1 unused), weights [4][64][n_links] (row 0 probe weights, rows
+ * 1-3 the x/y/z gradient weights), modes [n_links] (2 probe pair, 1 single
+ * probe, -k k upstream nodes, 0 not built) and status [n_links] (0 ok, 1 no
+ * full-rank quadratic fit within three cells, 2 inconsistent gradient
+ * weights: the reference raises ValueError for both).  Asynchronous on
+ * `stream`. */
+int cvlbm3d_build_char_stencil(const cvlbm3d_stencil_input *in, int32_t *indices, double *weights,
+                               int32_t *modes, int32_t *status, void *stream);
+
+/* ------------------------------------------------------------------------ */
 /* Kernel timing                                                             */
 /* ------------------------------------------------------------------------ */
 
@@ -414,8 +445,8 @@ int cvlbm_fno_adam(int64_t n, float *p, const float *g, float *m, float *v, floa
                    float b2, float eps, void *stream);
 
 /* sizeof of the ABI structs as this library was compiled: which = 0
- * cvlbm2d_problem, 1 cvlbm2d_fields, 2 cvlbm3d_problem, 3 cvlbm3d_fields;
- * -1 for anything else.  Bindings compare it with their own layout. */
+ * cvlbm2d_problem, 1 cvlbm2d_fields, 2 cvlbm3d_problem, 3 cvlbm3d_fields,
+ * 4 cvlbm3d_stencil_input; -1 for anything else.  Bindings compare it with their own layout. */
 int64_t cvlbm_struct_size(int32_t which);
 
 /* Library version (major*10000 + minor*100 + patch) and last error text. */

@@ -13,11 +13,12 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "lib" / "libcvlbm_oracle.so"
 SRC = HERE / "cvlbm_oracle.c"
+SRCS = (SRC, HERE / "char_stencil3d.c")
 FLAGS = ["-O2", "-std=c11", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC", "-shared"]
 
 
 def build(force: bool = False) -> Path:
-    deps = [SRC, HERE / "cvlbm_oracle.h", HERE.parent / "include" / "cvlbm.h"]
+    deps = [*SRCS, HERE / "cvlbm_oracle.h", HERE.parent / "include" / "cvlbm.h"]
     if not force and LIB.exists() and all(d.stat().st_mtime <= LIB.stat().st_mtime for d in deps):
         return LIB
     LIB.parent.mkdir(parents=True, exist_ok=True)
@@ -28,7 +29,7 @@ def build(force: bool = False) -> Path:
     ccs = [c for c in cands if c]
     for flags in (FLAGS, [f for f in FLAGS if f != "-fopenmp"]):
         for cc in ccs:
-            r = subprocess.run([cc, *flags, "-o", str(tmp), str(SRC), "-lm"], capture_output=True,
+            r = subprocess.run([cc, *flags, "-o", str(tmp), *map(str, SRCS), "-lm"], capture_output=True,
                                text=True)
             if r.returncode == 0:
                 os.replace(tmp, LIB)

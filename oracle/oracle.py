@@ -190,6 +190,39 @@ class Oracle2D:
             self.step()
 
 
+def build_char_stencil(geometry, tables, link_mask=None) -> dict:
+    """Characteristic stencil of the cut links (oracle/char_stencil3d.c), in
+    the reference's layout: indices (64, L), weights (4, 64, L), probe_modes
+    (L,).  Raises ValueError like the reference for a link without a
+    full-rank fit or with inconsistent gradient weights."""
+    lib = load()
+    g = geometry
+    L = int(g.n_links)
+    idx = np.full((64, L), -1, np.int32)
+    w = np.zeros((4, 64, L))
+    modes = np.zeros(L, np.int32)
+    status = np.zeros(L, np.int32)
+    aid = np.ascontiguousarray(tables["active_id"], dtype=np.int32)
+    i32, f64 = np.int32, np.float64
+    arr = {k: np.ascontiguousarray(getattr(g, k), dtype=i32) for k in ("link_i", "link_j",
+                                                                       "link_k", "link_q")}
+    arr.update({k: np.ascontiguousarray(getattr(g, k), dtype=f64) for k in (
+        "link_eta", "link_xb", "link_yb", "link_zb", "link_nx", "link_ny", "link_nz")})
+    mask = None if link_mask is None else np.ascontiguousarray(link_mask, dtype=np.uint8)
+    lib.oracle3d_char_stencil.restype = C.c_int
+    bad = lib.oracle3d_char_stencil(
+        C.c_int(g.nx), C.c_int(g.ny), C.c_int(g.nz), _ptr(aid), C.c_int(L),
+        *(_ptr(arr[k]) for k in ("link_i", "link_j", "link_k", "link_q", "link_eta", "link_xb",
+                                 "link_yb", "link_zb", "link_nx", "link_ny", "link_nz")),
+        C.c_double(float(g.dx)), _ptr(mask), _ptr(idx), _ptr(w), _ptr(modes), _ptr(status))
+    if bad >= 0:
+        if status[bad] == 1:
+            raise ValueError("local_f needs a full-rank quadratic stencil within three cells; "
+                             f"cut links {np.flatnonzero(status == 1)[:8].tolist()}")
+        raise ValueError(f"invalid local_f gradient weights near link {bad}")
+    return {"indices": idx, "weights": w, "probe_modes": modes}
+
+
 class Oracle3D:
     """Serial/OpenMP CPU replay of WarpSparseCurvedBoundaryLBM3D (reference C3:3852-4802)."""
 
@@ -199,9 +232,11 @@ class Oracle3D:
                  local_displacement_sweeps=1, local_displacement_relax=0.85,
                  local_displacement_boundary_weight=20.0, local_displacement_boundary_id=-1,
                  local_compatibility_interval=0, local_compatibility_blend=0.1,
-                 normal_jacobian=None, neumann_solver=None, threads=1, **_unused):
+                 normal_jacobian=None, neumann_solver=None, threads=1, char_stencil=None,
+                 **_unused):
+        """`char_stencil`: characteristic stencil tables to use (e.g. the ones a
+        CUDA solver built), else they are built by oracle/char_stencil3d.c."""
         from curved_lbm import _native
-        from curved_lbm.three_d import characteristic_stencil3d as cs3
         from curved_lbm.three_d import curved_boundary_warp3d as c3
         from curved_lbm.three_d import geometry3d as g3
 
@@ -243,7 +278,8 @@ class Oracle3D:
         p.source_mode = self.source_mode
         char = None
         if recon == 3 and has_neu:
-            char = cs3.build_characteristic_weights(g, tables, link_mask=np.any(lck == 2, axis=0))
+            char = char_stencil if char_stencil is not None else build_char_stencil(
+                g, tables, link_mask=np.any(lck == 2, axis=0))
         p.has_char = int(char is not None)
         p.has_tangent_lsq = int(recon == 2)
         p.disp_interval = int(max(0, local_displacement_interval))

@@ -62,7 +62,8 @@ def test_struct_layouts_match_the_library():
     lib = ctypes.CDLL(str(_native.lib_path()))
     lib.cvlbm_struct_size.restype = ctypes.c_int64
     lib.cvlbm_struct_size.argtypes = [ctypes.c_int32]
-    mirrors = (_native.Problem2D, _native.Fields2D, _native.Problem3D, _native.Fields3D)
+    mirrors = (_native.Problem2D, _native.Fields2D, _native.Problem3D, _native.Fields3D,
+               _native.StencilInput3D)
     for which, cls in enumerate(mirrors):
         assert lib.cvlbm_struct_size(which) == ctypes.sizeof(cls), cls.__name__
     assert lib.cvlbm_struct_size(7) == -1

@@ -71,8 +71,14 @@ def test_oracle_2d_reproduces_reference(golden_dir, name, threads):
 
 @pytest.mark.parametrize("name", GOLD3)
 def test_oracle_3d_reproduces_reference(golden_dir, name):
+    """The time step on the reference's own characteristic stencil tables
+    (stored in the fixture; the builders are pinned in test_char_stencil.py)."""
     d, cfg = cases.load(golden_dir / f"{name}.npz")
-    o = oracle_3d(cfg, threads=2)
+    kw = {}
+    if "char_indices" in d.files:
+        kw["char_stencil"] = {"indices": d["char_indices"], "weights": d["char_weights"],
+                              "probe_modes": d["char_modes"]}
+    o = oracle_3d(cfg, threads=2, **kw)
     o.initialize_identity()
     close("f0_init", o.f0, d["f0_init"])
     close("ustar_init", o.u_star, d["ustar_init"])

@@ -113,7 +113,10 @@ def test_annulus_tile_variants_match_oracle(variant):
         close_rel(k, s.numpy_field(k), ref[k])
 
 
-def _oracle_shell(n, steps):
+def _oracle_shell(n, steps, stencil=None):
+    """Oracle replay of the shell; `stencil`: the characteristic stencil
+    tables the CUDA solver built, so both step on identical inputs (the
+    builders themselves are pinned in test_char_stencil.py)."""
     key = ("shell", n, steps)
     if key not in _cache:
         from curved_lbm import workloads
@@ -122,7 +125,8 @@ def _oracle_shell(n, steps):
         if not available():
             pytest.skip("oracle library not built")
         geom, mat, spec, kw = workloads.shell(n)
-        o = Oracle3D(geom, material=mat, boundary=spec, threads=THREADS, **kw)
+        o = Oracle3D(geom, material=mat, boundary=spec, threads=THREADS, char_stencil=stencil,
+                     **kw)
         o.initialize_identity()
         o.run(steps)
         ref = {"f0": np.array(o.f0), "u_star": np.array(o.u_star)}
@@ -147,8 +151,8 @@ def _gpu_shell(n, variant):
 def test_shell64_1000_steps_match_oracle():
     """A 64^3 spherical shell (90,240 active nodes) of the 3-D benchmark
     physics for 1000 steps with the default (autotuned) collide."""
-    ref = _oracle_shell(64, 1000)
     s = _gpu_shell(64, None)
+    ref = _oracle_shell(64, 1000, s.characteristic_stencil)
     s.autotune(steps=10)
     s.run(1000)
     close_rel("f0", s.active_populations(), ref["f0"])
@@ -161,8 +165,8 @@ def test_shell64_1000_steps_match_oracle():
 
 @pytest.mark.parametrize("variant", [0, 1, 2])
 def test_shell_200_steps_match_oracle(variant):
-    ref = _oracle_shell(40, 200)
     s = _gpu_shell(40, variant)
+    ref = _oracle_shell(40, 200, s.characteristic_stencil)
     s.run(200)
     close_rel("f0", s.active_populations(), ref["f0"])
     close_rel("u_star", s.active_ustar(), ref["u_star"])
