@@ -281,46 +281,79 @@ __device__ __forceinline__ void fused2_tile(
   if (J <= m.jf) *invalid = 1;
   const P2 Po = piola2(S[2], S[3], S[4], S[5], m);
   const double k2c = 2.0 / p.c, om = p.omega, sw = p.dt * (2.0 - om) * 0.125;
-  double d11 = 0.0, d12 = 0.0, d21 = 0.0, d22 = 0.0;
+  const double ff = 0.5 / p.c, qt = 0.25;
+  // Per-node constants of the collision.  The reference's equilibrium
+  // 0.25*(U_a + (2/c)*(cx*phix_a + cy*phiy_a)) has cx, cy in {0, +-1}: a
+  // product with an exact zero adds nothing to a finite sum and a product
+  // with -1 is a negation, so with g = (2/c)*phi along the direction's axis
+  // it is 0.25*(U_a +- g_a), the same double (up to the sign of an exact
+  // zero).  The source and repair terms do not depend on q and are formed
+  // once per component.
+  P2 dP{0.0, 0.0, 0.0, 0.0};
   if (repaired) {
     const P2 Pn = piola2(Fn[0], Fn[1], Fn[2], Fn[3], m);
-    d11 = Pn.a - Po.a;
-    d12 = Pn.b - Po.b;
-    d21 = Pn.c - Po.c;
-    d22 = Pn.d - Po.d;
+    dP = {Pn.a - Po.a, Pn.b - Po.b, Pn.c - Po.c, Pn.d - Po.d};
   }
-  const double ff = 0.5 / p.c, qt = 0.25;
-  // collision, repair delta and push-streaming, one population at a time
-  // (f0 of the owner is re-read from L1: the tile loaded it in phase A)
+  // destinations of the four directions: a neighbour node, a cut link's
+  // scratch row, or nowhere (a cut link without scratch)
+  int dst[4];
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     const int cq = cx2(q), cy = cy2(q);
-    const double cxd = (double)cq, cyd = (double)cy;
-    const bool to_node = sA[r_own + cq * kRX + cy] != 0;
-    const int d = n + cq * ny + cy;
-    int ell_out = -1;
-    if (!to_node) {
+    if (sA[r_own + cq * kRX + cy] != 0) {
+      dst[q] = n + cq * ny + cy;
+    } else {
+      int ell_out = -1;
       for (int k = p.node_link_start[n]; k < p.node_link_start[n + 1]; ++k) {
         const int e = p.node_link_list[k];
         if (p.link_q[e] == q) ell_out = e;
       }
+      dst[q] = ell_out >= 0 ? -2 - ell_out : -1;
     }
+  }
+  const bool add_src = p.source_mode != kSrcNone;
+  const bool add_src_f = p.source_mode == kSrcConstant;  // damping: rows 2-5 get +0
+  // collision, repair delta and push-streaming, component by component
+  // (f0 of the owner is re-read from L1: the tile loaded it in phase A)
 #pragma unroll
-    for (int a = 0; a < 6; ++a) {
+  for (int a = 0; a < 6; ++a) {
+    // g along x and y for this component (zero rows: 3, 5 along x; 2, 4 along y)
+    const double gx = a == 0 ? k2c * -Po.a : a == 1 ? k2c * -Po.c : a == 2 ? k2c * -S[0]
+                    : a == 4 ? k2c * -S[1] : 0.0;
+    const double gy = a == 0 ? k2c * -Po.b : a == 1 ? k2c * -Po.d : a == 3 ? k2c * -S[0]
+                    : a == 5 ? k2c * -S[1] : 0.0;
+    const bool hx = a == 0 || a == 1 || a == 2 || a == 4;
+    const bool hy = a == 0 || a == 1 || a == 3 || a == 5;
+    const double swB = (add_src && (a < 2 || add_src_f))
+                           ? sw * source_comp(a, p.source_mode, p.source, S) : 0.0;
+    // repair: ff*(cx*dP_a1 + cy*dP_a2) for the velocity rows, qt*(Fn - F) for the F rows
+    const double tx = a == 0 ? ff * dP.a : a == 1 ? ff * dP.c : 0.0;
+    const double ty = a == 0 ? ff * dP.b : a == 1 ? ff * dP.d : 0.0;
+    const double rF = a >= 2 ? qt * (Fn[a - 2] - S[a]) : 0.0;
+    const double Ua = S[a];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int cq = cx2(q), cy = cy2(q);
+      const bool neg = cq < 0 || cy < 0;
+      const bool has_g = cq != 0 ? hx : hy;
+      const double g = cq != 0 ? gx : gy;
       const double old = f0[(size_t)(q * 6 + a) * N + n];
-      const double fe = feq2(q, a, S, Po, k2c);
-      double v = old + om * (fe - old) + sw * source_comp(a, p.source_mode, p.source, S);
+      const double fe = 0.25 * (has_g ? (neg ? Ua - g : Ua + g) : Ua);
+      double v = old + om * (fe - old);
+      if (add_src && (a < 2 || add_src_f)) v = v + swB;
       if (repaired) {
-        switch (a) {
-          case 0: v = v - ff * (cxd * d11 + cyd * d12); break;
-          case 1: v = v - ff * (cxd * d21 + cyd * d22); break;
-          default: v = v + qt * (Fn[a - 2] - S[a]); break;
+        if (a < 2) {
+          const double t = cq != 0 ? tx : ty;
+          v = neg ? v + t : v - t;
+        } else {
+          v = v + rF;
         }
       }
-      if (to_node)
+      const int d = dst[q];
+      if (d >= 0)
         f1[(size_t)(q * 6 + a) * N + d] = v;
-      else if (ell_out >= 0)
-        fz.scratch[(size_t)ell_out * 6 + a] = v;
+      else if (d <= -2)
+        fz.scratch[(size_t)(-2 - d) * 6 + a] = v;
     }
   }
   const double dt = p.dt;
