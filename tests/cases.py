@@ -88,7 +88,7 @@ def solver_2d(cfg, geom=None, **overrides):
 
     geom = geom or geometry_2d(cfg["geometry"])
     m = cfg["material"]
-    material = WarpHyperelasticMaterial.from_poisson(m["model"], m["poisson"], mu=m["mu"])
+    material = WarpHyperelasticMaterial.from_poisson(m["model"], m["poisson"], mu=m["mu"], **m.get("extra", {}))
     kw = dict(cfg["solver"])
     if "source_vector" in kw:
         kw["source_vector"] = tuple(kw["source_vector"])
@@ -103,7 +103,7 @@ def solver_3d(cfg, geom=None, **overrides):
 
     geom = geom or geometry_3d(cfg["geometry"])
     m = cfg["material"]
-    material = c3.WarpHyperelasticMaterial3D.from_poisson(m["model"], m["poisson"], mu=m["mu"])
+    material = c3.WarpHyperelasticMaterial3D.from_poisson(m["model"], m["poisson"], mu=m["mu"], **m.get("extra", {}))
     kw = dict(cfg["solver"])
     kw.update(overrides)
     return c3.WarpSparseCurvedBoundaryLBM3D(

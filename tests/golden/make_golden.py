@@ -326,6 +326,40 @@ CASES_3D = {
 }
 
 # Geometry-only pins (tables are compared bit for bit).
+# One small case per material law other than neo-Hooke: the 2-D traction
+# annulus (local_f closure, sweep, repair) from a perturbed state, and a 3-D
+# traction shell, so that every branch of the Piola maps (and of the normal
+# solves that use them) is exercised.
+MATERIALS_2D = {
+    "svk": {},
+    "log_neo_hooke": {},
+    "mooney_rivlin": {"mooney_c01_fraction": 0.3},
+    "yeoh": {"yeoh_c2": 0.08, "yeoh_c3": 0.02},
+    "gent": {"gent_jm": 20.0},
+    "sugiyama_svk": {},
+}
+MATERIALS_3D = {
+    "svk": {},
+    "log_neo_hooke": {},
+    "mooney_rivlin": {"mooney_c01_fraction": 0.3},
+    "yeoh": {"yeoh_c2": 0.08, "yeoh_c3": 0.02},
+    "gent": {"gent_jm": 20.0},
+    "sph_neo_hooke": {},
+}
+for _m, _extra in MATERIALS_2D.items():
+    _c = json.loads(json.dumps(CASES_2D["g2_traction_localf"]))
+    _c["geometry"]["nx"] = _c["geometry"]["ny"] = 20
+    _c["material"] = dict(model=_m, poisson=0.25, mu=1.0, extra=_extra)
+    _c["init"] = dict(kind="identity_perturbed", init_order=2)
+    _c["steps"] = 8
+    CASES_2D[f"g2_mat_{_m}"] = _c
+for _m, _extra in MATERIALS_3D.items():
+    _c = json.loads(json.dumps(CASES_3D["g3_shell_localf"]))
+    _c["geometry"]["nx"] = _c["geometry"]["ny"] = _c["geometry"]["nz"] = 14
+    _c["material"] = dict(model=_m, poisson=0.25, mu=1.0, extra=_extra)
+    _c["steps"] = 4
+    CASES_3D[f"g3_mat_{_m}"] = _c
+
 GEOMETRY_CASES = {
     "geo2_circle_fd_normal": dict(dim=2, kind="circle_fd", nx=30, ny=30, radius=0.37),
     "geo2_superellipse": dict(
@@ -414,7 +448,7 @@ def run_2d(c2, v2, name, case, out_dir):
     t0 = time.time()
     geom = build_geometry_2d(c2, case["geometry"])
     mat = case["material"]
-    material = v2.WarpHyperelasticMaterial.from_poisson(mat["model"], mat["poisson"], mu=mat["mu"])
+    material = v2.WarpHyperelasticMaterial.from_poisson(mat["model"], mat["poisson"], mu=mat["mu"], **mat.get("extra", {}))
     boundary = c2.CurvedBoundarySpec(**boundary_kwargs(case["boundary"]))
     solver_kw = dict(case["solver"])
     if "source_vector" in solver_kw:
@@ -486,7 +520,7 @@ def run_3d(c3, name, case, out_dir):
     t0 = time.time()
     geom = build_geometry_3d(c3, case["geometry"])
     mat = case["material"]
-    material = c3.WarpHyperelasticMaterial3D.from_poisson(mat["model"], mat["poisson"], mu=mat["mu"])
+    material = c3.WarpHyperelasticMaterial3D.from_poisson(mat["model"], mat["poisson"], mu=mat["mu"], **mat.get("extra", {}))
     boundary = c3.CurvedBoundarySpec3D(**boundary_kwargs(case["boundary"]))
     solver = c3.WarpSparseCurvedBoundaryLBM3D(geom, material=material, boundary=boundary, **case["solver"])
     U_id = np.zeros((12, solver.n_active))

@@ -126,7 +126,7 @@ def test_host_initial_populations_2d(golden_dir, name):
     d, cfg = cases.load(golden_dir / f"{name}.npz")
     g = cases.geometry_2d(cfg["geometry"])
     m = cfg["material"]
-    mat = v2.WarpHyperelasticMaterial.from_poisson(m["model"], m["poisson"], mu=m["mu"])
+    mat = v2.WarpHyperelasticMaterial.from_poisson(m["model"], m["poisson"], mu=m["mu"], **m.get("extra", {}))
     s = cfg["solver"]
     c = s["lattice_speed"]
     dt = g.dx / c
@@ -162,7 +162,7 @@ def test_host_initial_populations_3d(golden_dir):
         U = np.zeros((12, n))
         U[3] = U[7] = U[11] = 1.0
         m = cfg["material"]
-        mat = v3.WarpHyperelasticMaterial3D.from_poisson(m["model"], m["poisson"], mu=m["mu"])
+        mat = v3.WarpHyperelasticMaterial3D.from_poisson(m["model"], m["poisson"], mu=m["mu"], **m.get("extra", {}))
         c = cfg["solver"]["lattice_speed"]
         g = cases.geometry_3d(cfg["geometry"])
         dt = g.dx / c

@@ -15,6 +15,11 @@ RTOL = 1e-12
 ATOL = 1e-15
 GOLD2 = ["g2_affine_compat", "g2_traction_localf", "g2_bfl_mixed_fd", "g2_energy_intervals"]
 GOLD3 = ["g3_shell_localf", "g3_shell_bfl_fd", "g3_shell_compat"]
+# one case per material law other than neo-Hooke (tests/golden/make_golden.py)
+GOLD2 += [f"g2_mat_{m}" for m in ("svk", "log_neo_hooke", "mooney_rivlin", "yeoh", "gent",
+                                   "sugiyama_svk")]
+GOLD3 += [f"g3_mat_{m}" for m in ("svk", "log_neo_hooke", "mooney_rivlin", "yeoh", "gent",
+                                   "sph_neo_hooke")]
 
 
 def close(name, got, ref, rtol=RTOL, atol=ATOL):
@@ -32,7 +37,7 @@ def oracle_2d(cfg, **kw):
 
     g = cases.geometry_2d(cfg["geometry"])
     m = cfg["material"]
-    mat = WarpHyperelasticMaterial.from_poisson(m["model"], m["poisson"], mu=m["mu"])
+    mat = WarpHyperelasticMaterial.from_poisson(m["model"], m["poisson"], mu=m["mu"], **m.get("extra", {}))
     spec = c2.CurvedBoundarySpec(**cases.boundary_kwargs(cfg["boundary"]))
     return Oracle2D(g, material=mat, boundary=spec, **cfg["solver"], **kw)
 
@@ -43,7 +48,7 @@ def oracle_3d(cfg, **kw):
 
     g = cases.geometry_3d(cfg["geometry"])
     m = cfg["material"]
-    mat = c3.WarpHyperelasticMaterial3D.from_poisson(m["model"], m["poisson"], mu=m["mu"])
+    mat = c3.WarpHyperelasticMaterial3D.from_poisson(m["model"], m["poisson"], mu=m["mu"], **m.get("extra", {}))
     spec = c3.CurvedBoundarySpec3D(**cases.boundary_kwargs(cfg["boundary"]))
     return Oracle3D(g, material=mat, boundary=spec, **cfg["solver"], **kw)
 

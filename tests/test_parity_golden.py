@@ -22,6 +22,11 @@ ATOL = 1e-15
 
 GOLD2 = ["g2_affine_compat", "g2_traction_localf", "g2_bfl_mixed_fd", "g2_energy_intervals"]
 GOLD3 = ["g3_shell_localf", "g3_shell_bfl_fd", "g3_shell_compat"]
+# one case per material law other than neo-Hooke (tests/golden/make_golden.py)
+GOLD2 += [f"g2_mat_{m}" for m in ("svk", "log_neo_hooke", "mooney_rivlin", "yeoh", "gent",
+                                   "sugiyama_svk")]
+GOLD3 += [f"g3_mat_{m}" for m in ("svk", "log_neo_hooke", "mooney_rivlin", "yeoh", "gent",
+                                   "sph_neo_hooke")]
 
 
 def close(name, got, ref, rtol=RTOL, atol=ATOL):
