@@ -536,33 +536,43 @@ Overlap2* overlap_resources(cudaStream_t s) {
 }
 
 using FusedFn2 = void (*)(Ctx2, Fused2, const double*, double*, double*, double*, const double*,
-                          double*, int*, const double*, double, int, int);
+                          double*, int*, const double*, double, int, int, const double*);
+using MomFn2 = void (*)(Ctx2, Fused2, const double*, const double*, double*);
+
 struct FusedLaunch2 {
   FusedFn2 fn;
   int threads;
   size_t smem;
   int tile_i;
+  MomFn2 mom;  // PRE form: moments kernel launched before the tile kernel, else null
 };
 
-// Compiled tile variants: (tile rows, resident blocks per SM).  The tile list
-// in the problem must have been built for the variant's tile height.
-// Variant 5 selects the split form (cvlbm2d_split.cuh) instead of a tile shape.
+// Compiled tile variants: (tile rows, resident blocks per SM, PRE).  The tile
+// list in the problem must have been built for the variant's tile height.
+// Variant 5 selects the split form (cvlbm2d_split.cuh) instead of a tile
+// shape; variants 6 and 7 are the PRE form (moments of every active node
+// written once per step by k_mom2 into fields->fpost, halo moments read from
+// there instead of recomputed), which runs without the link overlap.
 constexpr int kSplitVariant = 5;
+constexpr int kMaxVariant = 7;
 
 FusedLaunch2 fused_variant(int v) {
   switch (v) {
-    case 1: return {k_fused2<8, 2>, kTX * 8, fused_smem2<8>(), 8};
-    case 2: return {k_fused2<8, 3>, kTX * 8, fused_smem2<8>(), 8};
-    case 3: return {k_fused2<16, 2>, kTX * 16, fused_smem2<16>(), 16};
-    case 4: return {k_fused2<4, 4>, kTX * 4, fused_smem2<4>(), 4};
-    case kSplitVariant: return {nullptr, 0, 0, 16};  // split kernels, no tiles used
-    default: return {k_fused2<16, 1>, kTX * 16, fused_smem2<16>(), 16};
+    case 1: return {k_fused2<8, 2, false>, kTX * 8, fused_smem2<8>(), 8, nullptr};
+    case 2: return {k_fused2<8, 3, false>, kTX * 8, fused_smem2<8>(), 8, nullptr};
+    case 3: return {k_fused2<16, 2, false>, kTX * 16, fused_smem2<16>(), 16, nullptr};
+    case 4: return {k_fused2<4, 4, false>, kTX * 4, fused_smem2<4>(), 4, nullptr};
+    case kSplitVariant: return {nullptr, 0, 0, 16, nullptr};  // split kernels, no tiles used
+    case 6: return {k_fused2<16, 1, true>, kTX * 16, fused_smem2<16>(), 16, k_mom2<16>};
+    case 7: return {k_fused2<8, 3, true>, kTX * 8, fused_smem2<8>(), 8, k_mom2<8>};
+    default: return {k_fused2<16, 1, false>, kTX * 16, fused_smem2<16>(), 16, nullptr};
   }
 }
 
 bool fused_ok(const cvlbm2d_problem* p, const cvlbm2d_fields* f) {
+  const FusedLaunch2 fl = fused_variant(p->tile_variant);
   return p->tiles && p->need_fields && p->link_partner && f->link_scratch && p->lsq_node &&
-         p->disp_sweeps <= 1 && fused_variant(p->tile_variant).tile_i == p->tile_i;
+         p->disp_sweeps <= 1 && fl.tile_i == p->tile_i && (!fl.mom || f->fpost);
 }
 
 }  // namespace
@@ -589,8 +599,8 @@ extern "C" int cvlbm2d_run(const cvlbm2d_problem* p, cvlbm2d_fields* f, double t
   double* us_cur = f->u_star;
   double* us_nxt = f->u_next;
   Overlap2* ov = nullptr;
-  if (fused && !split && p->overlap && p->n_tiles_inner > 0 && p->n_tiles_inner < p->n_tiles &&
-      nsteps > 0) {
+  if (fused && !split && !fl.mom && p->overlap && p->n_tiles_inner > 0 &&
+      p->n_tiles_inner < p->n_tiles && nsteps > 0) {
     ov = overlap_resources(s);
     if (ov) {
       cudaEventRecord(ov->boundary_done, s);  // the inner stream starts after prior work
@@ -635,12 +645,13 @@ extern "C" int cvlbm2d_run(const cvlbm2d_problem* p, cvlbm2d_fields* f, double t
         cudaStreamWaitEvent(ov->inner, ov->boundary_done, 0);
       }
       fl.fn<<<n_bd, fl.threads, fl.smem, s>>>(c, fz_bd, f->f0, f->f1, f->U, f->u, us_cur,
-                                              us_nxt, f->invalid, clock, t, sweep, repair);
+                                              us_nxt, f->invalid, clock, t, sweep, repair,
+                                              nullptr);
       cudaEventRecord(ov->boundary_done, s);
       // inner tiles read no time (they have no cut-point anchors)
       fl.fn<<<n_in, fl.threads, fl.smem, ov->inner>>>(c, fz_in, f->f0, f->f1, f->U, f->u, us_cur,
                                                       us_nxt, f->invalid, nullptr, t, sweep,
-                                                      repair);
+                                                      repair, nullptr);
       cudaEventRecord(ov->inner_done, ov->inner);
       cv::count_launches(2);
       double* us = us_cur;
@@ -653,8 +664,13 @@ extern "C" int cvlbm2d_run(const cvlbm2d_problem* p, cvlbm2d_fields* f, double t
                 f->link_scratch, k == nsteps - 1};
       int tk = timer_begin(s);
       if (p->n_tiles > 0) {
+        if (fl.mom) {
+          fl.mom<<<p->n_tiles, fl.threads, 0, s>>>(c, fz, f->f0, us_cur, f->fpost);
+          cv::count_launches(1);
+        }
         fl.fn<<<p->n_tiles, fl.threads, fl.smem, s>>>(c, fz, f->f0, f->f1, f->U, f->u, us_cur,
-                                                      us_nxt, f->invalid, clock, t, sweep, repair);
+                                                      us_nxt, f->invalid, clock, t, sweep, repair,
+                                                      f->fpost);
         cv::count_launches(1);
       }
       double* us = us_cur;
@@ -731,7 +747,7 @@ extern "C" int cvlbm2d_refresh(const cvlbm2d_problem* p, cvlbm2d_fields* f, void
 }
 
 extern "C" int cvlbm2d_tile_variant(int32_t v) {
-  if (v < 0 || v > kSplitVariant) return 0;
+  if (v < 0 || v > kMaxVariant) return 0;
   return fused_variant(v).tile_i;
 }
 

@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(kTX * TY, MINB)
     const int sweep = p.disp_interval > 0 && step % p.disp_interval == 0;
     const int repair = p.rep_interval > 0 && step % p.rep_interval == 0;
     Fused2 fz{nullptr, 0, p.tiles_j, I.need, I.partner, I.scratch, store_all};
-    fused2_tile<TY>(I.c, fz, wk.y, I.f[par], I.f[par ^ 1], I.U, I.u, I.us[par], I.us[par ^ 1],
+    fused2_tile<TY, false>(I.c, fz, wk.y, I.f[par], I.f[par ^ 1], I.U, I.u, I.us[par], I.us[par ^ 1],
                     I.invalid, &st[wk.x].clock, 0.0, sweep, repair, smem2);
   }
 }
@@ -319,7 +319,7 @@ extern "C" int cvlbm2d_batch_create(int32_t n_inst, const cvlbm2d_problem* probl
     return fail(CVLBM_ERR_INVALID_ARG, "cvlbm2d_batch_create: bad arguments");
   *out = nullptr;
   const int tile_i = cvlbm2d_tile_variant(tile_variant);
-  if (tile_i <= 0 || tile_variant == kSplitVariant)
+  if (tile_i <= 0 || tile_variant >= kSplitVariant)
     return fail(CVLBM_ERR_INVALID_ARG, "cvlbm2d_batch_create: unknown tile variant");
   std::vector<Inst2> hi(n_inst);
   std::vector<InstState2> hs(n_inst);

@@ -64,13 +64,17 @@ constexpr size_t fused_smem2() {
 
 // One tile of the fused step (phases A-C above); `tile` is a tile id of the
 // problem's tile list.  Every thread of the block calls it; it returns
-// early only after the last block-wide barrier.
-template <int TY>
+// early only after the last block-wide barrier.  PRE: the collide-time
+// moments of every active node were written by k_mom2 into `mom` this step
+// ([8][N]: U (6), collide-time u (2)), so phase A reads them instead of
+// summing populations (the same doubles: k_mom2 evaluates the same sums).
+template <int TY, bool PRE = false>
 __device__ __forceinline__ void fused2_tile(
     const Ctx2& c, const Fused2& fz, int tile, const double* __restrict__ f0,
     double* __restrict__ f1, double* __restrict__ Ug, double* __restrict__ ug,
     const double* __restrict__ ustar, double* __restrict__ ustar_out, int* __restrict__ invalid,
-    const double* clock, double t_host, int do_sweep, int do_repair, double* smem2) {
+    const double* clock, double t_host, int do_sweep, int do_repair, double* smem2,
+    const double* __restrict__ mom = nullptr) {
   constexpr int kTY = TY;
   constexpr int kRN = kRX * (TY + 2 * kH);
   constexpr int kSN = kSX * (TY + 4);
@@ -93,9 +97,16 @@ __device__ __forceinline__ void fused2_tile(
   double S[6];
   double ucol0 = 0.0, ucol1 = 0.0;
   if (own_act) {
-    moments2(p, f0, N, n, S);
-    ucol0 = ustar[n] + 0.5 * p.dt * S[0];
-    ucol1 = ustar[N + n] + 0.5 * p.dt * S[1];
+    if constexpr (PRE) {
+#pragma unroll
+      for (int a = 0; a < 6; ++a) S[a] = mom[(size_t)a * N + n];
+      ucol0 = mom[6 * (size_t)N + n];
+      ucol1 = mom[7 * (size_t)N + n];
+    } else {
+      moments2(p, f0, N, n, S);
+      ucol0 = ustar[n] + 0.5 * p.dt * S[0];
+      ucol1 = ustar[N + n] + 0.5 * p.dt * S[1];
+    }
   }
   for (int r = threadIdx.x; r < kRN; r += blockDim.x) {
     const int ri = r / kRX, rj = r - ri * kRX;
@@ -107,14 +118,21 @@ __device__ __forceinline__ void fused2_tile(
     const int act = inb ? p.active[m] : 0;
     sA[r] = act;
     if (act) {
-      double Sh[6];
-      moments2(p, f0, N, m, Sh);
-      sF[0][r] = Sh[2];
-      sF[1][r] = Sh[3];
-      sF[2][r] = Sh[4];
-      sF[3][r] = Sh[5];
-      sU[0][r] = ustar[m] + 0.5 * p.dt * Sh[0];
-      sU[1][r] = ustar[N + m] + 0.5 * p.dt * Sh[1];
+      if constexpr (PRE) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) sF[k][r] = mom[(size_t)(2 + k) * N + m];
+        sU[0][r] = mom[6 * (size_t)N + m];
+        sU[1][r] = mom[7 * (size_t)N + m];
+      } else {
+        double Sh[6];
+        moments2(p, f0, N, m, Sh);
+        sF[0][r] = Sh[2];
+        sF[1][r] = Sh[3];
+        sF[2][r] = Sh[4];
+        sF[3][r] = Sh[5];
+        sU[0][r] = ustar[m] + 0.5 * p.dt * Sh[0];
+        sU[1][r] = ustar[N + m] + 0.5 * p.dt * Sh[1];
+      }
     } else {
       sF[0][r] = sF[1][r] = sF[2][r] = sF[3][r] = 0.0;
       sU[0][r] = sU[1][r] = 0.0;
@@ -375,16 +393,39 @@ __device__ __forceinline__ void fused2_tile(
 
 // Tile kTX x TY, one node per thread; MINB resident blocks per SM bounds the
 // registers per thread (tuned per problem, see curved_lbm autotune).
-template <int TY, int MINB>
+template <int TY, int MINB, bool PRE>
 __global__ void __launch_bounds__(kTX * TY, MINB)
     k_fused2(Ctx2 c, Fused2 fz, const double* __restrict__ f0, double* __restrict__ f1,
              double* __restrict__ Ug, double* __restrict__ ug,
              const double* __restrict__ ustar, double* __restrict__ ustar_out,
              int* __restrict__ invalid, const double* clock, double t_host, int do_sweep,
-             int do_repair) {
+             int do_repair, const double* __restrict__ mom) {
   extern __shared__ double smem2[];
-  fused2_tile<TY>(c, fz, fz.tiles[blockIdx.x], f0, f1, Ug, ug, ustar, ustar_out, invalid, clock,
-                  t_host, do_sweep, do_repair, smem2);
+  fused2_tile<TY, PRE>(c, fz, fz.tiles[blockIdx.x], f0, f1, Ug, ug, ustar, ustar_out, invalid,
+                       clock, t_host, do_sweep, do_repair, smem2, mom);
+}
+
+// Collide-time moments of the active nodes of the listed tiles, for the PRE
+// form of the tile kernel: mom[0..5] = U with the damping half step
+// (moments2), mom[6..7] = u* + dt/2 v.  One thread per node, coalesced rows.
+template <int TY>
+__global__ void __launch_bounds__(kTX * TY)
+    k_mom2(Ctx2 c, Fused2 fz, const double* __restrict__ f0, const double* __restrict__ ustar,
+           double* __restrict__ mom) {
+  const cvlbm2d_problem& p = c.p;
+  const int N = c.N;
+  const int tile = fz.tiles[blockIdx.x];
+  const int i = (tile / fz.tiles_j) * TY + (threadIdx.x >> 5);
+  const int j = (tile % fz.tiles_j) * kTX + (threadIdx.x & 31);
+  if (i >= p.nx || j >= p.ny) return;
+  const int n = i * p.ny + j;
+  if (p.active[n] == 0) return;
+  double S[6];
+  moments2(p, f0, N, n, S);
+#pragma unroll
+  for (int a = 0; a < 6; ++a) mom[(size_t)a * N + n] = S[a];
+  mom[6 * (size_t)N + n] = ustar[n] + 0.5 * p.dt * S[0];
+  mom[7 * (size_t)N + n] = ustar[N + n] + 0.5 * p.dt * S[1];
 }
 
 // ---------------------------------------------------------------------------
