@@ -473,7 +473,10 @@ __device__ __forceinline__ void link2_group(
   const cvlbm2d_problem& p = c.p;
   const Mat& m = c.m;
   const bool live = slot < p.n_links;
-  const int ell = live ? (p.link_order ? p.link_order[slot] : slot) : 0;
+  // with link rows every per-link input the chain starts from is one load
+  // away from the slot (no link_order / link-table / stencil-id indirection)
+  const cvlbm2d_link_row* row = (live && p.link_rows) ? p.link_rows + slot : nullptr;
+  const int ell = live ? (row ? row->ell : (p.link_order ? p.link_order[slot] : slot)) : 0;
   const int N = c.N, nx = p.nx, ny = p.ny, recon = p.recon;
   const double tmid = time_of(clock, t_host, offset);
 
@@ -482,50 +485,72 @@ __device__ __forceinline__ void link2_group(
   bool up_ok = false, lsq_ok = false;
   const double* pp = p.bc_params;
   if (live) {
-    i = p.link_i[ell];
-    j = p.link_j[ell];
-    qo = p.link_q[ell];
-    int bid = p.link_bid[ell];
+    int bid;
+    if (row) {
+      i = row->i;
+      j = row->j;
+      qo = row->q;
+      bid = row->bid;
+      eta = row->eta;
+      xb = row->xb;
+      yb = row->yb;
+      nxb = row->nx;
+      nyb = row->ny;
+      n = row->node;
+      up_ok = row->upstream >= 0;
+      nu = up_ok ? row->upstream : n;
+      lsq_ok = row->lsq_valid != 0;
+    } else {
+      i = p.link_i[ell];
+      j = p.link_j[ell];
+      qo = p.link_q[ell];
+      bid = p.link_bid[ell];
+      eta = p.link_eta[ell];
+      xb = p.link_xb[ell];
+      yb = p.link_yb[ell];
+      nxb = p.link_nx[ell];
+      nyb = p.link_ny[ell];
+      n = i * ny + j;
+      const int iu = i - cx2(qo), ju = j - cy2(qo);
+      up_ok = iu >= 0 && iu < nx && ju >= 0 && ju < ny && p.active[iu * ny + ju] != 0;
+      nu = up_ok ? iu * ny + ju : n;
+      lsq_ok = p.lsq_valid[ell] != 0;
+    }
     if (bid < 0 || bid >= kMaxIds2) bid = 0;
     kind = p.bc_kind[bid];
     mode = p.bc_mode[bid];
     pp = p.bc_params + bid * 8;
     qi = qo + 2;
     if (qi >= 4) qi -= 4;
-    eta = p.link_eta[ell];
-    xb = p.link_xb[ell];
-    yb = p.link_yb[ell];
-    nxb = p.link_nx[ell];
-    nyb = p.link_ny[ell];
-    n = i * ny + j;
     bv0 = value2(0, mode, pp, xb, yb, nxb, nyb, tmid);
     bv1 = value2(1, mode, pp, xb, yb, nxb, nyb, tmid);
     if (kind == kNeumann && p.use_dynamic_traction != 0) {
       bv0 = p.traction_x[ell];
       bv1 = p.traction_y[ell];
     }
-    const int iu = i - cx2(qo), ju = j - cy2(qo);
-    up_ok = iu >= 0 && iu < nx && ju >= 0 && ju < ny && p.active[iu * ny + ju] != 0;
-    nu = up_ok ? iu * ny + ju : n;
-    lsq_ok = p.lsq_valid[ell] != 0;
   }
+  // stencil ids and weights of this link (slot order when rows are given)
+  const size_t sl = (size_t)(row ? slot : ell) * kMaxLsq2;
+  const int* lnode = (row ? p.lsq_node_slot : p.lsq_node) + sl;
+  const double* w_b = (row ? p.lsq_wb_slot : p.lsq_wb) + sl;
+  const double* w_t = (row ? p.lsq_wt_slot : p.lsq_wt) + sl;
+  const double* w_x = (row ? p.lsq_wx_slot : p.lsq_wx) + sl;
+  const double* w_y = (row ? p.lsq_wy_slot : p.lsq_wy) + sl;
   const bool use_char = live && (recon == 11 || recon == 12) && kind == kNeumann && lsq_ok;
   const bool compat = live && (recon == 9 || recon == 11) && lsq_ok;
-  const int* lnode = p.lsq_node + (size_t)ell * kMaxLsq2;
 
   // -- gathers ----------------------------------------------------------------
   if (live) {
     if (lane < 12) {
       const int a = lane < 6 ? lane : lane - 6;
       if (use_char) {
-        const double* w = (lane < 6 ? p.lsq_wx : p.lsq_wy) + (size_t)ell * kMaxLsq2;
-        const double g = lsq_sum(lnode, w, U + (size_t)a * N);
+        const double g = lsq_sum(lnode, lane < 6 ? w_x : w_y, U + (size_t)a * N);
         if (lane < 6)
           S.ux[a] = g;
         else
           S.uy[a] = g;
       } else if (compat && kind == kNeumann && lane < 2) {
-        const double* wt = p.lsq_wt + (size_t)ell * kMaxLsq2;
+        const double* wt = w_t;
         double d = 0.0, wa = 0.0;
         for (int mm = 0; mm < kMaxLsq2; ++mm) {
           const int nd = lnode[mm];
@@ -541,14 +566,14 @@ __device__ __forceinline__ void link2_group(
       const int k = lane - 12;
       const double* Uk = U + (size_t)(2 + k) * N;
       double fg;
-      if (recon == 0 || recon == 2 || recon == 13) {
+      if ((recon == 11 || recon == 12) && lsq_ok) {
+        fg = lsq_sum(lnode, w_b, Uk);
+      } else if (recon == 0 || recon == 2 || recon == 13) {
         fg = up_ok ? Uk[n] + eta * (Uk[n] - Uk[nu]) : Uk[n];
-        if (recon == 2 && lsq_ok) fg = lsq_sum(lnode, p.lsq_wb + (size_t)ell * kMaxLsq2, Uk);
+        if (recon == 2 && lsq_ok) fg = lsq_sum(lnode, w_b, Uk);
       } else {
         fg = interp_link(Uk, p.active, i, j, qo, eta, nx, ny);
       }
-      if ((recon == 11 || recon == 12) && lsq_ok)
-        fg = lsq_sum(lnode, p.lsq_wb + (size_t)ell * kMaxLsq2, Uk);
       S.Fg[k] = fg;
     }
   }

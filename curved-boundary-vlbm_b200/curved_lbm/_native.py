@@ -49,7 +49,20 @@ class Problem2D(C.Structure):
         ("tiles", pI), ("n_tiles", i32), ("tiles_j", i32), ("need_fields", pI),
         ("link_partner", pI), ("lsq_node", pI), ("link_order", pI),
         ("tile_variant", i32), ("tile_i", i32), ("n_tiles_inner", i32), ("overlap", i32),
+        ("link_rows", pI), ("lsq_node_slot", pI), ("lsq_wb_slot", pI), ("lsq_wt_slot", pI),
+        ("lsq_wx_slot", pI), ("lsq_wy_slot", pI),
     ]
+
+
+def link_row2_dtype():
+    """cvlbm2d_link_row (96 bytes) as a NumPy record."""
+    import numpy as np
+
+    return np.dtype({"names": ["ell", "node", "upstream", "q", "bid", "lsq_valid", "i", "j",
+                               "eta", "xb", "yb", "nx", "ny"],
+                     "formats": ["<i4"] * 8 + ["<f8"] * 5,
+                     "offsets": [0, 4, 8, 12, 16, 20, 24, 28, 32, 40, 48, 56, 64],
+                     "itemsize": 96})
 
 
 class Fields2D(C.Structure):

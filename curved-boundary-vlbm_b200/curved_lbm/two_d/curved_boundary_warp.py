@@ -488,7 +488,29 @@ class WarpCurvedBoundaryLBM2D:
         t["lsq_node"] = dev_i(np.where((li_np >= 0) & (lj_np >= 0), li_np * self.ny + lj_np, -1))
         # traction (Neumann) links first, then by node: a warp's links share branches
         link_kind = kind[np.clip(geometry.link_boundary_id, 0, MAX_BOUNDARY_IDS - 1)]
-        t["link_order"] = dev_i(np.lexsort((np.arange(nl), link_kind != BC_NEUMANN)))
+        order = np.lexsort((np.arange(nl), link_kind != BC_NEUMANN))
+        t["link_order"] = dev_i(order)
+        # the link kernel's first loads, one row per processing slot
+        rows = np.zeros(nl, dtype=_native.link_row2_dtype())
+        li_o, lj_o, lq_o = (np.asarray(getattr(geometry, k))[order].astype(np.int64)
+                            for k in ("link_i", "link_j", "link_q"))
+        rows["ell"], rows["i"], rows["j"], rows["q"] = order, li_o, lj_o, lq_o
+        rows["node"] = li_o * self.ny + lj_o
+        ui, uj = li_o - _CX[lq_o], lj_o - _CY[lq_o]
+        inb = (ui >= 0) & (ui < self.nx) & (uj >= 0) & (uj < self.ny)
+        up_act = np.zeros(nl, dtype=bool)
+        up_act[inb] = self.active_np[ui[inb], uj[inb]] != 0
+        rows["upstream"] = np.where(up_act, ui * self.ny + uj, -1)
+        bid = np.asarray(geometry.link_boundary_id)[order]
+        rows["bid"] = np.where((bid >= 0) & (bid < MAX_BOUNDARY_IDS), bid, 0)
+        rows["lsq_valid"] = np.asarray(lsq_valid)[order]
+        for k in ("eta", "xb", "yb", "nx", "ny"):
+            rows[k] = np.asarray(getattr(geometry, "link_" + k))[order]
+        t["link_rows"] = torch.as_tensor(rows.view(np.uint8), device=dev)
+        lsq_node_np = np.where((li_np >= 0) & (lj_np >= 0), li_np * self.ny + lj_np, -1)
+        t["lsq_node_slot"] = dev_i(np.asarray(lsq_node_np)[order])
+        for k, w in (("wb", lsq_wb), ("wt", lsq_wt), ("wx", lsq_wx), ("wy", lsq_wy)):
+            t[f"lsq_{k}_slot"] = dev_f(np.asarray(w)[order])
         self.link_scratch = torch.zeros(max(6 * nl, 1), dtype=f64, device=dev)
         self.link_traction_x = torch.zeros(nl, dtype=f64, device=dev)
         self.link_traction_y = torch.zeros(nl, dtype=f64, device=dev)

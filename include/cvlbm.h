@@ -61,6 +61,20 @@ typedef struct cvlbm_material {
 /* D2Q4x6                                                                    */
 /* ------------------------------------------------------------------------ */
 
+/* One cut link in processing order (see cvlbm2d_problem.link_rows): what the
+ * link kernel reads first, in one 96-byte row. */
+typedef struct cvlbm2d_link_row {
+  int32_t ell;       /* link id (index of the per-link tables) */
+  int32_t node;      /* i*ny + j */
+  int32_t upstream;  /* node (i,j) - c_q when it is active, else -1 */
+  int32_t q;         /* outgoing direction */
+  int32_t bid;       /* boundary id, clamped to [0, 8) */
+  int32_t lsq_valid;
+  int32_t i, j;
+  double eta, xb, yb, nx, ny;
+  double reserved[3];
+} cvlbm2d_link_row;
+
 /* Static description of one 2-D problem: lattice, material, boundary tables
  * and cut-link geometry.  Mirrors the constructor state of
  * WarpCurvedBoundaryLBM2D (two_d/curved_boundary_warp.py:3621-3843). */
@@ -111,6 +125,12 @@ typedef struct cvlbm2d_problem {
                                                  tiles (0: not classified) */
   int32_t overlap;                            /* nonzero: the next step's inner tiles run on
                                                  a second stream while the link kernel runs */
+  /* cut links in processing order (optional): one row per slot, and the
+     LSQ stencil node ids and weights in slot order, so that the link kernel
+     starts its stencil gathers after one level of loads */
+  const cvlbm2d_link_row *link_rows;          /* [n_links] */
+  const int32_t *lsq_node_slot;               /* [n_links*24] */
+  const double *lsq_wb_slot, *lsq_wt_slot, *lsq_wx_slot, *lsq_wy_slot;
 } cvlbm2d_problem;
 
 /* Tile rows (i extent, tiles are 32 nodes wide in j) of fused-kernel variant
