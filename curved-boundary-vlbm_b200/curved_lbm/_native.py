@@ -224,6 +224,15 @@ def load(require_cuda: bool = True):
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
+    # a library built from another header would read these structs with
+    # another layout: refuse it before any call can pass one
+    mirrors = (Problem2D, Fields2D, Problem3D, Fields3D, StencilInput3D)
+    for which, cls in enumerate(mirrors):
+        have = int(lib.cvlbm_struct_size(which))
+        if have != C.sizeof(cls):
+            raise RuntimeError(
+                f"{path} was built for another ABI: sizeof({cls.__name__}) is {have} there and "
+                f"{C.sizeof(cls)} in this binding; rebuild it (curved_lbm._build.build())")
     _lib = lib
     return lib
 
