@@ -584,6 +584,30 @@ Overlap3* overlap3_resources(cudaStream_t s) {
   return &(g_overlap3[key] = o);
 }
 
+// Persistent grid of the wavefront kernel: the blocks one device holds at
+// once (all resident, each taking items until none are left).
+template <int MINB>
+int wave_grid() {
+  static std::mutex mu;
+  static std::map<int, int> cache;
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = cache.find(dev);
+  if (it != cache.end()) return it->second;
+  int sms = 0, per = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k3_wave<MINB>, 128, 0);
+  if (per < 1) per = 1;
+  if (sms < 1) sms = 1;
+  return cache[dev] = sms * per;
+}
+
+bool wave_ok3(const cvlbm3d_problem* p, const cvlbm3d_fields* f) {
+  return (p->node_variant == 3 || p->node_variant == 4) && p->wave_items && p->n_wave_items > 0 && p->n_planes > 0 &&
+         p->wave_plane_chunks && f->wave_sync;
+}
+
 Ctx3 make_ctx(const cvlbm3d_problem* p) {
   Ctx3 c;
   c.p = *p;
@@ -615,16 +639,30 @@ extern "C" int cvlbm3d_run(const cvlbm3d_problem* p, cvlbm3d_fields* f, double t
     // of step k + 1 at nodes without a cut link read f1 elsewhere and write
     // U and u_next.  So they run on a second stream after the collide of step
     // k, while the links do; the moments of the link nodes follow the links.
+    const bool wave = wave_ok3(p, f) && N > 0;
     Overlap3* ov = nullptr;
-    if (p->overlap && p->disp_interval == 1 && N > 0 && L > 0 && p->link_nodes &&
+    if (!wave && p->overlap && p->disp_interval == 1 && N > 0 && L > 0 && p->link_nodes &&
         p->n_link_nodes > 0 && nsteps > 1)
       ov = overlap3_resources(s);
+    const Wave3 wv{reinterpret_cast<const int4*>(p->wave_items), p->n_wave_items, p->n_planes,
+                   p->wave_plane_chunks, f->wave_sync};
     for (int k = 0; k < nsteps; ++k) {
       const long long step = step0 + k;
       const int sweep = N > 0 && due(p->disp_interval, step);
       const int repair = due(p->rep_interval, step);
       int tk = ov ? -1 : timer_begin(s);
-      if (N > 0 && ov && k > 0) {
+      if (wave) {
+        cudaMemsetAsync(f->wave_sync, 0, sizeof(int32_t) * (2 + 3 * (size_t)p->n_planes), s);
+        if (p->node_variant == 4)
+          k3_wave<3><<<wave_grid<3>(), 128, 0, s>>>(c, fz, wv, f->f0, f->f1, f->U, f->u_next,
+                                                     f->u, f->u_star, f->invalid, clock, t,
+                                                     sweep, repair, k == nsteps - 1);
+        else
+          k3_wave<4><<<wave_grid<4>(), 128, 0, s>>>(c, fz, wv, f->f0, f->f1, f->U, f->u_next,
+                                                     f->u, f->u_star, f->invalid, clock, t,
+                                                     sweep, repair, k == nsteps - 1);
+        cv::count_launches(1);
+      } else if (N > 0 && ov && k > 0) {
         cudaStreamWaitEvent(s, ov->inner_done, 0);
         k3_moments_part<1><<<blocks(p->n_link_nodes, 256), 256, 0, s>>>(
             c, f->f0, f->U, f->u_next, f->u_star, f->invalid, sweep);
@@ -634,7 +672,7 @@ extern "C" int cvlbm3d_run(const cvlbm3d_problem* p, cvlbm3d_fields* f, double t
                                                   f->u_star, f->invalid, sweep);
         cv::count_launches(1);
       }
-      if (N > 0) {
+      if (N > 0 && !wave) {
         if (sweep) {
           k3_sweep<<<blocks(N, 256), 256, 0, s>>>(c, f->U, f->u_next, f->u, f->u_star, clock, t);
           cv::count_launches(1);

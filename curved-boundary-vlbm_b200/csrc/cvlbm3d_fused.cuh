@@ -131,14 +131,21 @@ __device__ __forceinline__ void moments_node3(const Ctx3& c, const double* __res
 
 // One Jacobi sweep (three_d/curved_boundary_warp3d.py:2402-2540); ucol holds
 // the collide-time u of every node, the swept u goes to `u`.
-__global__ void __launch_bounds__(256) k3_sweep(Ctx3 c, const double* __restrict__ U,
-                                                const double* __restrict__ ucol,
-                                                double* __restrict__ u,
-                                                double* __restrict__ ustar, const double* clock,
-                                                double t_host) {
+// Loads of values that other blocks of the same launch write (the wavefront
+// kernel): through L2 only, so that no stale L1 line is read.
+template <bool CG>
+__device__ __forceinline__ double ldx(const double* q) {
+  if constexpr (CG)
+    return __ldcg(q);
+  else
+    return *q;
+}
+
+template <bool CG>
+__device__ __forceinline__ void sweep_node3(const Ctx3& c, const double* U, const double* ucol,
+                                            double* __restrict__ u, double* __restrict__ ustar,
+                                            const double* clock, double t_host, int n) {
   const int N = c.N;
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= N) return;
   const cvlbm3d_problem& p = c.p;
   double d[3] = {0.0, 0.0, 0.0}, r[3] = {0.0, 0.0, 0.0};
   const double time = time_of(clock, t_host, 0.5 * p.dt);
@@ -162,7 +169,8 @@ __global__ void __launch_bounds__(256) k3_sweep(Ctx3 c, const double* __restrict
       if (!(force_all || p.bc_comp_kind[comp * kMaxIds3 + bid] == kDirichlet)) continue;
       const double ub = disp3(mode, pp, comp, x, y, z, time);
       const double* F = U + (size_t)(3 + 3 * comp) * N;
-      double e0 = F[n], e1 = F[(size_t)N + n], e2 = F[2 * (size_t)N + n];
+      double e0 = ldx<CG>(F + n), e1 = ldx<CG>(F + (size_t)N + n),
+             e2 = ldx<CG>(F + 2 * (size_t)N + n);
       if (comp == 0) e0 = e0 - 1.0;
       if (comp == 1) e1 = e1 - 1.0;
       if (comp == 2) e2 = e2 - 1.0;
@@ -174,24 +182,26 @@ __global__ void __launch_bounds__(256) k3_sweep(Ctx3 c, const double* __restrict
   const double* Ub = U + 3 * (size_t)N;
   double Fs[9];
 #pragma unroll
-  for (int k = 0; k < 9; ++k) Fs[k] = Ub[(size_t)k * N + n];
+  for (int k = 0; k < 9; ++k) Fs[k] = ldx<CG>(Ub + (size_t)k * N + n);
 #pragma unroll
   for (int q = 0; q < kQ3; ++q) {
     const int m = p.neighbor[(size_t)q * N + n];
     if (m < 0) continue;
     const double ddx = (double)dx3(q) * p.dx, ddy = (double)dy3(q) * p.dy,
                  ddz = (double)dz3(q) * p.dz;
-    const double g0 = 0.5 * ((Fs[0] + Ub[m] - 2.0) * ddx + (Fs[1] + Ub[N + m]) * ddy +
-                             (Fs[2] + Ub[2 * (size_t)N + m]) * ddz);
-    const double g1 = 0.5 * ((Fs[3] + Ub[3 * (size_t)N + m]) * ddx +
-                             (Fs[4] + Ub[4 * (size_t)N + m] - 2.0) * ddy +
-                             (Fs[5] + Ub[5 * (size_t)N + m]) * ddz);
-    const double g2 = 0.5 * ((Fs[6] + Ub[6 * (size_t)N + m]) * ddx +
-                             (Fs[7] + Ub[7 * (size_t)N + m]) * ddy +
-                             (Fs[8] + Ub[8 * (size_t)N + m] - 2.0) * ddz);
-    r[0] += ucol[m] - g0;
-    r[1] += ucol[(size_t)N + m] - g1;
-    r[2] += ucol[2 * (size_t)N + m] - g2;
+    const double* Um = Ub + m;
+    const size_t NN = (size_t)N;
+    const double g0 = 0.5 * ((Fs[0] + ldx<CG>(Um) - 2.0) * ddx + (Fs[1] + ldx<CG>(Um + NN)) * ddy +
+                             (Fs[2] + ldx<CG>(Um + 2 * NN)) * ddz);
+    const double g1 = 0.5 * ((Fs[3] + ldx<CG>(Um + 3 * NN)) * ddx +
+                             (Fs[4] + ldx<CG>(Um + 4 * NN) - 2.0) * ddy +
+                             (Fs[5] + ldx<CG>(Um + 5 * NN)) * ddz);
+    const double g2 = 0.5 * ((Fs[6] + ldx<CG>(Um + 6 * NN)) * ddx +
+                             (Fs[7] + ldx<CG>(Um + 7 * NN)) * ddy +
+                             (Fs[8] + ldx<CG>(Um + 8 * NN) - 2.0) * ddz);
+    r[0] += ldx<CG>(ucol + m) - g0;
+    r[1] += ldx<CG>(ucol + (size_t)N + m) - g1;
+    r[2] += ldx<CG>(ucol + 2 * (size_t)N + m) - g2;
     d[0] += 1.0;
     d[1] += 1.0;
     d[2] += 1.0;
@@ -199,12 +209,22 @@ __global__ void __launch_bounds__(256) k3_sweep(Ctx3 c, const double* __restrict
   const double hdt = 0.5 * p.dt;
 #pragma unroll
   for (int comp = 0; comp < 3; ++comp) {
-    const double uo = ucol[(size_t)comp * N + n];
+    const double uo = ldx<CG>(ucol + (size_t)comp * N + n);
     double un = uo;
     if (d[comp] > 0.0) un = uo + p.relax * (r[comp] / d[comp] - uo);
     u[(size_t)comp * N + n] = un;
-    ustar[(size_t)comp * N + n] = (uo + hdt * U[(size_t)comp * N + n]) + (un - uo);
+    ustar[(size_t)comp * N + n] = (uo + hdt * ldx<CG>(U + (size_t)comp * N + n)) + (un - uo);
   }
+}
+
+__global__ void __launch_bounds__(256) k3_sweep(Ctx3 c, const double* __restrict__ U,
+                                                const double* __restrict__ ucol,
+                                                double* __restrict__ u,
+                                                double* __restrict__ ustar, const double* clock,
+                                                double t_host) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= c.N) return;
+  sweep_node3<false>(c, U, ucol, u, ustar, clock, t_host, n);
 }
 
 // Collision + F repair + push streaming (three_d/curved_boundary_warp3d.py
@@ -440,15 +460,15 @@ struct NodeState3 {
 
 // Moments, neighbours, P(F), the F repair and its Piola difference; the U
 // and U_need rows of the node.
-__device__ __forceinline__ void node_prologue3(const Ctx3& c, const Fused3& fz,
-                                               double* __restrict__ U,
-                                               const double* __restrict__ u, int do_repair,
-                                               int store_all, int n, NodeState3& st) {
+template <bool CG = false>
+__device__ __forceinline__ void node_prologue3(const Ctx3& c, const Fused3& fz, double* U,
+                                               const double* u, int do_repair, int store_all,
+                                               int n, NodeState3& st) {
   const int N = c.N;
   const cvlbm3d_problem& p = c.p;
   const Mat& m = c.m;
 #pragma unroll
-  for (int a = 0; a < kC3; ++a) st.S[a] = U[(size_t)a * N + n];
+  for (int a = 0; a < kC3; ++a) st.S[a] = ldx<CG>(U + (size_t)a * N + n);
 #pragma unroll
   for (int q = 0; q < kQ3; ++q) st.nb[q] = p.neighbor[(size_t)q * N + n];
   const double* F = st.S + 3;
@@ -466,26 +486,26 @@ __device__ __forceinline__ void node_prologue3(const Ctx3& c, const Fused3& fz,
 #pragma unroll
     for (int comp = 0; comp < 3; ++comp) {
       const double* uc = u + (size_t)comp * N;
-      const double u0 = uc[n];
+      const double u0 = ldx<CG>(uc + n);
 #pragma unroll
       for (int ax = 0; ax < 3; ++ax) {
         const int pp = st.nb[ax], pm = st.nb[ax + 3];
         const double hh = h[ax];
         double g = 0.0;
         if (pp >= 0 && pm >= 0) {
-          g = (uc[pp] - uc[pm]) / (2.0 * hh);
+          g = (ldx<CG>(uc + pp) - ldx<CG>(uc + pm)) / (2.0 * hh);
         } else if (pp >= 0) {
           const int pp2 = p.neighbor[(size_t)ax * N + pp];
           if (pp2 >= 0)
-            g = (-3.0 * u0 + 4.0 * uc[pp] - uc[pp2]) / (2.0 * hh);
+            g = (-3.0 * u0 + 4.0 * ldx<CG>(uc + pp) - ldx<CG>(uc + pp2)) / (2.0 * hh);
           else
-            g = (uc[pp] - u0) / hh;
+            g = (ldx<CG>(uc + pp) - u0) / hh;
         } else if (pm >= 0) {
           const int pm2 = p.neighbor[(size_t)(ax + 3) * N + pm];
           if (pm2 >= 0)
-            g = (3.0 * u0 - 4.0 * uc[pm] + uc[pm2]) / (2.0 * hh);
+            g = (3.0 * u0 - 4.0 * ldx<CG>(uc + pm) + ldx<CG>(uc + pm2)) / (2.0 * hh);
           else
-            g = (u0 - uc[pm]) / hh;
+            g = (u0 - ldx<CG>(uc + pm)) / hh;
         }
         T[3 * comp + ax] = comp == ax ? 1.0 + g : g;
       }
@@ -590,6 +610,99 @@ __global__ void __launch_bounds__(128, MINB)
   collide_dir3<3>(p, fz, st, f0, f1, N, n);
   collide_dir3<4>(p, fz, st, f0, f1, N, n);
   collide_dir3<5>(p, fz, st, f0, f1, N, n);
+}
+
+// ---------------------------------------------------------------------------
+// Wavefront form of the node work (node_variant 3): the moments, sweep and
+// collide of chunks of one x-plane (the slowest index of the active order)
+// in ONE persistent launch.  Blocks take work items from a ticket counter in
+// the order  moments(w), sweep(w-1), collide(w-3)  for w = 0, 1, ..., so the
+// collide of a plane re-reads f0 a few planes after the moments read it,
+// while it is still in L2: f0 crosses HBM once per step instead of twice.
+// Dependencies (whole planes): the sweep of plane i needs the moments of
+// planes i-1..i+1 (+-x neighbours, same-plane +-y/z); the collide of plane i
+// needs the sweep of planes i-2..i+2 (repair stencil +-2) - which also
+// orders it after every read of its U by a neighbouring sweep.  A block
+// waits only on items with lower tickets, which are held by running blocks,
+// so the order cannot deadlock; every wait is bounded all the same, and a
+// wait that runs out sets the timeout flag and the invalid flag and goes on
+// (a wrong step, never a hung device).  Values other blocks of the launch
+// write (U, collide-time u, swept u) are read through L2 only (ldx<true>).
+// ---------------------------------------------------------------------------
+struct Wave3 {
+  const int4* items;         // [n_items] (stage, plane, first active id, end active id)
+  int n_items, n_planes;
+  const int32_t* chunks;     // [n_planes] items of one stage per plane
+  int32_t* sync;             // [2 + 3*n_planes] ticket, timeout flag, done counters
+};
+
+// A wait gives up after this many polls (about a quarter of a second); the
+// first wait that gives up makes every later wait of the launch return at
+// once, so a broken dependency costs one bound, not one per item.
+constexpr long long kWaveMaxSpins = 1LL << 20;
+
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB)
+    k3_wave(Ctx3 c, Fused3 fz, Wave3 wv, const double* __restrict__ f0, double* __restrict__ f1,
+            double* U, double* ucol, double* u, double* ustar, int* __restrict__ invalid,
+            const double* clock, double t_host, int sweep_due, int do_repair, int store_all) {
+  __shared__ int s_item;
+  int* ticket = wv.sync;
+  int* timeout = wv.sync + 1;
+  int* done = wv.sync + 2;
+  const cvlbm3d_problem& p = c.p;
+  const int N = c.N;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(ticket, 1);
+    __syncthreads();
+    const int it = s_item;
+    __syncthreads();  // s_item is rewritten only after every thread has read it
+    if (it >= wv.n_items) return;
+    const int4 w = wv.items[it];
+    const int stage = w.x, plane = w.y;
+    if (stage > 0 && threadIdx.x == 0) {
+      const int dep = stage - 1;
+      const int r = stage == 1 ? 1 : 2;
+      const int lo = plane - r < 0 ? 0 : plane - r;
+      const int hi = plane + r >= wv.n_planes ? wv.n_planes - 1 : plane + r;
+      const volatile int* gave_up = timeout;
+      for (int pl = lo; pl <= hi && !*gave_up; ++pl) {
+        const int want = wv.chunks[pl];
+        const volatile int* d = done + dep * wv.n_planes + pl;
+        long long spins = 0;
+        while (*d < want && !*gave_up) {
+          if (++spins > kWaveMaxSpins) {
+            atomicExch(timeout, 1);
+            atomicExch(invalid, 1);
+            break;
+          }
+          __nanosleep(64);
+        }
+      }
+      __threadfence();
+    }
+    __syncthreads();
+    const int n = w.z + (int)threadIdx.x;
+    if (n < w.w) {
+      if (stage == 0) {
+        moments_node3(c, f0, U, sweep_due ? ucol : u, ustar, invalid, sweep_due, n);
+      } else if (stage == 1) {
+        if (sweep_due) sweep_node3<true>(c, U, ucol, u, ustar, clock, t_host, n);
+      } else {
+        NodeState3 st;
+        node_prologue3<true>(c, fz, U, u, do_repair, store_all, n, st);
+        collide_dir3<0>(p, fz, st, f0, f1, N, n);
+        collide_dir3<1>(p, fz, st, f0, f1, N, n);
+        collide_dir3<2>(p, fz, st, f0, f1, N, n);
+        collide_dir3<3>(p, fz, st, f0, f1, N, n);
+        collide_dir3<4>(p, fz, st, f0, f1, N, n);
+        collide_dir3<5>(p, fz, st, f0, f1, N, n);
+      }
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) atomicAdd(done + stage * wv.n_planes + plane, 1);
+  }
 }
 
 // -- link kernels -------------------------------------------------------------

@@ -94,6 +94,7 @@ class Problem3D(C.Structure):
         ("need_slot", pI), ("n_need", i32), ("node_variant", i32), ("char_slot", pI),
         ("link_partner", pI), ("link_order", pI), ("link_nodes", pI), ("n_link_nodes", i32),
         ("overlap", i32),
+        ("wave_items", pI), ("n_wave_items", i32), ("n_planes", i32), ("wave_plane_chunks", pI),
     ]
 
 
@@ -101,7 +102,7 @@ class Fields3D(C.Structure):
     _fields_ = [(name, pI) for name in
                 ("f0", "f1", "U", "u", "u_next", "u_star", "link_kind", "link_comp_kind",
                  "link_bv", "link_Fb", "link_Pb", "char_state", "invalid", "clock",
-                 "link_scratch", "U_need")]
+                 "link_scratch", "U_need", "wave_sync")]
 
 
 class StencilInput3D(C.Structure):

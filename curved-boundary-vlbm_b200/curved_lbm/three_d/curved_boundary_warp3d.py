@@ -152,6 +152,35 @@ def _recon_name(rid: int) -> str:
         int(rid), f"unknown({rid})")
 
 
+WAVE_CHUNK = 128  # nodes per work item of the wavefront kernel (its block size)
+
+
+def _wave_tables3(active_i, nx: int):
+    """Work items of the wavefront node kernel (node_variant 3/4), in ticket order.
+
+    The active ids run through the x-planes in order; each plane is cut into
+    chunks of WAVE_CHUNK nodes.  For w = 0, 1, ... the items are the moments
+    chunks of plane w, the sweep chunks of plane w-1 and the collide chunks of
+    plane w-3: every item depends only on items before it (sweep of plane i
+    on the moments of i-1..i+1, collide of plane i on the sweeps of
+    i-2..i+2).  Returns (items [n, 4] int32: stage, plane, first id, end id;
+    chunks per plane [nx] int32).
+    """
+    ai = np.asarray(active_i, dtype=np.int64)
+    start = np.searchsorted(ai, np.arange(nx + 1), side="left")
+    counts = np.diff(start)
+    chunks = ((counts + WAVE_CHUNK - 1) // WAVE_CHUNK).astype(np.int32)
+    rows = []
+    for w in range(nx + 3):
+        for stage, plane in ((0, w), (1, w - 1), (2, w - 3)):
+            if 0 <= plane < nx:
+                a, b = int(start[plane]), int(start[plane + 1])
+                for c0 in range(a, b, WAVE_CHUNK):
+                    rows.append((stage, plane, c0, min(c0 + WAVE_CHUNK, b)))
+    items = np.asarray(rows, dtype=np.int32).reshape(-1, 4)
+    return np.ascontiguousarray(items), chunks
+
+
 def _fused_tables3(tables, link_q, comp_kind, stencil, n_active):
     """Tables of the fused 3-D step, or None when the links do not allow it.
 
@@ -393,6 +422,11 @@ class WarpSparseCurvedBoundaryLBM3D:
         self._n_link_nodes = int(link_nodes.size)
         if link_nodes.size:
             t["link_nodes"] = dev_i(link_nodes)
+        items, chunks = _wave_tables3(tables["active_i"], self.nx)
+        self._n_wave_items = int(items.shape[0])
+        t["wave_items"] = dev_i(items.reshape(-1))
+        t["wave_plane_chunks"] = dev_i(chunks)
+        self._wave_sync = torch.zeros(2 + 3 * self.nx, dtype=i32, device=dev)
         self._tables = t
         self.neighbor = t["neighbor"]
         self.link_p = t["link_p"]
@@ -450,6 +484,7 @@ class WarpSparseCurvedBoundaryLBM3D:
             setattr(p, name, _native.ptr(tensor))
         p.n_need = self._n_need
         p.n_link_nodes = self._n_link_nodes
+        p.n_wave_items, p.n_planes = self._n_wave_items, self.nx
         p.overlap = 0  # measured slower on shell192: the link kernels are throughput-bound
         p.dyn_enabled = _native.ptr(self.dynamic_traction_override_enabled)
         p.dyn_traction = _native.ptr(self.dynamic_traction_override)
@@ -466,7 +501,8 @@ class WarpSparseCurvedBoundaryLBM3D:
                              ("link_Pb", self.link_Pb),
                              ("char_state", self.char_state if has_char else None),
                              ("invalid", self.invalid), ("clock", self._clock),
-                             ("link_scratch", self.link_scratch), ("U_need", self.U_need)):
+                             ("link_scratch", self.link_scratch), ("U_need", self.U_need),
+                             ("wave_sync", self._wave_sync)):
             setattr(fl, name, _native.ptr(tensor))
         return fl
 
@@ -667,7 +703,7 @@ class WarpSparseCurvedBoundaryLBM3D:
 
     # fused collide kernel: 0 one thread per node (128 registers), 1 six warps
     # per 32 nodes (shared memory), 2 one thread per node (168 registers)
-    NODE_VARIANTS = (0, 1, 2)
+    NODE_VARIANTS = (0, 1, 2, 3, 4)
 
     @property
     def overlap_links(self) -> bool:

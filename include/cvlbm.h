@@ -285,7 +285,9 @@ typedef struct cvlbm3d_problem {
   int32_t node_variant;                           /* fused collide kernel: 0 one thread per
                                                      node within 128 registers, 1 six warps
                                                      per 32 nodes (shared memory), 2 one
-                                                     thread per node within 168 registers;
+                                                     thread per node within 168 registers,
+                                                     3 / 4 the wavefront form (wave_*
+                                                     tables) within 128 / 168 registers;
                                                      results are identical */
   const int32_t *char_slot;                       /* [64*n_links] char_idx mapped to
                                                      U_need rows (-1 unused) */
@@ -302,6 +304,15 @@ typedef struct cvlbm3d_problem {
                                                      second stream while the link kernels
                                                      run (measured slower on shell192: the
                                                      link kernels are throughput-bound) */
+  /* wavefront form of the fused node work (node_variant 3): moments, sweep
+     and collide of x-plane chunks in one persistent launch, taken in
+     dependency order from a ticket counter (needs fields->wave_sync) */
+  const int32_t *wave_items;                      /* [4*n_wave_items] stage (0 moments,
+                                                     1 sweep, 2 collide), x-plane, first and
+                                                     end active id; ticket order */
+  int32_t n_wave_items;
+  int32_t n_planes;                               /* x-planes (nx) */
+  const int32_t *wave_plane_chunks;               /* [n_planes] items of one stage per plane */
 } cvlbm3d_problem;
 
 typedef struct cvlbm3d_fields {
@@ -318,6 +329,9 @@ typedef struct cvlbm3d_fields {
                                leaving through each cut link */
   double *U_need;           /* [n_need*12] fused step: post-step U of the nodes cut
                                links read, one 96-byte row per node */
+  int32_t *wave_sync;       /* [2 + 3*n_planes] node_variant 3: ticket, wait-timeout
+                               flag and per-plane completion counters, zeroed by every
+                               step (a timed-out wait also sets invalid) */
 } cvlbm3d_fields;
 
 /* Replaces WarpSparseCurvedBoundaryLBM3D.step
