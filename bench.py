@@ -234,7 +234,7 @@ def batch_bench(args, dev):
     n_conv, n_bad = int((st["status"] == 1).sum()), int((st["status"] == -1).sum())
     # instance numbers (in the seeded table) of the instances that went invalid
     mine = replicas.deal(list(range(n_inst)), rank, world)
-    bad_ids = [int(mine[k]) for k in np.flatnonzero(st["status"] == -1)]
+    bad_ids = [[int(mine[k]), int(st["steps"][k])] for k in np.flatnonzero(st["status"] == -1)]
     (device_ms, wall_s), (updates, n_conv, n_bad) = replicas.reduce_times_and_counts(
         [device_ms, wall_s], [updates, n_conv, n_bad], device=dev)
     n_conv, n_bad = int(n_conv), int(n_bad)
@@ -261,7 +261,7 @@ def batch_bench(args, dev):
                          % (sum_n2 * 24 * 8 * 2 / 1e9)},
         "time_to_residual_s": {"device": device_ms * 1e-3, "wall": wall_s},
         "instances_converged": n_conv, "instances_invalid": n_bad,
-        "invalid_instances_rank0": bad_ids,
+        "invalid_instances_rank0": bad_ids,  # [instance number, step when retired]
         "steps_per_instance_rank0": {"min": int(steps.min()), "max": int(steps.max()),
                                      "mean": float(steps.mean())},
         "clocks": clocks.summary(),
