@@ -15,6 +15,11 @@ import pytest
 
 from oracle import fno_oracle as fo
 
+# native (fp32 weights and accumulation, bf16 GEMM operands) against the FP64
+# oracle rounding at the same bf16 points: the remaining differences are fp32
+# accumulation and the odd element rounding to the other bf16 neighbour
+GRAD_RTOL = 2e-2
+
 
 def _random_params(rng, cin, c, cout, M, L):
     p = {"W0": rng.normal(0, 0.5, (c, cin)), "b0": rng.normal(0, 0.1, c)}
@@ -100,20 +105,24 @@ def test_native_gradients_match_oracle():
     y_n = y.double().cpu().numpy()
     assert np.linalg.norm(y_n - y_o) <= 2e-3 * np.linalg.norm(y_o)
     assert abs(float(part.sum().item()) - loss_o) <= 2e-3 * abs(loss_o)
+    errs = {}
     for k, go in g_o.items():
         gn = net.grads[k].double().cpu().numpy()
-        err = np.linalg.norm(gn - go) / max(np.linalg.norm(go), 1e-30)
-        assert err <= 2e-2, (k, err)
+        errs[k] = float(np.linalg.norm(gn - go) / max(np.linalg.norm(go), 1e-30))
+    print("relative gradient errors:", {k: f"{v:.2e}" for k, v in errs.items()})
+    bad = {k: v for k, v in errs.items() if v > GRAD_RTOL}
+    assert not bad, bad
 
 
 @pytest.mark.gpu
 def test_trained_surrogate_beats_cold_start():
     from curved_lbm import warmstart as ws
 
-    rep = ws.train_and_compare(nxy=24, n_train=12, n_test=2, epochs=60, tol=1e-7, seed=3)
+    rep = ws.train_and_compare(nxy=24, n_train=12, n_test=2, epochs=60, tol=1e-8, seed=3)
     for case in rep["cases"]:
         assert case["warm_ok"], case
         assert case["warm_steps"] < case["cold_steps"], case
-        # both runs reach the converged field to within the tolerance's reach
-        assert case["warm_err"] <= max(10 * case["cold_err"], 1e-4), case
+        # both stop at the same residual; measured against the converged FP64
+        # field their errors are of one size (warm within 1.5x of cold)
+        assert case["warm_err"] <= 1.5 * case["cold_err"] + 1e-9, case
     assert rep["train_loss_last"] < 0.5 * rep["train_loss_first"]
