@@ -120,6 +120,105 @@ __global__ void __launch_bounds__(256) k_collide2(Ctx2 c, const double* __restri
 }
 
 // ---------------------------------------------------------------------------
+// Moment-space collision with ghost damping, two_d/curved_boundary_warp.py
+// :1846-2040 (collision_model "mrt_ghost"): the D2Q4 moments m0 (sum), m1,
+// m2 (fluxes) relax with omega, the ghost m3 = fE - fN + fW - fS with
+// ghost_omega; omega_ghost = omega is the BGK collision.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_collide2_mrt(Ctx2 c, const double* __restrict__ f0,
+                                                      double* __restrict__ fpost,
+                                                      double* __restrict__ U,
+                                                      double* __restrict__ u,
+                                                      double* __restrict__ ustar,
+                                                      int* __restrict__ invalid) {
+  const int N = c.N;
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const cvlbm2d_problem& p = c.p;
+  if (p.active[n] == 0) {
+    for (int k = 0; k < kQ2 * kC2; ++k) fpost[(size_t)k * N + n] = 0.0;
+    for (int a = 0; a < kC2; ++a) U[(size_t)a * N + n] = 0.0;
+    u[n] = 0.0;
+    u[N + n] = 0.0;
+    return;
+  }
+  double f[kQ2 * kC2];
+#pragma unroll
+  for (int k = 0; k < kQ2 * kC2; ++k) f[k] = f0[(size_t)k * N + n];
+  double S[kC2];
+#pragma unroll
+  for (int a = 0; a < kC2; ++a) {
+    double s = 0.0;
+#pragma unroll
+    for (int q = 0; q < kQ2; ++q) s += f[q * kC2 + a];
+    S[a] = s;
+  }
+  const double hdt = 0.5 * p.dt;
+  if (p.source_mode == kSrcConstant) {
+#pragma unroll
+    for (int a = 0; a < kC2; ++a) S[a] += hdt * p.source[a];
+  } else if (p.source_mode == kSrcDamping) {
+    double den = 1.0 + hdt * p.source[0];
+    S[0] = S[0] / den;
+    S[1] = S[1] / den;
+  }
+#pragma unroll
+  for (int a = 0; a < kC2; ++a) U[(size_t)a * N + n] = S[a];
+  double ux = ustar[n] + 0.5 * p.dt * S[0];
+  double uy = ustar[N + n] + 0.5 * p.dt * S[1];
+  u[n] = ux;
+  u[N + n] = uy;
+  ustar[n] = ux + 0.5 * p.dt * S[0];
+  ustar[N + n] = uy + 0.5 * p.dt * S[1];
+  if (S[2] * S[5] - S[3] * S[4] <= c.m.jf) *invalid = 1;
+  const P2 P = piola2(S[2], S[3], S[4], S[5], c.m);
+  const double phx[kC2] = {-P.a, -P.c, -S[0], 0.0, -S[1], 0.0};
+  const double phy[kC2] = {-P.b, -P.d, 0.0, -S[0], 0.0, -S[1]};
+  const double om = p.omega, og = p.ghost_omega;
+#pragma unroll
+  for (int a = 0; a < kC2; ++a) {
+    const double fE = f[a], fN = f[kC2 + a], fW = f[2 * kC2 + a], fS = f[3 * kC2 + a];
+    const double m0 = fE + fN + fW + fS;
+    const double m1 = fE - fW;
+    const double m2 = fN - fS;
+    const double m3 = fE - fN + fW - fS;
+    const double b = source_comp(a, p.source_mode, p.source, S);
+    const double m0p = m0 + om * (S[a] - m0) + p.dt * (2.0 - om) * 0.5 * b;
+    const double m1p = m1 + om * (phx[a] / p.c - m1);
+    const double m2p = m2 + om * (phy[a] / p.c - m2);
+    const double m3p = (1.0 - og) * m3;
+    fpost[(size_t)(0 * kC2 + a) * N + n] = 0.25 * (m0p + m3p + 2.0 * m1p);
+    fpost[(size_t)(1 * kC2 + a) * N + n] = 0.25 * (m0p - m3p + 2.0 * m2p);
+    fpost[(size_t)(2 * kC2 + a) * N + n] = 0.25 * (m0p + m3p - 2.0 * m1p);
+    fpost[(size_t)(3 * kC2 + a) * N + n] = 0.25 * (m0p - m3p - 2.0 * m2p);
+  }
+}
+
+// Kinetic ghost filter, two_d/curved_boundary_warp.py:3101-3124: the ghost
+// moment of each component damped by `strength`, U and the fluxes unchanged.
+__global__ void __launch_bounds__(256) k_ghost_filter2(Ctx2 c, double* __restrict__ f) {
+  const int N = c.N;
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N || c.p.active[n] == 0) return;
+  const double str = c.p.kinetic_filter;
+  if (str <= 0.0) return;
+#pragma unroll
+  for (int a = 0; a < kC2; ++a) {
+    double* fE = f + (size_t)(0 * kC2 + a) * N + n;
+    double* fN = f + (size_t)(1 * kC2 + a) * N + n;
+    double* fW = f + (size_t)(2 * kC2 + a) * N + n;
+    double* fS = f + (size_t)(3 * kC2 + a) * N + n;
+    const double m3 = *fE - *fN + *fW - *fS;
+    const double delta = -str * m3;
+    const double quarter = 0.25 * delta;
+    *fE = *fE + quarter;
+    *fW = *fW + quarter;
+    *fN = *fN - quarter;
+    *fS = *fS - quarter;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Local displacement sweep, two_d/curved_boundary_warp.py:3275-3490, with the
 // link anchors (:3287-3417) gathered per node.
 // ---------------------------------------------------------------------------
@@ -582,7 +681,8 @@ FusedLaunch2 fused_variant(int v) {
 bool fused_ok(const cvlbm2d_problem* p, const cvlbm2d_fields* f) {
   const FusedLaunch2 fl = fused_variant(p->tile_variant);
   return p->tiles && p->need_fields && p->link_partner && f->link_scratch && p->lsq_node &&
-         p->disp_sweeps <= 1 && fl.tile_i == p->tile_i && (!fl.mom || f->fpost);
+         p->disp_sweeps <= 1 && fl.tile_i == p->tile_i && (!fl.mom || f->fpost) &&
+         p->collision_model == 0 && !(p->kinetic_filter > 0.0);
 }
 
 }  // namespace
@@ -691,7 +791,10 @@ extern "C" int cvlbm2d_run(const cvlbm2d_problem* p, cvlbm2d_fields* f, double t
                    p->link_partner, clock_next);
     } else {
       int tk = timer_begin(s);
-      k_collide2<<<nb, 256, 0, s>>>(c, f->f0, f->fpost, f->U, f->u, f->u_star, f->invalid);
+      if (p->collision_model == 1)
+        k_collide2_mrt<<<nb, 256, 0, s>>>(c, f->f0, f->fpost, f->U, f->u, f->u_star, f->invalid);
+      else
+        k_collide2<<<nb, 256, 0, s>>>(c, f->f0, f->fpost, f->U, f->u, f->u_star, f->invalid);
       cv::count_launches(1);
       timer_end(tk, s);
       if (sweep) {
@@ -710,6 +813,10 @@ extern "C" int cvlbm2d_run(const cvlbm2d_problem* p, cvlbm2d_fields* f, double t
       cv::count_launches(1);
       launch_links(c, f->fpost, f->f1, f->U, f->u, clock, t, 0.5 * p->dt, s, 0, nullptr, nullptr,
                    clock_next);
+      if (p->kinetic_filter > 0.0) {
+        k_ghost_filter2<<<nb, 256, 0, s>>>(c, f->f1);
+        cv::count_launches(1);
+      }
     }
     if (graph_mode && p->n_links <= 0) {
       k_tick<<<1, 1, 0, s>>>(f->clock + (k & 1), f->clock + ((k + 1) & 1), p->dt);
@@ -724,6 +831,17 @@ extern "C" int cvlbm2d_run(const cvlbm2d_problem* p, cvlbm2d_fields* f, double t
   if (us_cur != f->u_star)
     cudaMemcpyAsync(f->u_star, us_cur, sizeof(double) * 2 * (size_t)N, cudaMemcpyDeviceToDevice, s);
   return check_launch("cvlbm2d_run");
+}
+
+extern "C" int cvlbm2d_kinetic_filter(const cvlbm2d_problem* p, cvlbm2d_fields* f,
+                                      void* stream) {
+  int rc = check_problem(p, f);
+  if (rc) return rc;
+  Ctx2 c = make_ctx(p);
+  if (!(p->kinetic_filter > 0.0) || c.N == 0) return CVLBM_OK;
+  k_ghost_filter2<<<blocks(c.N, 256), 256, 0, (cudaStream_t)stream>>>(c, f->f0);
+  cv::count_launches(1);
+  return check_launch("cvlbm2d_kinetic_filter");
 }
 
 extern "C" int cvlbm2d_apply_boundary(const cvlbm2d_problem* p, cvlbm2d_fields* f, double t,

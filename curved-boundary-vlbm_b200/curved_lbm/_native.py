@@ -51,6 +51,7 @@ class Problem2D(C.Structure):
         ("tile_variant", i32), ("tile_i", i32), ("n_tiles_inner", i32), ("overlap", i32),
         ("link_rows", pI), ("lsq_node_slot", pI), ("lsq_wb_slot", pI), ("lsq_wt_slot", pI),
         ("lsq_wx_slot", pI), ("lsq_wy_slot", pI),
+        ("collision_model", i32), ("ghost_omega", f64), ("kinetic_filter", f64),
     ]
 
 
@@ -117,6 +118,7 @@ EXPORTED = (
     "cvlbm2d_apply_boundary",
     "cvlbm2d_refresh",
     "cvlbm2d_stress",
+    "cvlbm2d_kinetic_filter",
     "cvlbm3d_run",
     "cvlbm3d_apply_boundary",
     "cvlbm3d_refresh",
@@ -178,6 +180,7 @@ def load(require_cuda: bool = True):
         "cvlbm2d_apply_boundary": (i32, [P2, F2, f64, i32, pI]),
         "cvlbm2d_refresh": (i32, [P2, F2, pI]),
         "cvlbm2d_stress": (i32, [P2, F2, pI]),
+        "cvlbm2d_kinetic_filter": (i32, [P2, F2, pI]),
         "cvlbm3d_run": (i32, [P3, F3, f64, i64, i32, i32, pI]),
         "cvlbm3d_apply_boundary": (i32, [P3, F3, f64, i32, pI]),
         "cvlbm3d_refresh": (i32, [P3, F3, pI]),

@@ -19,7 +19,8 @@ import numpy as np
 # solver attributes that decide what a step computes (those a class lacks are skipped)
 _SETTINGS = (
     "nx", "ny", "nz", "n_active", "dx", "dy", "dz", "dt", "lattice_speed", "collision_omega",
-    "collision_model", "boundary_reconstruction_name", "normal_jacobian_name",
+    "collision_model", "ghost_omega", "kinetic_filter_strength",
+    "boundary_reconstruction_name", "normal_jacobian_name",
     "neumann_solver_name", "jacobian_floor", "source_mode",
     "local_displacement_interval", "local_displacement_sweeps", "local_displacement_relax",
     "local_displacement_boundary_weight", "local_displacement_boundary_id",

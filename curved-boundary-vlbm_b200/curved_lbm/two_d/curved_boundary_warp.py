@@ -7,10 +7,11 @@ on PyTorch CUDA buffers instead of Warp kernels.  Reference line numbers are
 cited per method.
 
 Supported boundary reconstructions: ``bfl``, ``lsq_bfl``/``normal_probe_bfl``,
-``compat_bfl``, ``local_char2``, ``local_f`` and ``local_f_bfl``.  The other
-diagnostic closures of the reference (qbfl, regularized_*, *_nee, poly_ibb,
-lowq_reg_bfl), the ``mrt_ghost`` collision and the kinetic ghost filter are not
-implemented and raise ``NotImplementedError`` at construction.
+``compat_bfl``, ``local_char2``, ``local_f`` and ``local_f_bfl``, with the BGK
+or the ``mrt_ghost`` collision and the optional kinetic ghost filter.  The
+other diagnostic closures of the reference (qbfl, regularized_*, *_nee,
+poly_ibb, lowq_reg_bfl) are not implemented and raise ``NotImplementedError``
+at construction.
 """
 
 from __future__ import annotations
@@ -411,10 +412,6 @@ class WarpCurvedBoundaryLBM2D:
                 "local_displacement_sweeps must be in [1,8] to keep a bounded local dependency radius")
         if self.local_displacement_boundary_weight < 0.0:
             raise ValueError("local_displacement_boundary_weight must be non-negative")
-        if self.collision_model != "bgk":
-            raise NotImplementedError("collision_model='mrt_ghost' is not implemented")
-        if self.kinetic_filter_strength > 0.0:
-            raise NotImplementedError("the kinetic ghost filter is not implemented")
         if self.boundary_reconstruction not in SUPPORTED_RECONSTRUCTIONS:
             raise NotImplementedError(
                 f"boundary_reconstruction={self.boundary_reconstruction_name!r} is not implemented")
@@ -629,6 +626,9 @@ class WarpCurvedBoundaryLBM2D:
         p.relax = self.local_displacement_relax
         p.weight = self.local_displacement_boundary_weight
         p.blend = self.local_compatibility_blend
+        p.collision_model = 1 if self.collision_model == "mrt_ghost" else 0
+        p.ghost_omega = self.ghost_omega
+        p.kinetic_filter = self.kinetic_filter_strength
         for name, tensor in t.items():
             setattr(p, name, _native.ptr(tensor))
         p.traction_x = _native.ptr(self.link_traction_x)
@@ -710,6 +710,10 @@ class WarpCurvedBoundaryLBM2D:
         self.refresh_current()
         if apply_initial_boundaries:
             self.apply_boundary_reconstruction(float(initial_boundary_time), in_place=True)
+            if self.kinetic_filter_strength > 0.0:  # reference :3947-3952
+                _native.check(self._lib.cvlbm2d_kinetic_filter(self._problem, self._fields(),
+                                                               self._stream()),
+                              "cvlbm2d_kinetic_filter")
             self.refresh_current()
 
     # -- boundary ----------------------------------------------------------

@@ -131,6 +131,12 @@ typedef struct cvlbm2d_problem {
   const cvlbm2d_link_row *link_rows;          /* [n_links] */
   const int32_t *lsq_node_slot;               /* [n_links*24] */
   const double *lsq_wb_slot, *lsq_wt_slot, *lsq_wx_slot, *lsq_wy_slot;
+  /* collision options (two_d/curved_boundary_warp.py:3629-3631); either one
+     selects the per-phase kernels */
+  int32_t collision_model;                    /* 0 bgk, 1 mrt_ghost (:1846-2040) */
+  double ghost_omega;                         /* relaxation of the D2Q4 ghost moment */
+  double kinetic_filter;                      /* ghost filter strength in [0, 1]
+                                                 (:3101-3124), applied after each step */
 } cvlbm2d_problem;
 
 /* Tile rows (i extent, tiles are 32 nodes wide in j) of fused-kernel variant
@@ -173,6 +179,12 @@ int cvlbm2d_run(const cvlbm2d_problem *p, cvlbm2d_fields *f, double time0, int64
 #define CVLBM2D_STATIC_SCRATCH_MAX_LINKS 16384
 int cvlbm2d_run_static_scratch(const cvlbm2d_problem *p, cvlbm2d_fields *f, double time0,
                                int64_t step0, int32_t nsteps, void *stream);
+
+/* Kinetic ghost filter (problem->kinetic_filter) applied in place to
+ * fields->f0, as initialize_from_numpy does after its in-place boundary pass
+ * (two_d/curved_boundary_warp.py:3947-3952; kernel :3101-3124).  A run
+ * applies it after every step by itself. */
+int cvlbm2d_kinetic_filter(const cvlbm2d_problem *p, cvlbm2d_fields *f, void *stream);
 
 /* Cut-link reconstruction at time t, fpost -> f1, or in place on f0 through a
  * frozen copy in fpost.  Replaces apply_boundary_reconstruction

@@ -536,6 +536,93 @@ static void collide_masked(const cvlbm2d_problem *p, const mat_t *m, cvlbm2d_fie
     }
 }
 
+/* C2:1846-2040 _collide_masked_mrt_ghost_kernel: moment-space collision,
+ * flux moments relaxed with omega, the D2Q4 ghost moment with ghost_omega */
+static void collide_masked_mrt(const cvlbm2d_problem *p, const mat_t *m, cvlbm2d_fields *f,
+                               size_t n, int *invalid) {
+  size_t N = (size_t)p->nx * p->ny;
+  if (p->active[n] == 0) {
+    for (int k = 0; k < 24; ++k) f->fpost[k * N + n] = 0.0;
+    for (int a = 0; a < 6; ++a) f->U[a * N + n] = 0.0;
+    f->u[n] = 0.0;
+    f->u[N + n] = 0.0;
+    return;
+  }
+  double S[6] = {0, 0, 0, 0, 0, 0};
+  for (int q = 0; q < 4; ++q)
+    for (int a = 0; a < 6; ++a) S[a] += f->f0[(q * 6 + a) * N + n];
+  double hdt = 0.5 * p->dt;
+  if (p->source_mode == 1) {
+    for (int a = 0; a < 6; ++a) S[a] += hdt * p->source[a];
+  } else if (p->source_mode == 2) {
+    double den = 1.0 + hdt * p->source[0];
+    S[0] = S[0] / den;
+    S[1] = S[1] / den;
+  }
+  double b[6];
+  for (int a = 0; a < 6; ++a) b[a] = source_comp(a, p->source_mode, p->source, S[0], S[1]);
+  for (int a = 0; a < 6; ++a) f->U[a * N + n] = S[a];
+  double ux = f->u_star[n] + 0.5 * p->dt * S[0], uy = f->u_star[N + n] + 0.5 * p->dt * S[1];
+  f->u[n] = ux;
+  f->u[N + n] = uy;
+  f->u_star[n] = ux + 0.5 * p->dt * S[0];
+  f->u_star[N + n] = uy + 0.5 * p->dt * S[1];
+  double J = S[2] * S[5] - S[3] * S[4];
+  if (J <= m->jf) *invalid = 1;
+  double Js = clamp_j(J, m->jf), P[4];
+  piola_vec(S[2], S[3], S[4], S[5], m, P);
+  if (f->P) {
+    for (int k = 0; k < 4; ++k) f->P[k * N + n] = P[k];
+    f->sigma[n] = (P[0] * S[2] + P[1] * S[3]) / Js;
+    f->sigma[N + n] = (P[0] * S[4] + P[1] * S[5]) / Js;
+    f->sigma[2 * N + n] = (P[2] * S[2] + P[3] * S[3]) / Js;
+    f->sigma[3 * N + n] = (P[2] * S[4] + P[3] * S[5]) / Js;
+  }
+  const double phx[6] = {-P[0], -P[2], -S[0], 0.0, -S[1], 0.0};
+  const double phy[6] = {-P[1], -P[3], 0.0, -S[0], 0.0, -S[1]};
+  const double om = p->omega, og = p->ghost_omega;
+  for (int a = 0; a < 6; ++a) {
+    double fE = f->f0[(0 * 6 + a) * N + n], fN = f->f0[(1 * 6 + a) * N + n];
+    double fW = f->f0[(2 * 6 + a) * N + n], fS = f->f0[(3 * 6 + a) * N + n];
+    double m0 = fE + fN + fW + fS;
+    double m1 = fE - fW;
+    double m2 = fN - fS;
+    double m3 = fE - fN + fW - fS;
+    double m0p = m0 + om * (S[a] - m0) + p->dt * (2.0 - om) * 0.5 * b[a];
+    double m1p = m1 + om * (phx[a] / p->c - m1);
+    double m2p = m2 + om * (phy[a] / p->c - m2);
+    double m3p = (1.0 - og) * m3;
+    f->fpost[(0 * 6 + a) * N + n] = 0.25 * (m0p + m3p + 2.0 * m1p);
+    f->fpost[(1 * 6 + a) * N + n] = 0.25 * (m0p - m3p + 2.0 * m2p);
+    f->fpost[(2 * 6 + a) * N + n] = 0.25 * (m0p + m3p - 2.0 * m1p);
+    f->fpost[(3 * 6 + a) * N + n] = 0.25 * (m0p - m3p - 2.0 * m2p);
+  }
+}
+
+/* C2:3101-3124 _kinetic_ghost_filter_kernel: damp the ghost moment in place */
+static void kinetic_filter(const cvlbm2d_problem *p, double *fld, size_t n) {
+  size_t N = (size_t)p->nx * p->ny;
+  double str = p->kinetic_filter;
+  if (p->active[n] == 0 || str <= 0.0) return;
+  for (int a = 0; a < 6; ++a) {
+    size_t iE = (0 * 6 + a) * N + n, iN = (1 * 6 + a) * N + n;
+    size_t iW = (2 * 6 + a) * N + n, iS = (3 * 6 + a) * N + n;
+    double m3 = fld[iE] - fld[iN] + fld[iW] - fld[iS];
+    double delta = -str * m3;
+    double quarter = 0.25 * delta;
+    fld[iE] = fld[iE] + quarter;
+    fld[iW] = fld[iW] + quarter;
+    fld[iN] = fld[iN] - quarter;
+    fld[iS] = fld[iS] - quarter;
+  }
+}
+
+int oracle2d_kinetic_filter(const cvlbm2d_problem *p, cvlbm2d_fields *f) {
+  long N = (long)p->nx * p->ny;
+  for (long n = 0; n < N; ++n) kinetic_filter(p, f->f0, (size_t)n);
+  return 0;
+}
+
 /* C2:3287-3417 _local_displacement_bc_kernel, serial in link order */
 static void displacement_bc(const cvlbm2d_problem *p, const cvlbm2d_fields *f, oracle2d_scratch *s,
                             double time) {
@@ -920,8 +1007,13 @@ int oracle2d_step(const cvlbm2d_problem *p, cvlbm2d_fields *f, oracle2d_scratch 
 #else
   (void)threads;
 #endif
+  if (p->collision_model == 1) {
 #pragma omp parallel for schedule(static) reduction(| : invalid)
-  for (long n = 0; n < N; ++n) collide_masked(p, &m, f, (size_t)n, &invalid);
+    for (long n = 0; n < N; ++n) collide_masked_mrt(p, &m, f, (size_t)n, &invalid);
+  } else {
+#pragma omp parallel for schedule(static) reduction(| : invalid)
+    for (long n = 0; n < N; ++n) collide_masked(p, &m, f, (size_t)n, &invalid);
+  }
   if (due(p->disp_interval, step)) {
     for (int sw = 0; sw < p->disp_sweeps; ++sw) {
       memset(s->bc_diag, 0, sizeof(double) * N);
@@ -944,6 +1036,10 @@ int oracle2d_step(const cvlbm2d_problem *p, cvlbm2d_fields *f, oracle2d_scratch 
 #pragma omp parallel for schedule(static)
   for (int ell = 0; ell < p->n_links; ++ell)
     apply_links(p, &m, f->fpost, f->f1, f->U, f->u, ell, tmid);
+  if (p->kinetic_filter > 0.0) {
+#pragma omp parallel for schedule(static)
+    for (long n = 0; n < N; ++n) kinetic_filter(p, f->f1, (size_t)n);
+  }
   double *tmp = f->f0;
   f->f0 = f->f1;
   f->f1 = tmp;

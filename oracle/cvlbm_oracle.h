@@ -44,6 +44,8 @@ int oracle2d_step(const cvlbm2d_problem *p, cvlbm2d_fields *f, oracle2d_scratch 
                   int64_t step, int threads);
 int oracle2d_apply_boundary(const cvlbm2d_problem *p, cvlbm2d_fields *f, double t, int in_place);
 int oracle2d_refresh(const cvlbm2d_problem *p, cvlbm2d_fields *f);
+/* C2:3101-3124 kinetic ghost filter on fields->f0 (initialisation) */
+int oracle2d_kinetic_filter(const cvlbm2d_problem *p, cvlbm2d_fields *f);
 
 int oracle3d_step(const cvlbm3d_problem *p, cvlbm3d_fields *f, oracle3d_scratch *s, double time,
                   int64_t step, int threads);

@@ -54,6 +54,7 @@ class Oracle2D:
                  local_displacement_interval=0, local_displacement_sweeps=1,
                  local_displacement_relax=0.85, local_displacement_boundary_weight=20.0,
                  local_displacement_boundary_id=2, normal_jacobian=None, neumann_solver=None,
+                 collision_model="bgk", ghost_omega=None, kinetic_filter_strength=0.0,
                  threads=1, **_unused):
         from curved_lbm import _native
         from curved_lbm.two_d import curved_boundary_warp as c2
@@ -103,6 +104,9 @@ class Oracle2D:
         p.relax = float(local_displacement_relax)
         p.weight = float(local_displacement_boundary_weight)
         p.blend = float(local_compatibility_blend)
+        p.collision_model = 1 if collision_model == "mrt_ghost" else 0
+        p.ghost_omega = float(collision_omega if ghost_omega is None else ghost_omega)
+        p.kinetic_filter = float(kinetic_filter_strength)
         i32, f64 = np.int32, np.float64
         p.active = _ptr(keep(g.active.reshape(-1), i32))
         for name in ("link_i", "link_j", "link_q"):
@@ -171,6 +175,8 @@ class Oracle2D:
         if apply_initial_boundaries:
             self.lib.oracle2d_apply_boundary(C.byref(self.p), C.byref(self._fields()),
                                              C.c_double(initial_boundary_time), 1)
+            if self.p.kinetic_filter > 0.0:
+                self.lib.oracle2d_kinetic_filter(C.byref(self.p), C.byref(self._fields()))
             self.refresh()
 
     def refresh(self):

@@ -353,6 +353,17 @@ for _m, _extra in MATERIALS_2D.items():
     _c["init"] = dict(kind="identity_perturbed", init_order=2)
     _c["steps"] = 8
     CASES_2D[f"g2_mat_{_m}"] = _c
+# the MRT ghost collision and the kinetic ghost filter (reference options)
+for _name, _opts in (("g2_mrt_ghost", dict(collision_model="mrt_ghost", ghost_omega=1.2)),
+                     ("g2_kinetic_filter", dict(kinetic_filter_strength=0.3)),
+                     ("g2_mrt_filter", dict(collision_model="mrt_ghost", ghost_omega=0.9,
+                                            kinetic_filter_strength=0.15))):
+    _c = json.loads(json.dumps(CASES_2D["g2_traction_localf"]))
+    _c["geometry"]["nx"] = _c["geometry"]["ny"] = 20
+    _c["init"] = dict(kind="identity_perturbed", init_order=2)
+    _c["solver"].update(_opts)
+    _c["steps"] = 8
+    CASES_2D[_name] = _c
 for _m, _extra in MATERIALS_3D.items():
     _c = json.loads(json.dumps(CASES_3D["g3_shell_localf"]))
     _c["geometry"]["nx"] = _c["geometry"]["ny"] = _c["geometry"]["nz"] = 14

@@ -18,6 +18,7 @@ GOLD3 = ["g3_shell_localf", "g3_shell_bfl_fd", "g3_shell_compat"]
 # one case per material law other than neo-Hooke (tests/golden/make_golden.py)
 GOLD2 += [f"g2_mat_{m}" for m in ("svk", "log_neo_hooke", "mooney_rivlin", "yeoh", "gent",
                                    "sugiyama_svk")]
+GOLD2 += ["g2_mrt_ghost", "g2_kinetic_filter", "g2_mrt_filter"]
 GOLD3 += [f"g3_mat_{m}" for m in ("svk", "log_neo_hooke", "mooney_rivlin", "yeoh", "gent",
                                    "sph_neo_hooke")]
 
