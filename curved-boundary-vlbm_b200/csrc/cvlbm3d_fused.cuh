@@ -837,6 +837,8 @@ __global__ void __launch_bounds__(128)
     for (int k = 0; k < 9; ++k) Fb[k] = F[k];
     if (ck[0] == kNeumann && ck[1] == kNeumann && ck[2] == kNeumann)
       solve_Fb3(F, nx, ny, nz, T, m, p.normal_solver, Fb);
+    else if (ck[0] == kNeumann || ck[1] == kNeumann || ck[2] == kNeumann)
+      solve_Fb3_mixed(F, nx, ny, nz, T, ck, m, p.normal_solver, Fb);
     const M3 P = piola3(Fb, m);
     for (int k = 0; k < 9; ++k) Pb[k] = P.v[k];
   }

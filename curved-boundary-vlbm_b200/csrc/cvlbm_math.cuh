@@ -885,6 +885,150 @@ CV_DEV void solve_Fb3(const double* Fg, double nx, double ny, double nz, const d
   make_F_h(h, fr, g1, g2, Fout);
 }
 
+// Closed-form minimiser over the Neumann rows only, quadratic-volumetric
+// neo-Hooke, mixed rows (three_d/curved_boundary_warp3d.py:1249-1329, branch
+// with a Dirichlet row): J = d + a_N.h_N with d from the fixed rows.
+CV_DEV bool energy_Fb3_mixed(const double* F, const double* n, const double* T, const int* ck,
+                             double lam, double mu, double jf, double* Fb) {
+  double cof[9] = {F[4] * F[8] - F[5] * F[7], F[5] * F[6] - F[3] * F[8], F[3] * F[7] - F[4] * F[6],
+                   F[2] * F[7] - F[1] * F[8], F[0] * F[8] - F[2] * F[6], F[1] * F[6] - F[0] * F[7],
+                   F[1] * F[5] - F[2] * F[4], F[2] * F[3] - F[0] * F[5], F[0] * F[4] - F[1] * F[3]};
+  double a[3], ho[3], an[3] = {0.0, 0.0, 0.0}, tn[3] = {0.0, 0.0, 0.0}, fixed[3];
+  for (int i = 0; i < 3; ++i) {
+    a[i] = cof[3 * i] * n[0] + cof[3 * i + 1] * n[1] + cof[3 * i + 2] * n[2];
+    ho[i] = F[3 * i] * n[0] + F[3 * i + 1] * n[1] + F[3 * i + 2] * n[2];
+    fixed[i] = ho[i];
+    if (ck[i] == kNeumann) {
+      an[i] = a[i];
+      tn[i] = T[i];
+      fixed[i] = 0.0;
+    }
+  }
+  const double a2 = an[0] * an[0] + an[1] * an[1] + an[2] * an[2];
+  const double d = a[0] * fixed[0] + a[1] * fixed[1] + a[2] * fixed[2];
+  double h[3];
+  if (a2 > 1.0e-28) {
+    const double aa = mu + 0.5 * lam * a2;
+    const double bb = (mu + 0.5 * lam) * a2;
+    const double cc = mu * d + (an[0] * tn[0] + an[1] * tn[1] + an[2] * tn[2]);
+    const double disc = sqrt(cc * cc + 4.0 * aa * bb);
+    double J = (cc + disc) / (2.0 * aa);
+    if (cc < 0.0) J = 2.0 * bb / (disc - cc);
+    if (!(J > jf)) return false;
+    const double area = sqrt(a2);
+    const double e[3] = {an[0] / area, an[1] / area, an[2] / area};
+    const double te = tn[0] * e[0] + tn[1] * e[1] + tn[2] * e[2];
+    for (int i = 0; i < 3; ++i) h[i] = fixed[i] + (tn[i] - te * e[i]) / mu + ((J - d) / area) * e[i];
+  } else if (a2 == 0.0 && d > jf) {
+    for (int i = 0; i < 3; ++i) h[i] = fixed[i] + tn[i] / mu;
+  } else {
+    return false;
+  }
+  for (int i = 0; i < 3; ++i) {
+    const double dh = h[i] - ho[i];
+    for (int j = 0; j < 3; ++j) Fb[3 * i + j] = F[3 * i + j] + dh * n[j];
+  }
+  return true;
+}
+
+// Normal solve of the Neumann rows only, three_d/curved_boundary_warp3d.py
+// :1518-1737 (_solve_Fb_componentwise_normal): a Dirichlet row keeps its
+// extrapolated normal derivative (its residual and Jacobian row are replaced
+// by the identity), so its traction is not prescribed but retained in
+// P(F_b) n as the boundary reaction.
+CV_DEV void solve_Fb3_mixed(const double* Fg, double nx, double ny, double nz, const double* T,
+                            const int* ck, const Mat& m, int solver, double* Fout) {
+  Frame3 fr = frame3(nx, ny, nz);
+  if (solver == kSolverEnergy && m.model == kMatNeoHooke) {
+    double Fb[9];
+    if (energy_Fb3_mixed(Fg, fr.n, T, ck, m.lam, m.mu, m.jf, Fb) && det3v(Fb) > m.jf) {
+      for (int k = 0; k < 9; ++k) Fout[k] = Fb[k];
+      return;
+    }
+  }
+  double h[3], g1[3], g2[3];
+  for (int i = 0; i < 3; ++i) {
+    h[i] = Fg[3 * i] * fr.n[0] + Fg[3 * i + 1] * fr.n[1] + Fg[3 * i + 2] * fr.n[2];
+    g1[i] = Fg[3 * i] * fr.t1[0] + Fg[3 * i + 1] * fr.t1[1] + Fg[3 * i + 2] * fr.t1[2];
+    g2[i] = Fg[3 * i] * fr.t2[0] + Fg[3 * i + 1] * fr.t2[1] + Fg[3 * i + 2] * fr.t2[2];
+  }
+  const double eps = 1.0e-6;
+  for (int it = 0; it < 16; ++it) {
+    double r[3];
+    residual3(h, fr, g1, g2, T, m, r);
+    double rm[3];
+    for (int i = 0; i < 3; ++i) rm[i] = ck[i] == kNeumann ? r[i] : 0.0;
+    const double rn = sqrt(rm[0] * rm[0] + rm[1] * rm[1] + rm[2] * rm[2]);
+    if (rn < 1.0e-10) break;
+    double A[9];
+    if (solver != kSolverFD && m.model == kMatNeoHooke) {
+      double F[9];
+      make_F_h(h, fr, g1, g2, F);
+      double J = det3v(F);
+      if (J < m.jf) J = m.jf;
+      double H[9];
+      H[0] = (F[4] * F[8] - F[5] * F[7]) / J;
+      H[1] = (F[5] * F[6] - F[3] * F[8]) / J;
+      H[2] = (F[3] * F[7] - F[4] * F[6]) / J;
+      H[3] = (F[2] * F[7] - F[1] * F[8]) / J;
+      H[4] = (F[0] * F[8] - F[2] * F[6]) / J;
+      H[5] = (F[1] * F[6] - F[0] * F[7]) / J;
+      H[6] = (F[1] * F[5] - F[2] * F[4]) / J;
+      H[7] = (F[2] * F[3] - F[0] * F[5]) / J;
+      H[8] = (F[0] * F[4] - F[1] * F[3]) / J;
+      const double beta = 0.5 * m.lam * (J * J - 1.0) - m.mu;
+      const double coeff = m.lam * J * J - beta;
+      const double n2 = fr.n[0] * fr.n[0] + fr.n[1] * fr.n[1] + fr.n[2] * fr.n[2];
+      double v[3];
+      for (int i = 0; i < 3; ++i)
+        v[i] = H[3 * i] * fr.n[0] + H[3 * i + 1] * fr.n[1] + H[3 * i + 2] * fr.n[2];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+          A[3 * i + j] = (i == j) ? m.mu * n2 + coeff * v[i] * v[j] : coeff * v[i] * v[j];
+    } else {
+      double rp[3][3];
+      for (int k = 0; k < 3; ++k) {
+        double hp[3] = {h[0], h[1], h[2]};
+        hp[k] = hp[k] + eps;
+        residual3(hp, fr, g1, g2, T, m, rp[k]);
+      }
+      for (int i = 0; i < 3; ++i)
+        for (int k = 0; k < 3; ++k) A[3 * i + k] = (rp[k][i] - r[i]) / eps;
+    }
+    for (int i = 0; i < 3; ++i)
+      if (ck[i] != kNeumann)
+        for (int k = 0; k < 3; ++k) A[3 * i + k] = i == k ? 1.0 : 0.0;
+    const double a = A[0], b = A[1], c = A[2], d = A[3], e = A[4], f = A[5], g = A[6],
+                 hh = A[7], ii = A[8];
+    const double det = a * (e * ii - f * hh) - b * (d * ii - f * g) + c * (d * hh - e * g);
+    if (fabs(det) < 1.0e-14) break;
+    const double i00 = (e * ii - f * hh) / det, i01 = (c * hh - b * ii) / det,
+                 i02 = (b * f - c * e) / det;
+    const double i10 = (f * g - d * ii) / det, i11 = (a * ii - c * g) / det,
+                 i12 = (c * d - a * f) / det;
+    const double i20 = (d * hh - e * g) / det, i21 = (b * g - a * hh) / det,
+                 i22 = (a * e - b * d) / det;
+    const double dl[3] = {-(i00 * rm[0] + i01 * rm[1] + i02 * rm[2]),
+                          -(i10 * rm[0] + i11 * rm[1] + i12 * rm[2]),
+                          -(i20 * rm[0] + i21 * rm[1] + i22 * rm[2])};
+    double step = 1.0;
+    for (int ls = 0; ls < 12; ++ls) {
+      double cand[3];
+      for (int i = 0; i < 3; ++i) cand[i] = ck[i] == kNeumann ? h[i] + step * dl[i] : h[i];
+      double F[9];
+      make_F_h(cand, fr, g1, g2, F);
+      if (det3v(F) > m.jf) {
+        h[0] = cand[0];
+        h[1] = cand[1];
+        h[2] = cand[2];
+        break;
+      }
+      step = 0.5 * step;
+    }
+  }
+  make_F_h(h, fr, g1, g2, Fout);
+}
+
 // Flux directional derivative for the 12-component state,
 // three_d/curved_boundary_warp3d.py:2728-2752 (_state_flux_jvp3).
 CV_DEV void jvp3(int axis, const double* U, const double* W, const Mat& m, double* out) {

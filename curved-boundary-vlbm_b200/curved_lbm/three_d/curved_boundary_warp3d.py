@@ -4,10 +4,10 @@ Same module path, names, constructor arguments, methods and errors as the
 reference's ``curved_lbm.three_d.curved_boundary_warp3d`` (curved_lbm 1.0.0),
 whose public class ``WarpCurvedBoundaryLBM3D`` is the sparse active-node
 solver (:3852-4805).  The time step runs in hand-written sm_100a kernels
-(``libcvlbm.so``) on PyTorch CUDA buffers.  Not implemented (raise
-``NotImplementedError``): the dense 3-D class and the component-wise mixed
-Neumann solve (links whose three displacement rows mix Dirichlet and
-Neumann kinds).
+(``libcvlbm.so``) on PyTorch CUDA buffers.  Links whose three displacement
+rows mix Dirichlet and Neumann kinds take the reference's component-wise
+normal solve.  ``WarpCurvedBoundaryLBM3D`` is this sparse class (the
+reference's dense 3-D class is not provided).
 """
 
 from __future__ import annotations
@@ -354,11 +354,6 @@ class WarpSparseCurvedBoundaryLBM3D:
         clipped = np.clip(link_ids, 0, MAX_BOUNDARY_IDS - 1)
         ck = self.component_kind_by_id[:, clipped]
         self._has_neumann_cut_links = bool(link_ids.size and np.any(ck == BC_NEUMANN))
-        mixed = np.any(ck == BC_NEUMANN, axis=0) & ~np.all(ck == BC_NEUMANN, axis=0)
-        if np.any(mixed):
-            raise NotImplementedError(
-                "cut links mixing Dirichlet and Neumann displacement rows (component-wise "
-                "normal solve) are not implemented")
         self.characteristic_stencil = None
         if self.boundary_reconstruction == BOUNDARY_RECON_LOCAL_F and self._has_neumann_cut_links:
             if characteristic_stencil is not None:

@@ -1343,6 +1343,133 @@ static void solve_Fb_arbitrary_normal(const double *Fg, double nx, double ny, do
   make_F_from_h(h, n, t1, t2, g1, g2, out);
 }
 
+/* C3:1249-1329 _energy_Fb_neo_hooke_3d, branch with Dirichlet rows */
+static int energy_Fb3_mixed(const double *F, const double *n, const double *T, const int *ck,
+                            double lam, double mu, double jf, double *Fb) {
+  double cof[9] = {F[4] * F[8] - F[5] * F[7], F[5] * F[6] - F[3] * F[8], F[3] * F[7] - F[4] * F[6],
+                   F[2] * F[7] - F[1] * F[8], F[0] * F[8] - F[2] * F[6], F[1] * F[6] - F[0] * F[7],
+                   F[1] * F[5] - F[2] * F[4], F[2] * F[3] - F[0] * F[5], F[0] * F[4] - F[1] * F[3]};
+  double a[3], ho[3], an[3] = {0, 0, 0}, tn[3] = {0, 0, 0}, fx[3], h[3];
+  for (int i = 0; i < 3; ++i) {
+    a[i] = cof[3 * i] * n[0] + cof[3 * i + 1] * n[1] + cof[3 * i + 2] * n[2];
+    ho[i] = F[3 * i] * n[0] + F[3 * i + 1] * n[1] + F[3 * i + 2] * n[2];
+    fx[i] = ho[i];
+    if (ck[i] == NEU_) {
+      an[i] = a[i];
+      tn[i] = T[i];
+      fx[i] = 0.0;
+    }
+  }
+  double a2 = an[0] * an[0] + an[1] * an[1] + an[2] * an[2];
+  double d = a[0] * fx[0] + a[1] * fx[1] + a[2] * fx[2];
+  if (a2 > 1.0e-28) {
+    double aa = mu + 0.5 * lam * a2, bb = (mu + 0.5 * lam) * a2;
+    double cc = mu * d + (an[0] * tn[0] + an[1] * tn[1] + an[2] * tn[2]);
+    double disc = sqrt(cc * cc + 4.0 * aa * bb);
+    double J = (cc + disc) / (2.0 * aa);
+    if (cc < 0.0) J = 2.0 * bb / (disc - cc);
+    if (!(J > jf)) return 0;
+    double area = sqrt(a2), e[3] = {an[0] / area, an[1] / area, an[2] / area};
+    double te = tn[0] * e[0] + tn[1] * e[1] + tn[2] * e[2];
+    for (int i = 0; i < 3; ++i) h[i] = fx[i] + (tn[i] - te * e[i]) / mu + ((J - d) / area) * e[i];
+  } else if (a2 == 0.0 && d > jf) {
+    for (int i = 0; i < 3; ++i) h[i] = fx[i] + tn[i] / mu;
+  } else {
+    return 0;
+  }
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) Fb[3 * i + j] = F[3 * i + j] + (h[i] - ho[i]) * n[j];
+  return 1;
+}
+
+/* C3:1518-1737 _solve_Fb_componentwise_normal: Newton on the Neumann rows only */
+static void solve_Fb_componentwise_normal(const double *Fg, double nx, double ny, double nz,
+                                          const double *T, const int *ck, const mat_t *m, int nj,
+                                          double *out) {
+  double n[3] = {nx, ny, nz};
+  normalize3(n);
+  if (nj == 2 && m->model == 1) {
+    double Fb[9];
+    if (energy_Fb3_mixed(Fg, n, T, ck, m->lam, m->mu, m->jf, Fb) && det3(Fb) > m->jf) {
+      memcpy(out, Fb, sizeof Fb);
+      return;
+    }
+  }
+  double ref[3] = {1.0, 0.0, 0.0};
+  if (fabs(n[0]) >= 0.75) {
+    ref[0] = 0.0;
+    ref[1] = 1.0;
+  }
+  double t1[3], t2[3];
+  cross3(n, ref, t1);
+  normalize3(t1);
+  cross3(n, t1, t2);
+  double h[3], g1[3], g2[3];
+  for (int i = 0; i < 3; ++i) {
+    h[i] = Fg[3 * i] * n[0] + Fg[3 * i + 1] * n[1] + Fg[3 * i + 2] * n[2];
+    g1[i] = Fg[3 * i] * t1[0] + Fg[3 * i + 1] * t1[1] + Fg[3 * i + 2] * t1[2];
+    g2[i] = Fg[3 * i] * t2[0] + Fg[3 * i + 1] * t2[1] + Fg[3 * i + 2] * t2[2];
+  }
+  double eps = 1.0e-6;
+  for (int it = 0; it < 16; ++it) {
+    double r[3], rm[3];
+    normal_residual_h(h, n, t1, t2, g1, g2, T, m, r);
+    for (int i = 0; i < 3; ++i) rm[i] = ck[i] == NEU_ ? r[i] : 0.0;
+    if (sqrt(rm[0] * rm[0] + rm[1] * rm[1] + rm[2] * rm[2]) < 1.0e-10) break;
+    double A[9];
+    if (nj != 0 && m->model == 1) {
+      double F[9];
+      make_F_from_h(h, n, t1, t2, g1, g2, F);
+      double J = det3(F);
+      if (J < m->jf) J = m->jf;
+      double H[9] = {(F[4] * F[8] - F[5] * F[7]) / J, (F[5] * F[6] - F[3] * F[8]) / J,
+                     (F[3] * F[7] - F[4] * F[6]) / J, (F[2] * F[7] - F[1] * F[8]) / J,
+                     (F[0] * F[8] - F[2] * F[6]) / J, (F[1] * F[6] - F[0] * F[7]) / J,
+                     (F[1] * F[5] - F[2] * F[4]) / J, (F[2] * F[3] - F[0] * F[5]) / J,
+                     (F[0] * F[4] - F[1] * F[3]) / J};
+      double beta = 0.5 * m->lam * (J * J - 1.0) - m->mu, coeff = m->lam * J * J - beta;
+      double n2 = n[0] * n[0] + n[1] * n[1] + n[2] * n[2], v[3];
+      for (int i = 0; i < 3; ++i) v[i] = H[3 * i] * n[0] + H[3 * i + 1] * n[1] + H[3 * i + 2] * n[2];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+          A[3 * i + j] = i == j ? m->mu * n2 + coeff * v[i] * v[j] : coeff * v[i] * v[j];
+    } else {
+      for (int k = 0; k < 3; ++k) {
+        double hp[3] = {h[0], h[1], h[2]}, rp[3];
+        hp[k] = hp[k] + eps;
+        normal_residual_h(hp, n, t1, t2, g1, g2, T, m, rp);
+        for (int i = 0; i < 3; ++i) A[3 * i + k] = (rp[i] - r[i]) / eps;
+      }
+    }
+    for (int i = 0; i < 3; ++i)
+      if (ck[i] != NEU_)
+        for (int k = 0; k < 3; ++k) A[3 * i + k] = i == k ? 1.0 : 0.0;
+    double a = A[0], b = A[1], c = A[2], d = A[3], e = A[4], ff = A[5], g = A[6], hh = A[7], ii = A[8];
+    double det = a * (e * ii - ff * hh) - b * (d * ii - ff * g) + c * (d * hh - e * g);
+    if (fabs(det) < 1.0e-14) break;
+    double inv[9] = {(e * ii - ff * hh) / det, (c * hh - b * ii) / det, (b * ff - c * e) / det,
+                     (ff * g - d * ii) / det,  (a * ii - c * g) / det,  (c * d - a * ff) / det,
+                     (d * hh - e * g) / det,   (b * g - a * hh) / det,  (a * e - b * d) / det};
+    double dl[3];
+    for (int i = 0; i < 3; ++i)
+      dl[i] = -(inv[3 * i] * rm[0] + inv[3 * i + 1] * rm[1] + inv[3 * i + 2] * rm[2]);
+    double step = 1.0;
+    for (int ls = 0; ls < 12; ++ls) {
+      double cand[3], F[9];
+      for (int i = 0; i < 3; ++i) cand[i] = ck[i] == NEU_ ? h[i] + step * dl[i] : h[i];
+      make_F_from_h(cand, n, t1, t2, g1, g2, F);
+      if (det3(F) > m->jf) {
+        h[0] = cand[0];
+        h[1] = cand[1];
+        h[2] = cand[2];
+        break;
+      }
+      step = 0.5 * step;
+    }
+  }
+  make_F_from_h(h, n, t1, t2, g1, g2, out);
+}
+
 /* C3:2719-2725 _state_det3 */
 static double state_det3(const double *U) {
   return U[3] * (U[7] * U[11] - U[8] * U[10]) - U[4] * (U[6] * U[11] - U[8] * U[9]) +
@@ -1630,6 +1757,8 @@ static void sparse_link(const cvlbm3d_problem *p, const mat_t *m, const cvlbm3d_
     memcpy(Fb, F, sizeof F);
     if (ck[0] == NEU_ && ck[1] == NEU_ && ck[2] == NEU_)
       solve_Fb_arbitrary_normal(F, nx, ny, nz, T, m, p->normal_solver, Fb);
+    else if (ck[0] == NEU_ || ck[1] == NEU_ || ck[2] == NEU_)
+      solve_Fb_componentwise_normal(F, nx, ny, nz, T, ck, m, p->normal_solver, Fb);
     piola_mat(Fb, m, Pb);
   }
   if (f->link_kind) {

@@ -27,11 +27,15 @@ def _int_keys(dct):
 
 def boundary_kwargs(spec):
     out = dict(spec)
-    for key in ("id_kinds", "id_value_modes", "id_params"):
+    for key in ("id_kinds", "id_value_modes", "id_params", "id_component_kinds"):
         if key in out:
             out[key] = _int_keys(out[key])
     if out.get("id_params"):
         out["id_params"] = {k: tuple(v) for k, v in out["id_params"].items()}
+    if out.get("id_component_kinds"):
+        out["id_component_kinds"] = {k: tuple(v) for k, v in out["id_component_kinds"].items()}
+    if out.get("component_kinds"):
+        out["component_kinds"] = tuple(out["component_kinds"])
     if "params" in out:
         out["params"] = tuple(out["params"])
     return out

@@ -14,9 +14,12 @@ package or the benchmarks imports it.
 
 from __future__ import annotations
 
+import ast
+import inspect
 import itertools
 import math
 import sys
+import textwrap
 import types
 
 import numpy as np
@@ -98,6 +101,42 @@ def _vec(n):
     return make
 
 
+def _wp_value(v):
+    """Warp vectors and matrices are values: binding one to a new name copies it."""
+    if isinstance(v, np.ndarray) and not isinstance(v, _Array):
+        return v.copy()
+    return v
+
+
+class _CopyOnBind(ast.NodeTransformer):
+    """`x = y` with y a bare name becomes `x = _wp_value(y)`."""
+
+    def visit_Assign(self, node):
+        if len(node.targets) == 1 and isinstance(node.value, ast.Name):
+            node.value = ast.Call(func=ast.Name(id="_wp_value", ctx=ast.Load()),
+                                  args=[node.value], keywords=[])
+        return node
+
+
+def _value_semantics(fn):
+    """The decorated kernel or function with Warp's value semantics for
+    vectors and matrices (NumPy arrays alias on assignment; Warp values do
+    not: `fixed = h_old; fixed[0] = 0.0` must leave h_old unchanged)."""
+    try:
+        src = textwrap.dedent(inspect.getsource(fn))
+    except (OSError, TypeError):
+        return fn
+    tree = ast.parse(src)
+    fdef = tree.body[0]
+    fdef.decorator_list = []
+    tree = ast.fix_missing_locations(_CopyOnBind().visit(tree))
+    glb = fn.__globals__
+    glb.setdefault("_wp_value", _wp_value)
+    ns: dict = {}
+    exec(compile(tree, inspect.getsourcefile(fn) or "<warp>", "exec"), glb, ns)
+    return ns[fdef.name]
+
+
 def _launch(kernel, dim, inputs, device=None, **_kw):
     dims = (dim,) if isinstance(dim, int) else tuple(int(d) for d in dim)
     if len(dims) == 1:
@@ -124,8 +163,8 @@ def install() -> types.ModuleType:
     wp = types.ModuleType("warp")
     wp.init = lambda: None
     wp.set_module_options = lambda *a, **k: None
-    wp.func = lambda f: f
-    wp.kernel = lambda f: f
+    wp.func = _value_semantics
+    wp.kernel = _value_semantics
     wp.constant = lambda x: x
     wp.float64 = float
     wp.int32 = int

@@ -364,6 +364,21 @@ for _name, _opts in (("g2_mrt_ghost", dict(collision_model="mrt_ghost", ghost_om
     _c["solver"].update(_opts)
     _c["steps"] = 8
     CASES_2D[_name] = _c
+# links whose displacement rows mix Dirichlet and Neumann kinds (the
+# component-wise normal solve): the outer sphere with rows (N, D, N), Newton
+# with the acoustic Jacobian and with finite differences, and the energy solver
+for _name, _opts in (("g3_mixed_localf", {}),
+                     ("g3_mixed_fd", {"normal_jacobian": "finite_difference"}),
+                     ("g3_mixed_energy", {"neumann_solver": "energy"})):
+    _c = json.loads(json.dumps(CASES_3D["g3_shell_localf"]))
+    _c["geometry"]["nx"] = _c["geometry"]["ny"] = _c["geometry"]["nz"] = 14
+    _c["boundary"].update(value_mode=1, params=[0.01, -0.02, 0.015],
+                          id_value_modes={"1": 1, "2": 0},
+                          id_params={"1": [0.01, -0.02, 0.015], "2": []},
+                          id_component_kinds={"1": ["neumann", "dirichlet", "neumann"]})
+    _c["solver"].update(_opts)
+    _c["steps"] = 4
+    CASES_3D[_name] = _c
 for _m, _extra in MATERIALS_3D.items():
     _c = json.loads(json.dumps(CASES_3D["g3_shell_localf"]))
     _c["geometry"]["nx"] = _c["geometry"]["ny"] = _c["geometry"]["nz"] = 14
@@ -420,11 +435,15 @@ def _int_keys(d):
 
 def boundary_kwargs(spec):
     out = dict(spec)
-    for key in ("id_kinds", "id_value_modes", "id_params"):
+    for key in ("id_kinds", "id_value_modes", "id_params", "id_component_kinds"):
         if key in out:
             out[key] = _int_keys(out[key])
     if "id_params" in out and out["id_params"] is not None:
         out["id_params"] = {k: tuple(v) for k, v in out["id_params"].items()}
+    if out.get("id_component_kinds"):
+        out["id_component_kinds"] = {k: tuple(v) for k, v in out["id_component_kinds"].items()}
+    if out.get("component_kinds"):
+        out["component_kinds"] = tuple(out["component_kinds"])
     if "params" in out:
         out["params"] = tuple(out["params"])
     return out

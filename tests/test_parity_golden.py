@@ -26,6 +26,7 @@ GOLD3 = ["g3_shell_localf", "g3_shell_bfl_fd", "g3_shell_compat"]
 GOLD2 += [f"g2_mat_{m}" for m in ("svk", "log_neo_hooke", "mooney_rivlin", "yeoh", "gent",
                                    "sugiyama_svk")]
 GOLD2 += ["g2_mrt_ghost", "g2_kinetic_filter", "g2_mrt_filter"]
+GOLD3 += ["g3_mixed_localf", "g3_mixed_fd", "g3_mixed_energy"]
 GOLD3 += [f"g3_mat_{m}" for m in ("svk", "log_neo_hooke", "mooney_rivlin", "yeoh", "gent",
                                    "sph_neo_hooke")]
 
@@ -33,12 +34,13 @@ GOLD3 += [f"g3_mat_{m}" for m in ("svk", "log_neo_hooke", "mooney_rivlin", "yeoh
 # Material laws whose Piola map calls log/exp/pow.  The reference evaluates
 # them with the host libm (as the oracle does, which matches every fixture
 # element by element); CUDA's versions are within one ulp of it but not
-# identical, and 8 steps of the traction cases carry those ulps to about
-# 1e-11 of the field's largest entry (measured: at most 1.1e-11).  For these
-# laws the absolute floor is scaled to the field: 2e-11 x max|ref|.
+# identical, and the 4-8 steps of these traction cases carry those ulps to
+# at most 1.1e-11 (populations) and 5e-11 (the small displacement fields) of
+# a field's largest entry (measured).  For these laws the absolute floor is
+# scaled to the field: 1e-10 x max|ref|.
 TRANSCENDENTAL = ("log_neo_hooke", "mooney_rivlin", "yeoh", "gent", "sugiyama_svk",
                   "sph_neo_hooke")
-FIELD_ATOL = 2e-11
+FIELD_ATOL = 1e-10
 
 
 def _atol_for(cfg):
@@ -106,7 +108,7 @@ def test_3d_steps_match_reference(golden_dir, name):
         close("char_state", s.char_state.cpu().numpy(), d["char_state"], field_atol=fa)
     s.refresh_current()
     close("U", s.active_system_state(), d["U"], field_atol=fa)
-    close("u", s.active_displacement(), d["u"])
+    close("u", s.active_displacement(), d["u"], field_atol=fa)
 
 
 def test_3d_localf_with_device_stencil_near_reference(golden_dir):
