@@ -661,9 +661,11 @@ struct FusedLaunch2 {
 // Variant 5 selects the split form (cvlbm2d_split.cuh) instead of a tile
 // shape; variants 6 and 7 are the PRE form (moments of every active node
 // written once per step by k_mom2 into fields->fpost, halo moments read from
-// there instead of recomputed), which runs without the link overlap.
+// there instead of recomputed), which runs without the link overlap;
+// variants 8-10 keep the owned nodes' populations in shared memory from the
+// moments to the collision (STAGE) instead of reloading them.
 constexpr int kSplitVariant = 5;
-constexpr int kMaxVariant = 7;
+constexpr int kMaxVariant = 10;
 
 FusedLaunch2 fused_variant(int v) {
   switch (v) {
@@ -674,6 +676,9 @@ FusedLaunch2 fused_variant(int v) {
     case kSplitVariant: return {nullptr, 0, 0, 16, nullptr};  // split kernels, no tiles used
     case 6: return {k_fused2<16, 1, true>, kTX * 16, fused_smem2<16>(), 16, k_mom2<16>};
     case 7: return {k_fused2<8, 3, true>, kTX * 8, fused_smem2<8>(), 8, k_mom2<8>};
+    case 8: return {k_fused2<8, 2, false, true>, kTX * 8, fused_smem2<8, true>(), 8, nullptr};
+    case 9: return {k_fused2<16, 1, false, true>, kTX * 16, fused_smem2<16, true>(), 16, nullptr};
+    case 10: return {k_fused2<4, 4, false, true>, kTX * 4, fused_smem2<4, true>(), 4, nullptr};
     default: return {k_fused2<16, 1, false>, kTX * 16, fused_smem2<16>(), 16, nullptr};
   }
 }

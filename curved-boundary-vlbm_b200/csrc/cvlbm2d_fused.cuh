@@ -78,10 +78,11 @@ __device__ __forceinline__ void moments2c(const Ctx2& c, const double* __restric
 // Region flags in shared memory: bit 0 active, bit 1 holds a cut link
 constexpr int kFlagLinks = 2;
 
-template <int TY>
+template <int TY, bool STAGE = false>
 constexpr size_t fused_smem2() {
   return sizeof(double) * (6 * kRX * (TY + 2 * kH) + 2 * kSX * (TY + 4)) +
-         sizeof(int) * kRX * (TY + 2 * kH);
+         sizeof(double) * ((kRX * (TY + 2 * kH) + 1) / 2) +  // int flags, padded to 8 bytes
+         (STAGE ? sizeof(double) * 24 * kTX * TY : 0);
 }
 
 // One tile of the fused step (phases A-C above); `tile` is a tile id of the
@@ -90,7 +91,7 @@ constexpr size_t fused_smem2() {
 // moments of every active node were written by k_mom2 into `mom` this step
 // ([8][N]: U (6), collide-time u (2)), so phase A reads them instead of
 // summing populations (the same doubles: k_mom2 evaluates the same sums).
-template <int TY, bool PRE = false>
+template <int TY, bool PRE = false, bool STAGE = false>
 __device__ __forceinline__ void fused2_tile(
     const Ctx2& c, const Fused2& fz, int tile, const double* __restrict__ f0,
     double* __restrict__ f1, double* __restrict__ Ug, double* __restrict__ ug,
@@ -104,6 +105,9 @@ __device__ __forceinline__ void fused2_tile(
   double(*sU)[kRN] = reinterpret_cast<double(*)[kRN]>(smem2 + 4 * kRN);  // collide-time u
   double(*sN)[kSN] = reinterpret_cast<double(*)[kSN]>(smem2 + 6 * kRN);  // swept u, tile+2
   int* sA = reinterpret_cast<int*>(smem2 + 6 * kRN + 2 * kSN);           // active flags
+  // STAGE: the owned nodes' populations, kept from phase A for phase C
+  double* sfo = smem2 + 6 * kRN + 2 * kSN + (kRN + 1) / 2;  // [24][kTX*TY]
+  constexpr int kTN = kTX * TY;
 
   const cvlbm2d_problem& p = c.p;
   const int N = c.N, nx = p.nx, ny = p.ny;
@@ -130,6 +134,27 @@ __device__ __forceinline__ void fused2_tile(
       for (int a = 0; a < 6; ++a) S[a] = mom[(size_t)a * N + n];
       ucol0 = mom[6 * (size_t)N + n];
       ucol1 = mom[7 * (size_t)N + n];
+    } else if constexpr (STAGE) {
+      // moments2c with every population also kept in shared memory
+#pragma unroll
+      for (int a = 0; a < 6; ++a) S[a] = 0.0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int a = 0; a < 6; ++a) {
+          const double v = f0[(size_t)(q * 6 + a) * N + n];
+          sfo[(q * 6 + a) * kTN + threadIdx.x] = v;
+          S[a] += v;
+        }
+      if (p.source_mode == kSrcConstant) {
+#pragma unroll
+        for (int a = 0; a < 6; ++a) S[a] += c.hdt * p.source[a];
+      } else if (p.source_mode == kSrcDamping) {
+        S[0] = S[0] / c.den;
+        S[1] = S[1] / c.den;
+      }
+      ucol0 = ustar[n] + c.hdt * S[0];
+      ucol1 = ustar[N + n] + c.hdt * S[1];
     } else {
       moments2c(c, f0, n, S);
       ucol0 = ustar[n] + c.hdt * S[0];
@@ -383,7 +408,11 @@ __device__ __forceinline__ void fused2_tile(
       const bool neg = cq < 0 || cy < 0;
       const bool has_g = cq != 0 ? hx : hy;
       const double g = cq != 0 ? gx : gy;
-      const double old = f0[(size_t)(q * 6 + a) * N + n];
+      double old;
+      if constexpr (STAGE)
+        old = sfo[(q * 6 + a) * kTN + threadIdx.x];
+      else
+        old = f0[(size_t)(q * 6 + a) * N + n];
       const double fe = 0.25 * (has_g ? (neg ? Ua - g : Ua + g) : Ua);
       double v = old + om * (fe - old);
       if (add_src && (a < 2 || add_src_f)) v = v + swB;
@@ -421,7 +450,7 @@ __device__ __forceinline__ void fused2_tile(
 
 // Tile kTX x TY, one node per thread; MINB resident blocks per SM bounds the
 // registers per thread (tuned per problem, see curved_lbm autotune).
-template <int TY, int MINB, bool PRE>
+template <int TY, int MINB, bool PRE, bool STAGE = false>
 __global__ void __launch_bounds__(kTX * TY, MINB)
     k_fused2(Ctx2 c, Fused2 fz, const double* __restrict__ f0, double* __restrict__ f1,
              double* __restrict__ Ug, double* __restrict__ ug,
@@ -429,8 +458,8 @@ __global__ void __launch_bounds__(kTX * TY, MINB)
              int* __restrict__ invalid, const double* clock, double t_host, int do_sweep,
              int do_repair, const double* __restrict__ mom) {
   extern __shared__ double smem2[];
-  fused2_tile<TY, PRE>(c, fz, fz.tiles[blockIdx.x], f0, f1, Ug, ug, ustar, ustar_out, invalid,
-                       clock, t_host, do_sweep, do_repair, smem2, mom);
+  fused2_tile<TY, PRE, STAGE>(c, fz, fz.tiles[blockIdx.x], f0, f1, Ug, ug, ustar, ustar_out,
+                              invalid, clock, t_host, do_sweep, do_repair, smem2, mom);
 }
 
 // Collide-time moments of the active nodes of the listed tiles, for the PRE

@@ -155,24 +155,31 @@ def _recon_name(rid: int) -> str:
 WAVE_CHUNK = 128  # nodes per work item of the wavefront kernel (its block size)
 
 
-def _wave_tables3(active_i, nx: int):
+WAVE_LAGS = (1, 3)  # planes by which the sweep and the collide trail the moments
+
+
+def _wave_tables3(active_i, nx: int, lags=WAVE_LAGS):
     """Work items of the wavefront node kernel (node_variant 3/4), in ticket order.
 
     The active ids run through the x-planes in order; each plane is cut into
     chunks of WAVE_CHUNK nodes.  For w = 0, 1, ... the items are the moments
-    chunks of plane w, the sweep chunks of plane w-1 and the collide chunks of
-    plane w-3: every item depends only on items before it (sweep of plane i
-    on the moments of i-1..i+1, collide of plane i on the sweeps of
-    i-2..i+2).  Returns (items [n, 4] int32: stage, plane, first id, end id;
-    chunks per plane [nx] int32).
+    chunks of plane w, the sweep chunks of plane w-ls and the collide chunks
+    of plane w-lc, (ls, lc) = `lags` with ls >= 1 and lc >= ls + 2: every
+    item depends only on items before it (sweep of plane i on the moments of
+    i-1..i+1, collide of plane i on the sweeps of i-2..i+2); larger lags wait
+    less and keep more planes in flight.  Returns (items [n, 4] int32: stage,
+    plane, first id, end id; chunks per plane [nx] int32).
     """
+    ls, lc = int(lags[0]), int(lags[1])
+    if ls < 1 or lc < ls + 2:
+        raise ValueError(f"wave lags {lags} break the item order (need ls >= 1, lc >= ls + 2)")
     ai = np.asarray(active_i, dtype=np.int64)
     start = np.searchsorted(ai, np.arange(nx + 1), side="left")
     counts = np.diff(start)
     chunks = ((counts + WAVE_CHUNK - 1) // WAVE_CHUNK).astype(np.int32)
     rows = []
-    for w in range(nx + 3):
-        for stage, plane in ((0, w), (1, w - 1), (2, w - 3)):
+    for w in range(nx + lc):
+        for stage, plane in ((0, w), (1, w - ls), (2, w - lc)):
             if 0 <= plane < nx:
                 a, b = int(start[plane]), int(start[plane + 1])
                 for c0 in range(a, b, WAVE_CHUNK):
@@ -417,7 +424,8 @@ class WarpSparseCurvedBoundaryLBM3D:
         self._n_link_nodes = int(link_nodes.size)
         if link_nodes.size:
             t["link_nodes"] = dev_i(link_nodes)
-        items, chunks = _wave_tables3(tables["active_i"], self.nx)
+        self._active_i_np = np.asarray(tables["active_i"])
+        items, chunks = _wave_tables3(self._active_i_np, self.nx)
         self._n_wave_items = int(items.shape[0])
         t["wave_items"] = dev_i(items.reshape(-1))
         t["wave_plane_chunks"] = dev_i(chunks)
@@ -722,6 +730,14 @@ class WarpSparseCurvedBoundaryLBM3D:
         if int(variant) not in self.NODE_VARIANTS:
             raise ValueError(f"fused collide variant {variant} does not exist")
         self._problem.node_variant = int(variant)
+
+    def _set_wave_lags(self, lags) -> None:
+        """Rebuild the wavefront item order with other stage lags (same results)."""
+        import torch
+
+        items, _ = _wave_tables3(self._active_i_np, self.nx, lags)
+        self._tables["wave_items"] = torch.as_tensor(items.reshape(-1), device=self._tdev)
+        self._problem.wave_items = _native.ptr(self._tables["wave_items"])
 
     def autotune(self, steps: int = 10, variants=None) -> dict:
         """Time every fused collide variant on this problem; keep the fastest.

@@ -582,7 +582,7 @@ class WarpCurvedBoundaryLBM2D:
             return {}
         saved = (self.f0.clone(), self.f1.clone(), self.u_star.clone(), self.U.clone(),
                  self.u.clone(), self.time, self.steps)
-        cand = [v for v in (variants if variants is not None else range(8))
+        cand = [v for v in (variants if variants is not None else range(16))
                 if int(self._lib.cvlbm2d_tile_variant(int(v))) > 0]
         times = {}
         use_graphs, self.use_graphs = self.use_graphs, False  # time launches, not captures

@@ -10,7 +10,9 @@ reports the first check (every `--every` steps) at which the oracle's state
 is invalid (the reference's `invalid_state`: flag set, or U not finite), or
 that it stayed valid for `--steps` steps.
 
-    python oracle/replay_instances.py --ids 3,17,42 [--steps 2000] [--procs 4]
+    python oracle/replay_instances.py --ids 3,17:900,42 [--steps 2000] [--procs 4]
+
+(`id:steps` sets that instance's own step limit.)
 
 Prints one JSON line per instance and a summary line.
 """
@@ -68,23 +70,27 @@ def replay(args):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ids", required=True, help="comma-separated instance numbers")
+    ap.add_argument("--ids", required=True,
+                    help="comma-separated instance numbers, each optionally id:steps")
     ap.add_argument("--instances", type=int, default=256, help="size of the seeded table")
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--every", type=int, default=100)
     ap.add_argument("--procs", type=int, default=max(1, (os.cpu_count() or 1) // 2))
     a = ap.parse_args()
-    ids = [int(v) for v in a.ids.split(",") if v.strip()]
+    ids = []
+    for v in a.ids.split(","):
+        if v.strip():
+            i, _, st = v.partition(":")
+            ids.append((int(i), int(st) if st else a.steps))
     threads = max(1, (os.cpu_count() or 1) // max(1, a.procs))
-    jobs = [(i, a.steps, a.every, threads, a.instances) for i in ids]
+    jobs = [(i, st, a.every, threads, a.instances) for i, st in ids]
     with mp.get_context("spawn").Pool(a.procs) as pool:
         out = []
         for r in pool.imap_unordered(replay, jobs):
             print(json.dumps(r), flush=True)
             out.append(r)
     bad = sorted(r["instance"] for r in out if r["invalid_at_step"] is not None)
-    print(json.dumps({"replayed": len(out), "invalid_on_oracle": len(bad), "invalid_ids": bad,
-                      "steps": a.steps}))
+    print(json.dumps({"replayed": len(out), "invalid_on_oracle": len(bad), "invalid_ids": bad}))
 
 
 if __name__ == "__main__":

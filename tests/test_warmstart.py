@@ -18,7 +18,9 @@ from oracle import fno_oracle as fo
 # native (fp32 weights and accumulation, bf16 GEMM operands) against the FP64
 # oracle rounding at the same bf16 points: the remaining differences are fp32
 # accumulation and the odd element rounding to the other bf16 neighbour
-GRAD_RTOL = 2e-2
+# (measured on a B200: at most 4.2e-4 relative, first spectral layer; the
+# other tensors 2e-5 - 1e-4)
+GRAD_RTOL = 2e-3
 
 
 def _random_params(rng, cin, c, cout, M, L):
