@@ -599,10 +599,10 @@ void launch_links(const Ctx2& c, const double* src, double* dst, const double* U
                   cudaStream_t s, int fused = 0, const double* scratch = nullptr,
                   const int32_t* partner = nullptr, double* clock_next = nullptr) {
   if (c.p.n_links <= 0) return;
-  const int per = 128 / kLG;
+  const int per = kLinksPerBlock2;
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3(blocks(c.p.n_links, per));
-  cfg.blockDim = dim3(128);
+  cfg.blockDim = dim3(kLinkThreads2);
   cfg.dynamicSmemBytes = 0;
   cfg.stream = s;
   cudaLaunchAttribute attr[1];

@@ -1,7 +1,7 @@
 // Batched D2Q4x6 step: many independent problems (geometries, load cases,
 // uneven lattice sizes) advanced together.  Included at the end of
 // cvlbm2d.cu; reuses the fused tile body (fused2_tile) and the cooperative
-// link body (link2_group).
+// link body (link2_block).
 //
 // Per lattice step three launches cover every instance:
 //   k_batch_nodes2   persistent: a grid of (SMs x resident blocks) walks the
@@ -78,20 +78,19 @@ __global__ void __launch_bounds__(kTX * TY, MINB)
   }
 }
 
-__global__ void __launch_bounds__(128, 4)
+__global__ void __launch_bounds__(kLinkThreads2, 4)
     k_batch_links2(const Inst2* __restrict__ inst, const InstState2* __restrict__ st,
                    const int2* __restrict__ work, int n_work) {
-  __shared__ LinkShared2 sh[128 / kLG];
-  const int lane = threadIdx.x & (kLG - 1);
-  const int grp = threadIdx.x / kLG;
+  __shared__ LinkShared2 sh[kLinksPerBlock2];
   for (int w = blockIdx.x; w < n_work; w += gridDim.x) {
-    __syncwarp();
     const int2 wk = work[w];
+    // uniform over the block (one work item per iteration): the barriers
+    // inside link2_block are reached by every thread or by none
     if (!st[wk.x].active) continue;
     const Inst2& I = inst[wk.x];
     double* f1 = I.f[parity_of(st[wk.x]) ^ 1];
-    link2_group(I.c, sh[grp], lane, wk.y + grp, f1, f1, I.U, I.u, &st[wk.x].clock, 0.0,
-                0.5 * I.c.p.dt, 1, I.scratch, I.partner);
+    link2_block(I.c, sh, wk.y, f1, f1, I.U, I.u, &st[wk.x].clock, 0.0, 0.5 * I.c.p.dt, 1,
+                I.scratch, I.partner);
   }
 }
 
@@ -241,7 +240,7 @@ void batch_nodes(cvlbm2d_batch* b, int w0, int w1, int store_all, cudaStream_t s
 void batch_links_tick(cvlbm2d_batch* b, int l0, int l1, int i0, int i1, cudaStream_t s) {
   if (l1 > l0) {
     const int grid = b->link_grid < l1 - l0 ? b->link_grid : l1 - l0;
-    k_batch_links2<<<grid, 128, 0, s>>>(b->d_inst, b->d_state, b->d_lwork + l0, l1 - l0);
+    k_batch_links2<<<grid, kLinkThreads2, 0, s>>>(b->d_inst, b->d_state, b->d_lwork + l0, l1 - l0);
     cv::count_launches(1);
   }
   if (i1 > i0) {
@@ -356,7 +355,7 @@ extern "C" int cvlbm2d_batch_create(int32_t n_inst, const cvlbm2d_problem* probl
     // raster order (a solver's list may hold its inner tiles first)
     std::sort(tiles.begin(), tiles.end());
     for (int t : tiles) work.push_back(make_int2(i, t));
-    for (int l = 0; l < p->n_links; l += 128 / kLG) lwork.push_back(make_int2(i, l));
+    for (int l = 0; l < p->n_links; l += kLinksPerBlock2) lwork.push_back(make_int2(i, l));
   }
   work_start[n_inst] = (int)work.size();
   cvlbm2d_batch* b = new cvlbm2d_batch();
@@ -384,7 +383,7 @@ extern "C" int cvlbm2d_batch_create(int32_t n_inst, const cvlbm2d_problem* probl
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.nodes, v.threads, v.smem);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_l, k_batch_links2, 128, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_l, k_batch_links2, kLinkThreads2, 0);
   const int full = sms * (per_sm > 0 ? per_sm : 1);
   b->node_grid = grid_blocks > 0 ? grid_blocks : full;
   if (b->node_grid > b->n_work) b->node_grid = b->n_work > 0 ? b->n_work : 1;

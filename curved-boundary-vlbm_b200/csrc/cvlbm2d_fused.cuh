@@ -486,18 +486,97 @@ __global__ void __launch_bounds__(kTX * TY)
 }
 
 // ---------------------------------------------------------------------------
-// Cooperative cut-link kernel: 16 lanes per link, 8 links per 128-thread block.
-// Lanes 0-5 gather d/dx of component `lane`, lanes 6-11 d/dy, lanes 12-15 the
-// F predictor; lane 0 runs the Newton solve; lanes 0/1 the two flux tangents;
-// lanes 0-5 write one population row each.  Links are visited in `order`
-// (traction links first) so a warp's links take the same branches.
+// Cut-link kernel: 8 links per 64-thread block, in two stages.
+//   gather  8 lanes per link, 16 gathered quantities: q < 6 sums d/dx of
+//           component q over the link's 24-node stencil, 6 <= q < 12 d/dy of
+//           component q - 6, 12 <= q < 16 the F predictor component q - 12;
+//           lane l takes q = l and l + 8 (one code path for every lane on
+//           characteristic links); lanes 0/1 then the tangential image of u
+//           (compatible predictors on a traction wall).
+//   finish  one thread per link: predictor, normal-image solve,
+//           characteristic state and flux tangents, the six population rows.
+//           In one thread the independent chains (the two flux tangents, the
+//           six rows, the BFL population loads) overlap instead of running
+//           lane after lane, and a warp carries 8 links, not 2.
+// Links are visited in `order` (traction links first) so neighbouring links
+// take the same branches.
 // ---------------------------------------------------------------------------
-constexpr int kLG = 16;
+constexpr int kLG = 8;
+constexpr int kLinksPerBlock2 = 8;
+constexpr int kLinkThreads2 = kLG * kLinksPerBlock2;
 
 struct LinkShared2 {
-  double Fg[4], ux[6], uy[6], dut[2], wt_abs;
-  double Fb[4], cv[6], cw[6], Ax[6], Ay[6], eqx[6], eqy[6], Pb[4], Pc[4];
+  double g[16];  // ux[6], uy[6], Fg[4]
+  double dut[2], wt_abs;
 };
+
+// Per-link inputs: the link row when the host built rows, else the link tables.
+struct LinkIn2 {
+  const double* pp;
+  double eta, xb, yb, nxb, nyb;
+  int ell, i, j, qo, qi, kind, mode, n, nu;
+  bool live, rowed, up_ok, lsq_ok;
+};
+
+__device__ __forceinline__ LinkIn2 link2_in(const Ctx2& c, int slot) {
+  const cvlbm2d_problem& p = c.p;
+  LinkIn2 L;
+  L.live = slot < p.n_links;
+  L.rowed = p.link_rows != nullptr;
+  L.pp = p.bc_params;
+  L.eta = 0.5;
+  L.xb = L.yb = L.nyb = 0.0;
+  L.nxb = 1.0;
+  L.ell = L.i = L.j = L.qo = L.n = L.nu = L.mode = 0;
+  L.qi = 2;
+  L.kind = kDirichlet;
+  L.up_ok = L.lsq_ok = false;
+  if (!L.live) return L;
+  int bid;
+  if (L.rowed) {
+    // every per-link input is one load away from the slot (no link_order /
+    // link-table / stencil-id indirection)
+    const cvlbm2d_link_row* row = p.link_rows + slot;
+    L.ell = row->ell;
+    L.i = row->i;
+    L.j = row->j;
+    L.qo = row->q;
+    bid = row->bid;
+    L.eta = row->eta;
+    L.xb = row->xb;
+    L.yb = row->yb;
+    L.nxb = row->nx;
+    L.nyb = row->ny;
+    L.n = row->node;
+    L.up_ok = row->upstream >= 0;
+    L.nu = L.up_ok ? row->upstream : L.n;
+    L.lsq_ok = row->lsq_valid != 0;
+  } else {
+    const int ell = p.link_order ? p.link_order[slot] : slot;
+    L.ell = ell;
+    L.i = p.link_i[ell];
+    L.j = p.link_j[ell];
+    L.qo = p.link_q[ell];
+    bid = p.link_bid[ell];
+    L.eta = p.link_eta[ell];
+    L.xb = p.link_xb[ell];
+    L.yb = p.link_yb[ell];
+    L.nxb = p.link_nx[ell];
+    L.nyb = p.link_ny[ell];
+    L.n = L.i * p.ny + L.j;
+    const int iu = L.i - cx2(L.qo), ju = L.j - cy2(L.qo);
+    L.up_ok = iu >= 0 && iu < p.nx && ju >= 0 && ju < p.ny && p.active[iu * p.ny + ju] != 0;
+    L.nu = L.up_ok ? iu * p.ny + ju : L.n;
+    L.lsq_ok = p.lsq_valid[ell] != 0;
+  }
+  if (bid < 0 || bid >= kMaxIds2) bid = 0;
+  L.kind = p.bc_kind[bid];
+  L.mode = p.bc_mode[bid];
+  L.pp = p.bc_params + bid * 8;
+  L.qi = L.qo + 2;
+  if (L.qi >= 4) L.qi -= 4;
+  return L;
+}
 
 // sum_m w[m] * Uc[node[m]] over the 24 stencil slots in slot order (as
 // _lsq_U_at_boundary, two_d/curved_boundary_warp.py:1213-1221), with all
@@ -520,215 +599,191 @@ __device__ __forceinline__ double lsq_sum(const int* __restrict__ node, const do
   return out;
 }
 
-// One cut link (processing slot `slot`) on the 16 lanes of a group; every
-// lane of the group calls it (only __syncwarp inside).
-__device__ __forceinline__ void link2_group(
-    const Ctx2& c, LinkShared2& S, int lane, int slot, const double* __restrict__ fpost,
-    double* __restrict__ fout, const double* __restrict__ U, const double* __restrict__ u,
-    const double* clock, double t_host, double offset, int fused,
-    const double* __restrict__ scratch, const int32_t* __restrict__ partner) {
+// Gather stage of one link (slot `slot`) on lane `lane` of its 8-lane group.
+__device__ __forceinline__ void link2_gather(const Ctx2& c, LinkShared2& S, int lane, int slot,
+                                             const double* __restrict__ U,
+                                             const double* __restrict__ u) {
+  const cvlbm2d_problem& p = c.p;
+  const LinkIn2 L = link2_in(c, slot);
+  if (!L.live) return;
+  const int N = c.N, recon = p.recon;
+  // stencil ids and weights of this link (slot order when rows are given)
+  const size_t sl = (size_t)(L.rowed ? slot : L.ell) * kMaxLsq2;
+  const int* lnode = (L.rowed ? p.lsq_node_slot : p.lsq_node) + sl;
+  const bool lsq_recon = (recon == 11 || recon == 12) && L.lsq_ok;
+  const bool use_char = lsq_recon && L.kind == kNeumann;
+  const bool compat = (recon == 9 || recon == 11) && L.lsq_ok;
+#pragma unroll
+  for (int q = lane; q < 16; q += kLG) {
+    if (q < 12 ? use_char : lsq_recon) {
+      const double* w = q < 6 ? (L.rowed ? p.lsq_wx_slot : p.lsq_wx)
+                      : q < 12 ? (L.rowed ? p.lsq_wy_slot : p.lsq_wy)
+                               : (L.rowed ? p.lsq_wb_slot : p.lsq_wb);
+      const int comp = q < 6 ? q : q < 12 ? q - 6 : q - 10;
+      S.g[q] = lsq_sum(lnode, w + sl, U + (size_t)comp * N);
+    } else if (q >= 12) {
+      const double* Uk = U + (size_t)(q - 10) * N;
+      double fg;
+      if (recon == 0 || recon == 2 || recon == 13) {
+        fg = L.up_ok ? Uk[L.n] + L.eta * (Uk[L.n] - Uk[L.nu]) : Uk[L.n];
+        if (recon == 2 && L.lsq_ok)
+          fg = lsq_sum(lnode, (L.rowed ? p.lsq_wb_slot : p.lsq_wb) + sl, Uk);
+      } else {
+        fg = interp_link(Uk, p.active, L.i, L.j, L.qo, L.eta, p.nx, p.ny);
+      }
+      S.g[q] = fg;
+    }
+  }
+  if (compat && L.kind == kNeumann && lane < 2) {
+    // tangential image of u along the wall, component `lane`
+    const double* wt = (L.rowed ? p.lsq_wt_slot : p.lsq_wt) + sl;
+    double d = 0.0, wa = 0.0;
+    for (int mm = 0; mm < kMaxLsq2; ++mm) {
+      const int nd = lnode[mm];
+      if (nd >= 0) {
+        d += wt[mm] * u[(size_t)lane * N + nd];
+        wa += fabs(wt[mm]);
+      }
+    }
+    S.dut[lane] = d;
+    if (lane == 0) S.wt_abs = wa;
+  }
+}
+
+// BFL inputs of population row a of a link: the outgoing post-collision value
+// fo, the incoming fi and the upstream value upv.
+__device__ __forceinline__ void link2_bfl_in(const LinkIn2& L, int a, int N,
+                                             const double* __restrict__ fpost, int fused,
+                                             const double* __restrict__ scratch,
+                                             const int32_t* __restrict__ partner, double& fo,
+                                             double& fi, double& upv) {
+  if (fused) {
+    fo = scratch[(size_t)L.ell * 6 + a];
+    fi = L.up_ok ? fpost[(size_t)(L.qi * 6 + a) * N + L.nu]
+                 : scratch[(size_t)partner[L.ell] * 6 + a];
+    upv = L.up_ok ? fpost[(size_t)(L.qo * 6 + a) * N + L.n] : fo;
+  } else {
+    fo = fpost[(size_t)(L.qo * 6 + a) * N + L.n];
+    fi = fpost[(size_t)(L.qi * 6 + a) * N + L.n];
+    upv = L.up_ok ? fpost[(size_t)(L.qo * 6 + a) * N + L.nu] : fo;
+  }
+}
+
+// Finish stage of one link, on one thread.
+__device__ __forceinline__ void link2_finish(
+    const Ctx2& c, const LinkShared2& S, int slot, const double* __restrict__ fpost,
+    double* __restrict__ fout, const double* __restrict__ U, const double* clock, double t_host,
+    double offset, int fused, const double* __restrict__ scratch,
+    const int32_t* __restrict__ partner) {
   const cvlbm2d_problem& p = c.p;
   const Mat& m = c.m;
-  const bool live = slot < p.n_links;
-  // with link rows every per-link input the chain starts from is one load
-  // away from the slot (no link_order / link-table / stencil-id indirection)
-  const cvlbm2d_link_row* row = (live && p.link_rows) ? p.link_rows + slot : nullptr;
-  const int ell = live ? (row ? row->ell : (p.link_order ? p.link_order[slot] : slot)) : 0;
-  const int N = c.N, nx = p.nx, ny = p.ny, recon = p.recon;
+  const LinkIn2 L = link2_in(c, slot);
+  if (!L.live) return;
+  const int N = c.N, recon = p.recon, kind = L.kind, mode = L.mode, n = L.n, qi = L.qi;
+  const double* pp = L.pp;
+  const double nxb = L.nxb, nyb = L.nyb, eta = L.eta;
+  const bool lsq_recon = (recon == 11 || recon == 12) && L.lsq_ok;
+  const bool use_char = lsq_recon && kind == kNeumann;
+  const bool compat = (recon == 9 || recon == 11) && L.lsq_ok;
+  // loads that do not depend on the chain below go first
+  const double Un0 = U[n], Un1 = U[(size_t)N + n];
+  double fo[6], fi[6], upv[6];
+  if (!use_char) {
+#pragma unroll
+    for (int a = 0; a < 6; ++a) link2_bfl_in(L, a, N, fpost, fused, scratch, partner, fo[a],
+                                             fi[a], upv[a]);
+  }
   const double tmid = time_of(clock, t_host, offset);
-
-  int i = 0, j = 0, qo = 0, qi = 2, kind = kDirichlet, mode = 0, n = 0, nu = 0;
-  double eta = 0.5, xb = 0, yb = 0, nxb = 1, nyb = 0, bv0 = 0, bv1 = 0;
-  bool up_ok = false, lsq_ok = false;
-  const double* pp = p.bc_params;
-  if (live) {
-    int bid;
-    if (row) {
-      i = row->i;
-      j = row->j;
-      qo = row->q;
-      bid = row->bid;
-      eta = row->eta;
-      xb = row->xb;
-      yb = row->yb;
-      nxb = row->nx;
-      nyb = row->ny;
-      n = row->node;
-      up_ok = row->upstream >= 0;
-      nu = up_ok ? row->upstream : n;
-      lsq_ok = row->lsq_valid != 0;
-    } else {
-      i = p.link_i[ell];
-      j = p.link_j[ell];
-      qo = p.link_q[ell];
-      bid = p.link_bid[ell];
-      eta = p.link_eta[ell];
-      xb = p.link_xb[ell];
-      yb = p.link_yb[ell];
-      nxb = p.link_nx[ell];
-      nyb = p.link_ny[ell];
-      n = i * ny + j;
-      const int iu = i - cx2(qo), ju = j - cy2(qo);
-      up_ok = iu >= 0 && iu < nx && ju >= 0 && ju < ny && p.active[iu * ny + ju] != 0;
-      nu = up_ok ? iu * ny + ju : n;
-      lsq_ok = p.lsq_valid[ell] != 0;
-    }
-    if (bid < 0 || bid >= kMaxIds2) bid = 0;
-    kind = p.bc_kind[bid];
-    mode = p.bc_mode[bid];
-    pp = p.bc_params + bid * 8;
-    qi = qo + 2;
-    if (qi >= 4) qi -= 4;
-    bv0 = value2(0, mode, pp, xb, yb, nxb, nyb, tmid);
-    bv1 = value2(1, mode, pp, xb, yb, nxb, nyb, tmid);
-    if (kind == kNeumann && p.use_dynamic_traction != 0) {
-      bv0 = p.traction_x[ell];
-      bv1 = p.traction_y[ell];
-    }
+  double bv0 = value2(0, mode, pp, L.xb, L.yb, nxb, nyb, tmid);
+  double bv1 = value2(1, mode, pp, L.xb, L.yb, nxb, nyb, tmid);
+  if (kind == kNeumann && p.use_dynamic_traction != 0) {
+    bv0 = p.traction_x[L.ell];
+    bv1 = p.traction_y[L.ell];
   }
-  // stencil ids and weights of this link (slot order when rows are given)
-  const size_t sl = (size_t)(row ? slot : ell) * kMaxLsq2;
-  const int* lnode = (row ? p.lsq_node_slot : p.lsq_node) + sl;
-  const double* w_b = (row ? p.lsq_wb_slot : p.lsq_wb) + sl;
-  const double* w_t = (row ? p.lsq_wt_slot : p.lsq_wt) + sl;
-  const double* w_x = (row ? p.lsq_wx_slot : p.lsq_wx) + sl;
-  const double* w_y = (row ? p.lsq_wy_slot : p.lsq_wy) + sl;
-  const bool use_char = live && (recon == 11 || recon == 12) && kind == kNeumann && lsq_ok;
-  const bool compat = live && (recon == 9 || recon == 11) && lsq_ok;
-
-  // -- gathers ----------------------------------------------------------------
-  if (live) {
-    if (lane < 12) {
-      const int a = lane < 6 ? lane : lane - 6;
-      if (use_char) {
-        const double g = lsq_sum(lnode, lane < 6 ? w_x : w_y, U + (size_t)a * N);
-        if (lane < 6)
-          S.ux[a] = g;
-        else
-          S.uy[a] = g;
-      } else if (compat && kind == kNeumann && lane < 2) {
-        const double* wt = w_t;
-        double d = 0.0, wa = 0.0;
-        for (int mm = 0; mm < kMaxLsq2; ++mm) {
-          const int nd = lnode[mm];
-          if (nd >= 0) {
-            d += wt[mm] * u[(size_t)lane * N + nd];
-            wa += fabs(wt[mm]);
-          }
-        }
-        S.dut[lane] = d;
-        if (lane == 0) S.wt_abs = wa;
-      }
-    } else {
-      const int k = lane - 12;
-      const double* Uk = U + (size_t)(2 + k) * N;
-      double fg;
-      if ((recon == 11 || recon == 12) && lsq_ok) {
-        fg = lsq_sum(lnode, w_b, Uk);
-      } else if (recon == 0 || recon == 2 || recon == 13) {
-        fg = up_ok ? Uk[n] + eta * (Uk[n] - Uk[nu]) : Uk[n];
-        if (recon == 2 && lsq_ok) fg = lsq_sum(lnode, w_b, Uk);
-      } else {
-        fg = interp_link(Uk, p.active, i, j, qo, eta, nx, ny);
-      }
-      S.Fg[k] = fg;
-    }
-  }
-  __syncwarp();
-
-  // -- predictor finalisation, Newton, characteristic state (lane 0) ---------
   const double dt = p.dt, cc = p.c, om = p.omega;
   const double dxin = (double)cx2(qi), dyin = (double)cy2(qi);
-  if (live && lane == 0) {
-    double Fg[4] = {S.Fg[0], S.Fg[1], S.Fg[2], S.Fg[3]};
-    if (compat) {
-      const double tanx = -nyb, tany = nxb;
-      double dut0 = 0.0, dut1 = 0.0, wt_abs = 0.0;
-      if (kind == kNeumann) {
-        dut0 = S.dut[0];
-        dut1 = S.dut[1];
-        wt_abs = S.wt_abs;
-      } else {
-        if (mode == 6) {
-          double at = tmid;
-          if (pp[6] > 0.0 && at > pp[6]) at = pp[6];
-          dut0 = at * (pp[0] * tanx + pp[1] * tany);
-          dut1 = at * (pp[3] * tanx + pp[4] * tany);
-        }
-        wt_abs = 1.0;
-      }
-      if (wt_abs > 0.0) {
-        const double hn0 = Fg[0] * nxb + Fg[1] * nyb, hn1 = Fg[2] * nxb + Fg[3] * nyb;
-        const double gt0 = tanx + dut0, gt1 = tany + dut1;
-        Fg[0] = hn0 * nxb + gt0 * tanx;
-        Fg[1] = hn0 * nyb + gt0 * tany;
-        Fg[2] = hn1 * nxb + gt1 * tanx;
-        Fg[3] = hn1 * nyb + gt1 * tany;
-      }
-    }
-    double Fb[4] = {Fg[0], Fg[1], Fg[2], Fg[3]};
-    if (kind == kNeumann) solve_normal_image2(Fg, nxb, nyb, bv0, bv1, m, p.normal_solver, Fb);
-    const P2 Pb = piola2(Fb[0], Fb[1], Fb[2], Fb[3], m);
-    S.Pb[0] = Pb.a;
-    S.Pb[1] = Pb.b;
-    S.Pb[2] = Pb.c;
-    S.Pb[3] = Pb.d;
-    for (int k = 0; k < 4; ++k) S.Fb[k] = Fb[k];
-    double cv[6] = {U[n], U[(size_t)N + n], Fb[0], Fb[1], Fb[2], Fb[3]};
-    if (kind == kDirichlet) {
-      cv[0] = bv0;
-      cv[1] = bv1;
-    }
-    if (use_char) {
-      const double sx = -eta * dt * cc * (double)cx2(qo);
-      const double sy = -eta * dt * cc * (double)cy2(qo);
-      double dv[6];
-      for (int a = 0; a < 6; ++a) dv[a] = sx * S.ux[a] + sy * S.uy[a];
-      double sc = 1.0;
-      for (int g = 0; g < 10; ++g) {
-        const double t11 = cv[2] + sc * dv[2], t12 = cv[3] + sc * dv[3];
-        const double t21 = cv[4] + sc * dv[4], t22 = cv[5] + sc * dv[5];
-        if (t11 * t22 - t12 * t21 > 10.0 * m.jf) break;
-        sc = 0.5 * sc;
-      }
-      for (int a = 0; a < 6; ++a) cv[a] = cv[a] + sc * dv[a];
-    }
-    for (int a = 0; a < 6; ++a) S.cv[a] = cv[a];
-  }
-  __syncwarp();
 
-  // -- flux tangents of the characteristic closure --------------------------
-  if (use_char && lane < 2) {
-    double tmp[6];
-    if (lane == 0)
-      flux2_jvp(S.cv, S.ux, m, S.Ax, tmp);  // A_x U_x
-    else
-      flux2_jvp(S.cv, S.uy, m, tmp, S.Ay);  // A_y U_y
-  }
-  __syncwarp();
-  if (use_char && lane < 6) {
-    const int a = lane;
-    const double b = source_comp(a, p.source_mode, p.source, S.cv);
-    S.cw[a] = b - S.Ax[a] - S.Ay[a] + cc * (dxin * S.ux[a] + dyin * S.uy[a]);
-  }
-  __syncwarp();
-  const bool char_ok = use_char && S.cv[2] * S.cv[5] - S.cv[3] * S.cv[4] > m.jf;
-  if (char_ok && lane < 2) {
-    if (lane == 0) {
-      flux2_jvp(S.cv, S.cw, m, S.eqx, S.eqy);
+  // -- predictor finalisation and the normal-image solve ---------------------
+  double Fg[4] = {S.g[12], S.g[13], S.g[14], S.g[15]};
+  if (compat) {
+    const double tanx = -nyb, tany = nxb;
+    double dut0 = 0.0, dut1 = 0.0, wt_abs = 0.0;
+    if (kind == kNeumann) {
+      dut0 = S.dut[0];
+      dut1 = S.dut[1];
+      wt_abs = S.wt_abs;
     } else {
-      const P2 Pc = piola2(S.cv[2], S.cv[3], S.cv[4], S.cv[5], m);
-      S.Pc[0] = Pc.a;
-      S.Pc[1] = Pc.b;
-      S.Pc[2] = Pc.c;
-      S.Pc[3] = Pc.d;
+      if (mode == 6) {
+        double at = tmid;
+        if (pp[6] > 0.0 && at > pp[6]) at = pp[6];
+        dut0 = at * (pp[0] * tanx + pp[1] * tany);
+        dut1 = at * (pp[3] * tanx + pp[4] * tany);
+      }
+      wt_abs = 1.0;
+    }
+    if (wt_abs > 0.0) {
+      const double hn0 = Fg[0] * nxb + Fg[1] * nyb, hn1 = Fg[2] * nxb + Fg[3] * nyb;
+      const double gt0 = tanx + dut0, gt1 = tany + dut1;
+      Fg[0] = hn0 * nxb + gt0 * tanx;
+      Fg[1] = hn0 * nyb + gt0 * tany;
+      Fg[2] = hn1 * nxb + gt1 * tanx;
+      Fg[3] = hn1 * nyb + gt1 * tany;
     }
   }
-  __syncwarp();
+  double Fb[4] = {Fg[0], Fg[1], Fg[2], Fg[3]};
+  if (kind == kNeumann) solve_normal_image2(Fg, nxb, nyb, bv0, bv1, m, p.normal_solver, Fb);
+  const P2 Pb = piola2(Fb[0], Fb[1], Fb[2], Fb[3], m);
 
-  // -- one population row per lane -----------------------------------------
-  if (live && lane < 6) {
-    const int a = lane;
+  // -- characteristic state, flux tangents and equilibrium flux --------------
+  double cv[6] = {Un0, Un1, Fb[0], Fb[1], Fb[2], Fb[3]};
+  if (kind == kDirichlet) {
+    cv[0] = bv0;
+    cv[1] = bv1;
+  }
+  double cw[6], eqx[6], eqy[6];
+  P2 Pc{0.0, 0.0, 0.0, 0.0};
+  bool char_ok = false;
+  if (use_char) {
+    double ux[6], uy[6];
+#pragma unroll
+    for (int a = 0; a < 6; ++a) {
+      ux[a] = S.g[a];
+      uy[a] = S.g[6 + a];
+    }
+    const double sx = -eta * dt * cc * (double)cx2(L.qo);
+    const double sy = -eta * dt * cc * (double)cy2(L.qo);
+    double dv[6];
+    for (int a = 0; a < 6; ++a) dv[a] = sx * ux[a] + sy * uy[a];
+    double sc = 1.0;
+    for (int g = 0; g < 10; ++g) {
+      const double t11 = cv[2] + sc * dv[2], t12 = cv[3] + sc * dv[3];
+      const double t21 = cv[4] + sc * dv[4], t22 = cv[5] + sc * dv[5];
+      if (t11 * t22 - t12 * t21 > 10.0 * m.jf) break;
+      sc = 0.5 * sc;
+    }
+    for (int a = 0; a < 6; ++a) cv[a] = cv[a] + sc * dv[a];
+    double Ax[6], Ay[6], unused[6];
+    flux2_jvp(cv, ux, m, Ax, unused);  // A_x U_x
+    flux2_jvp(cv, uy, m, unused, Ay);  // A_y U_y
+#pragma unroll
+    for (int a = 0; a < 6; ++a) {
+      const double b = source_comp(a, p.source_mode, p.source, cv);
+      cw[a] = b - Ax[a] - Ay[a] + cc * (dxin * ux[a] + dyin * uy[a]);
+    }
+    char_ok = cv[2] * cv[5] - cv[3] * cv[4] > m.jf;
+    if (char_ok) {
+      flux2_jvp(cv, cw, m, eqx, eqy);
+      Pc = piola2(cv[2], cv[3], cv[4], cv[5], m);
+    } else {
+#pragma unroll
+      for (int a = 0; a < 6; ++a) link2_bfl_in(L, a, N, fpost, fused, scratch, partner, fo[a],
+                                               fi[a], upv[a]);
+    }
+  }
+
+  // -- the six population rows ----------------------------------------------
+#pragma unroll
+  for (int a = 0; a < 6; ++a) {
     double D = 1.0, Sv = 0.0;
     if (kind == kDirichlet) {
       switch (a) {
@@ -741,52 +796,53 @@ __device__ __forceinline__ void link2_group(
       }
     } else {
       switch (a) {
-        case 0: Sv = -(dxin * S.Pb[0] + dyin * S.Pb[1]) / cc; break;
-        case 1: Sv = -(dxin * S.Pb[2] + dyin * S.Pb[3]) / cc; break;
-        default: D = -1.0; Sv = 0.5 * S.Fb[a - 2]; break;
+        case 0: Sv = -(dxin * Pb.a + dyin * Pb.b) / cc; break;
+        case 1: Sv = -(dxin * Pb.c + dyin * Pb.d) / cc; break;
+        default: D = -1.0; Sv = 0.5 * Fb[a - 2]; break;
       }
     }
     double val;
     if (char_ok) {
-      const P2 Pc{S.Pc[0], S.Pc[1], S.Pc[2], S.Pc[3]};
-      const double jv = 0.25 * (S.cw[a] + (2.0 / cc) * (dxin * S.eqx[a] + dyin * S.eqy[a]));
-      const double ge = feq2(qi, a, S.cv, Pc, 2.0 / cc);
-      const double sa = source_comp(a, p.source_mode, p.source, S.cv);
+      const double jv = 0.25 * (cw[a] + (2.0 / cc) * (dxin * eqx[a] + dyin * eqy[a]));
+      const double ge = feq2(qi, a, cv, Pc, 2.0 / cc);
+      const double sa = source_comp(a, p.source_mode, p.source, cv);
       val = ge - dt / om * jv + dt * (1.0 / om - 0.5) * 0.25 * sa;
+    } else if (eta >= 0.5) {
+      const double al = 1.0 / (2.0 * eta);
+      val = al * (D * fo[a] + Sv) + (1.0 - al) * fi[a];
     } else {
-      double fo, fi, upv;
-      if (fused) {
-        fo = scratch[(size_t)ell * 6 + a];
-        fi = up_ok ? fpost[(size_t)(qi * 6 + a) * N + nu] : scratch[(size_t)partner[ell] * 6 + a];
-        upv = up_ok ? fpost[(size_t)(qo * 6 + a) * N + n] : fo;
-      } else {
-        fo = fpost[(size_t)(qo * 6 + a) * N + n];
-        fi = fpost[(size_t)(qi * 6 + a) * N + n];
-        upv = up_ok ? fpost[(size_t)(qo * 6 + a) * N + nu] : fo;
-      }
-      if (eta >= 0.5) {
-        const double al = 1.0 / (2.0 * eta);
-        val = al * (D * fo + Sv) + (1.0 - al) * fi;
-      } else {
-        val = D * (2.0 * eta * fo + (1.0 - 2.0 * eta) * upv) + Sv;
-      }
+      val = D * (2.0 * eta * fo[a] + (1.0 - 2.0 * eta) * upv[a]) + Sv;
     }
     fout[(size_t)(qi * 6 + a) * N + n] = val;
   }
 }
 
-__global__ void __launch_bounds__(128, 4)
+// Links [slot0, slot0 + 8) on the 64 threads of a block (every thread calls
+// it; contains block barriers).
+__device__ __forceinline__ void link2_block(
+    const Ctx2& c, LinkShared2* sh, int slot0, const double* __restrict__ fpost,
+    double* __restrict__ fout, const double* __restrict__ U, const double* __restrict__ u,
+    const double* clock, double t_host, double offset, int fused,
+    const double* __restrict__ scratch, const int32_t* __restrict__ partner) {
+  const int lane = threadIdx.x & (kLG - 1);
+  const int grp = threadIdx.x / kLG;
+  link2_gather(c, sh[grp], lane, slot0 + grp, U, u);
+  __syncthreads();
+  if (threadIdx.x < kLinksPerBlock2)
+    link2_finish(c, sh[threadIdx.x], slot0 + threadIdx.x, fpost, fout, U, clock, t_host, offset,
+                 fused, scratch, partner);
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kLinkThreads2, 4)
     k_links2g(Ctx2 c, const double* __restrict__ fpost, double* __restrict__ fout,
               const double* __restrict__ U, const double* __restrict__ u, const double* clock,
               double t_host, double offset, int fused, const double* __restrict__ scratch,
               const int32_t* __restrict__ partner, double* clock_next) {
-  __shared__ LinkShared2 sh[128 / kLG];
-  const int lane = threadIdx.x & (kLG - 1);
-  const int grp = threadIdx.x / kLG;
-  const int slot = blockIdx.x * (128 / kLG) + grp;
+  __shared__ LinkShared2 sh[kLinksPerBlock2];
   if (clock_next && blockIdx.x == 0 && threadIdx.x == 0) *clock_next = clock[0] + c.p.dt;
-  link2_group(c, sh[grp], lane, slot, fpost, fout, U, u, clock, t_host, offset, fused, scratch,
-              partner);
+  link2_block(c, sh, blockIdx.x * kLinksPerBlock2, fpost, fout, U, u, clock, t_host, offset,
+              fused, scratch, partner);
 }
 
 }  // namespace

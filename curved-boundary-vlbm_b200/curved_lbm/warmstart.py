@@ -343,6 +343,71 @@ def run_to_residual(solver, tol: float, *, check: int = 100, t_min: float = 0.0,
             "invalid": bool(solver.invalid_state())}
 
 
+def run_batch_to_residual(solvers: list, tol: float, *, check: int = 100, t_min=0.0,
+                          max_steps: int = 400_000) -> dict:
+    """`run_to_residual` for several independent solvers at once.
+
+    Each solver replays its own captured `check`-step graph on its own CUDA
+    stream, so the small per-solver launches of one round run side by side
+    on the SMs; the residual norms of every solver land in one device array
+    read back with a single copy per round.  A solver stops at the first
+    round its residual criterion holds, exactly as it would alone (same
+    graph, same steps), so each solver's steps and final state equal those of
+    a solo `run_to_residual`.  `t_min` is one time for all or one per
+    solver.  Returns per-solver steps / residual / invalid and the wall time
+    of the whole batch."""
+    import torch
+
+    if not solvers:
+        return {"wall_s": 0.0, "solvers": []}
+    dev = solvers[0]._tdev
+    if any(s._tdev != dev for s in solvers):
+        raise ValueError("run_batch_to_residual: every solver must live on the same device")
+    n = len(solvers)
+    t_mins = [float(t) for t in t_min] if isinstance(t_min, (list, tuple)) else [float(t_min)] * n
+    if len(t_mins) != n:
+        raise ValueError("run_batch_to_residual: one t_min per solver")
+    graphs = [s.capture_graph(check) for s in solvers]
+    streams = [torch.cuda.Stream(device=dev) for _ in range(n)]
+    prev = [s.u.clone() for s in solvers]
+    norms = torch.zeros((n, 2), dtype=torch.float64, device=dev)
+    steps0 = [s.steps for s in solvers]
+    res = [float("inf")] * n
+    active = list(range(n))
+    torch.cuda.synchronize(dev)
+    main = torch.cuda.current_stream(dev)
+    for st in streams:
+        st.wait_stream(main)
+    t0 = _time.perf_counter()
+    while active:
+        for i in active:
+            s = solvers[i]
+            with torch.cuda.stream(streams[i]):
+                graphs[i].launch()
+                torch.linalg.vector_norm(s.u - prev[i], out=norms[i, 0])
+                torch.linalg.vector_norm(s.u, out=norms[i, 1])
+                prev[i].copy_(s.u)
+        for i in active:
+            main.wait_stream(streams[i])
+        h = norms.cpu().numpy()
+        still = []
+        for i in active:
+            s = solvers[i]
+            du, nu = float(h[i, 0]), float(h[i, 1])
+            res[i] = du / (check * nu) if nu > 0 else float("inf")
+            done = s.time >= t_mins[i] and res[i] < tol
+            if not done and s.steps - steps0[i] < max_steps:
+                still.append(i)
+        active = still
+        for i in active:
+            streams[i].wait_stream(main)
+    torch.cuda.synchronize(dev)
+    wall = _time.perf_counter() - t0
+    return {"wall_s": wall,
+            "solvers": [{"steps": s.steps - s0, "residual": r, "invalid": bool(s.invalid_state())}
+                        for s, s0, r in zip(solvers, steps0, res)]}
+
+
 def warm_initialize(solver, pred: np.ndarray) -> bool:
     """Start `solver` from a predicted [12, G] (u, F - I) field; returns False
     (and leaves the solver undeformed) if the prediction has det F <= floor
@@ -366,20 +431,25 @@ def warm_initialize(solver, pred: np.ndarray) -> bool:
 
 
 def generate_equilibria(params: list[dict], nxy: int, tol: float, device="cuda:0",
-                        check: int = 100) -> list[dict]:
+                        check: int = 100, batch: int = 32) -> list[dict]:
     """Cold-start solves of the given tube cases to the residual tolerance:
-    the solver's own equilibria, the surrogate's training data."""
+    the solver's own equilibria, the surrogate's training data.  `batch`
+    solvers at a time run side by side (`run_batch_to_residual`)."""
     from . import workloads
 
     out = []
-    for prm in params:
-        s = make_tube_solver(prm, nxy, ramp_time=workloads.TUBE_RAMP_TIME, device=device)
-        info = run_to_residual(s, tol, check=check, t_min=workloads.TUBE_RAMP_TIME)
-        x, mask = tube_features(prm, nxy)
-        out.append({"params": prm, "x": x, "mask": mask,
-                    "target": solver_targets(s) - kinematic_guess(prm, nxy) * mask[None, :],
-                    "steps": info["steps"], "wall_s": info["wall_s"],
-                    "residual": info["residual"], "invalid": info["invalid"]})
+    for k in range(0, len(params), max(1, batch)):
+        group = params[k:k + max(1, batch)]
+        solvers = [make_tube_solver(prm, nxy, ramp_time=workloads.TUBE_RAMP_TIME, device=device)
+                   for prm in group]
+        info = run_batch_to_residual(solvers, tol, check=check, t_min=workloads.TUBE_RAMP_TIME)
+        for prm, s, si in zip(group, solvers, info["solvers"]):
+            x, mask = tube_features(prm, nxy)
+            out.append({"params": prm, "x": x, "mask": mask,
+                        "target": solver_targets(s) - kinematic_guess(prm, nxy) * mask[None, :],
+                        "steps": si["steps"], "wall_s": info["wall_s"] / len(group),
+                        "residual": si["residual"], "invalid": si["invalid"]})
+        del solvers
     return out
 
 
@@ -493,9 +563,16 @@ def _rel_err(a: np.ndarray, b: np.ndarray, mask: np.ndarray) -> float:
     return float(np.linalg.norm((a - b)[:, m]) / max(np.linalg.norm(b[:, m]), 1e-300))
 
 
+def _solver_state(s) -> np.ndarray:
+    import torch
+
+    torch.cuda.synchronize(s._tdev)
+    return torch.cat([s.u.reshape(-1), s.U.reshape(-1), s.f0.reshape(-1)]).cpu().numpy()
+
+
 def train_and_compare(*, nxy: int = 32, n_train: int = 64, n_test: int = 4, epochs: int = 200,
                       tol: float = 1e-8, seed: int = 7, device="cuda:0", modes=(4, 4, 8),
-                      lr: float = 2e-3) -> dict:
+                      lr: float = 2e-3, gen_batch: int = 32) -> dict:
     """Generate solver equilibria, train the surrogate, then compare warm and
     cold starts on held-out cases.
 
@@ -503,6 +580,11 @@ def train_and_compare(*, nxy: int = 32, n_train: int = 64, n_test: int = 4, epoc
     TUBE_RAMP_TIME) and the warm start (surrogate prediction, end load at
     once) both run to `tol`; the cold run then continues to tol/100, whose
     field is the converged reference both final errors are measured against.
+
+    Wall times: cold and warm plain (one solve after another, the way the
+    reference runs its cases) and batched (every held-out case side by side,
+    `run_batch_to_residual`).  The batched runs are checked to reach the
+    plain runs' step counts and states bit for bit.
     """
     from . import replicas, workloads
 
@@ -515,7 +597,8 @@ def train_and_compare(*, nxy: int = 32, n_train: int = 64, n_test: int = 4, epoc
     params = workloads.tube_params(n_train + n_test, seed, min_wall=4.0 * dx)
     t0 = _time.perf_counter()
     # under a process group every rank solves its own share of the cases
-    train = generate_equilibria(replicas.deal(params[:n_train], rank, world), nxy, tol, device)
+    train = generate_equilibria(replicas.deal(params[:n_train], rank, world), nxy, tol, device,
+                                batch=gen_batch)
     gen_s = _time.perf_counter() - t0
     sur = Surrogate(nxy, modes=modes, device=device, seed=seed)
     t0 = _time.perf_counter()
@@ -525,22 +608,29 @@ def train_and_compare(*, nxy: int = 32, n_train: int = 64, n_test: int = 4, epoc
         [gen_s, fit_s], [sum(d["steps"] for d in train), len(train)], device=device)
     if rank != 0:  # the held-out comparison runs on one GPU
         return {"rank": rank, "n_train_local": len(train)}
+    ramp = workloads.TUBE_RAMP_TIME
+    test = params[n_train:]
+    feats = [tube_features(prm, nxy) for prm in test]
+    preds = [p + kinematic_guess(prm, nxy) * m[None, :]
+             for prm, p, (_, m) in zip(test, sur.predict([x for x, _ in feats]), feats)]
+
+    def warm_solver(prm, pred):
+        s = make_tube_solver(prm, nxy, ramp_time=0.0, device=device)
+        if warm_initialize(s, pred):
+            return s, True, 0.0
+        # fallback: the plain cold start
+        return make_tube_solver(prm, nxy, ramp_time=ramp, device=device), False, ramp
+
     cases = []
-    for prm in params[n_train:]:
-        x, mask = tube_features(prm, nxy)
-        pred = sur.predict([x])[0] + kinematic_guess(prm, nxy) * mask[None, :]
-        cold = make_tube_solver(prm, nxy, ramp_time=workloads.TUBE_RAMP_TIME, device=device)
-        ci = run_to_residual(cold, tol, t_min=workloads.TUBE_RAMP_TIME)
+    for prm, pred, (x, mask) in zip(test, preds, feats):
+        cold = make_tube_solver(prm, nxy, ramp_time=ramp, device=device)
+        ci = run_to_residual(cold, tol, t_min=ramp)
         u_cold = solver_targets(cold)
+        st_cold = _solver_state(cold)
         run_to_residual(cold, tol / 100.0)
         ref = solver_targets(cold)
-        warm = make_tube_solver(prm, nxy, ramp_time=0.0, device=device)
-        ok = warm_initialize(warm, pred)
-        if ok:
-            wi = run_to_residual(warm, tol)
-        else:  # fallback: the plain cold start
-            warm = make_tube_solver(prm, nxy, ramp_time=workloads.TUBE_RAMP_TIME, device=device)
-            wi = run_to_residual(warm, tol, t_min=workloads.TUBE_RAMP_TIME)
+        warm, ok, t_min = warm_solver(prm, pred)
+        wi = run_to_residual(warm, tol, t_min=t_min)
         u_warm = solver_targets(warm)
         cases.append({"params": prm, "warm_ok": ok, "cold_steps": ci["steps"],
                       "warm_steps": wi["steps"], "cold_wall_s": ci["wall_s"],
@@ -548,14 +638,34 @@ def train_and_compare(*, nxy: int = 32, n_train: int = 64, n_test: int = 4, epoc
                       "warm_err": _rel_err(u_warm, ref, mask),
                       "prediction_err": _rel_err(pred, ref, mask),
                       "guess_err": _rel_err(kinematic_guess(prm, nxy) * mask[None, :], ref, mask),
-                      "warm_invalid": wi["invalid"], "cold_invalid": ci["invalid"]})
+                      "warm_invalid": wi["invalid"], "cold_invalid": ci["invalid"],
+                      "_cold_state": st_cold, "_warm_state": _solver_state(warm)})
+        del cold, warm
+    # the same solves again, every case side by side
+    colds = [make_tube_solver(prm, nxy, ramp_time=ramp, device=device) for prm in test]
+    cb = run_batch_to_residual(colds, tol, t_min=ramp)
+    cold_same = all(c["cold_steps"] == b["steps"] and np.array_equal(c["_cold_state"],
+                                                                      _solver_state(s))
+                    for c, b, s in zip(cases, cb["solvers"], colds))
+    del colds
+    built = [warm_solver(prm, pred) for prm, pred in zip(test, preds)]
+    wb = run_batch_to_residual([s for s, _, _ in built], tol, t_min=[t for _, _, t in built])
+    warm_same = all(c["warm_steps"] == b["steps"] and np.array_equal(c["_warm_state"],
+                                                                      _solver_state(s))
+                    for c, b, (s, _, _) in zip(cases, wb["solvers"], built))
+    del built
+    for c in cases:
+        del c["_cold_state"], c["_warm_state"]
     cold_w = sum(c["cold_wall_s"] for c in cases)
     warm_w = sum(c["warm_wall_s"] for c in cases)
-    return {"nxy": nxy, "dx": dx, "min_wall": 4.0 * dx, "n_train": n_train, "n_test": n_test, "epochs": epochs, "tol": tol,
-            "modes": list(modes), "generate_s": gen_s, "fit_s": fit_s,
-            "train_loss_first": hist[0], "train_loss_last": hist[-1],
+    return {"nxy": nxy, "dx": dx, "min_wall": 4.0 * dx, "n_train": n_train, "n_test": n_test,
+            "epochs": epochs, "tol": tol, "modes": list(modes), "generate_s": gen_s,
+            "fit_s": fit_s, "train_loss_first": hist[0], "train_loss_last": hist[-1],
             "train_steps_mean": steps_sum / max(n_done, 1), "ranks": world,
             "cases": cases, "cold_wall_s": cold_w, "warm_wall_s": warm_w,
+            "cold_batched_wall_s": cb["wall_s"], "warm_batched_wall_s": wb["wall_s"],
+            "batched_equals_plain": bool(cold_same and warm_same),
             "speedup_wall": cold_w / max(warm_w, 1e-12),
+            "speedup_batched": cold_w / max(wb["wall_s"], 1e-12),
             "speedup_steps": sum(c["cold_steps"] for c in cases)
             / max(sum(c["warm_steps"] for c in cases), 1)}

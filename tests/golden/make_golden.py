@@ -208,6 +208,38 @@ CASES_2D = {
     ),
 }
 
+
+def _recon_case(recon: str, *, poisson=0.25, solver_extra=None, steps=10):
+    """Traction (outer wall, radial pressure ramp) and clamped inner wall on a
+    perturbed annulus, with the given boundary reconstruction."""
+    solver = dict(lattice_speed=10.0, collision_omega=1.8, boundary_reconstruction=recon,
+                  source_mode="damping", damping_gamma=5.0)
+    solver.update(solver_extra or {})
+    return dict(
+        geometry=dict(kind="annulus", nx=24, ny=24, length_x=1.1, length_y=1.1, center_x=0.55,
+                      center_y=0.55, inner_radius=0.24, outer_radius=0.49),
+        material=dict(model="neo_hooke", poisson=poisson, mu=1.0),
+        boundary=dict(kind="neumann", value_mode=103, params=[0.04, 0.03, 0.0],
+                      id_kinds={"1": "neumann", "2": "dirichlet"},
+                      id_value_modes={"1": 103, "2": 0},
+                      id_params={"1": [0.04, 0.03, 0.0], "2": []}),
+        solver=solver,
+        init=dict(kind="identity_perturbed", init_order=2),
+        steps=steps,
+    )
+
+
+# The remaining supported reconstructions on a traction case: the least-squares
+# BFL predictor, the compatible BFL predictor with a traction wall (tangential
+# image from the u stencil), the second-order characteristic closure (local_f
+# plus the compatible predictor) and the single-history BFL of local_f.
+CASES_2D.update({
+    "g2_lsq_bfl": _recon_case("lsq_bfl"),
+    "g2_compat_bfl_traction": _recon_case("compat_bfl", poisson=0.3),
+    "g2_local_char2": _recon_case("local_char2"),
+    "g2_local_f_bfl": _recon_case("local_f_bfl", poisson=0.2),
+})
+
 CASES_3D = {
     # Inner clamp, outer sine^2 normal traction, production local_f closure.
     "g3_shell_localf": dict(

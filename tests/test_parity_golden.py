@@ -26,6 +26,7 @@ GOLD3 = ["g3_shell_localf", "g3_shell_bfl_fd", "g3_shell_compat"]
 GOLD2 += [f"g2_mat_{m}" for m in ("svk", "log_neo_hooke", "mooney_rivlin", "yeoh", "gent",
                                    "sugiyama_svk")]
 GOLD2 += ["g2_mrt_ghost", "g2_kinetic_filter", "g2_mrt_filter"]
+GOLD2 += ["g2_lsq_bfl", "g2_compat_bfl_traction", "g2_local_char2", "g2_local_f_bfl"]
 GOLD3 += ["g3_mixed_localf", "g3_mixed_fd", "g3_mixed_energy"]
 GOLD3 += [f"g3_mat_{m}" for m in ("svk", "log_neo_hooke", "mooney_rivlin", "yeoh", "gent",
                                    "sph_neo_hooke")]

@@ -117,10 +117,35 @@ def test_native_gradients_match_oracle():
 
 
 @pytest.mark.gpu
+def test_batched_solves_equal_solo_solves():
+    """Solvers stepped side by side on their own streams stop at the same
+    step and hold the same state, bit for bit, as when each runs alone."""
+    from curved_lbm import warmstart as ws
+    from curved_lbm import workloads
+
+    nxy = 24
+    dx = workloads.tube_lattice(nxy)[3]
+    params = workloads.tube_params(3, 11, min_wall=4.0 * dx)
+    ramp = workloads.TUBE_RAMP_TIME
+    solo = []
+    for prm in params:
+        s = ws.make_tube_solver(prm, nxy, ramp_time=ramp)
+        info = ws.run_to_residual(s, 1e-6, t_min=ramp)
+        solo.append((info["steps"], ws._solver_state(s)))
+    batch = [ws.make_tube_solver(prm, nxy, ramp_time=ramp) for prm in params]
+    rep = ws.run_batch_to_residual(batch, 1e-6, t_min=ramp)
+    for (steps, state), s, info in zip(solo, batch, rep["solvers"]):
+        assert info["steps"] == steps
+        assert not info["invalid"]
+        assert np.array_equal(ws._solver_state(s), state)
+
+
+@pytest.mark.gpu
 def test_trained_surrogate_beats_cold_start():
     from curved_lbm import warmstart as ws
 
     rep = ws.train_and_compare(nxy=24, n_train=12, n_test=2, epochs=60, tol=1e-8, seed=3)
+    assert rep["batched_equals_plain"]
     for case in rep["cases"]:
         assert case["warm_ok"], case
         assert case["warm_steps"] < case["cold_steps"], case
