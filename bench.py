@@ -208,6 +208,7 @@ def batch_bench(args, dev):
     params = replicas.deal(workloads.superellipse_params(n_inst), rank, world)
     geoms = workloads.superellipse_geometries(
         params, processes=max(1, (os.cpu_count() or 1) // world))
+    geom_s = time.perf_counter() - t0
     solvers = workloads.superellipse_solvers(params, geoms, device=str(dev))
     setup_s = time.perf_counter() - t0
     batch = BatchedCurvedBoundaryLBM2D(solvers)
@@ -261,7 +262,7 @@ def batch_bench(args, dev):
                    "persistent_node_grid": ng, "work_items": nw,
                    "residual": "|u-u_prev|_2/(100 |u|_2) over active nodes, checked every 100 steps "
                                f"after t >= {workloads.SUPERELLIPSE_RAMP_TIME}",
-                   "tol": args.tol, "host_setup_s": round(setup_s, 1),
+                   "tol": args.tol, "host_setup_s": round(setup_s, 1), "host_geometry_s": round(geom_s, 1),
                    "l2": "working set (%.1f GB of populations) far above L2"
                          % (sum_n2 * 24 * 8 * 2 / 1e9)},
         "time_to_residual_s": {"device": device_ms * 1e-3, "wall": wall_s},

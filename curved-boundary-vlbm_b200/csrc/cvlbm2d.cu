@@ -1017,3 +1017,8 @@ extern "C" int cvlbm2d_run_static_scratch(const cvlbm2d_problem* p, cvlbm2d_fiel
 // Batched step of many independent 2-D problems (see cvlbm2d_batch.cuh).
 // ---------------------------------------------------------------------------
 #include "cvlbm2d_batch.cuh"
+
+// ---------------------------------------------------------------------------
+// Initial populations on the device (see cvlbm2d_init.cuh).
+// ---------------------------------------------------------------------------
+#include "cvlbm2d_init.cuh"

@@ -119,6 +119,8 @@ EXPORTED = (
     "cvlbm2d_refresh",
     "cvlbm2d_stress",
     "cvlbm2d_kinetic_filter",
+    "cvlbm2d_init_populations",
+    "cvlbm2d_init_work_bytes",
     "cvlbm3d_run",
     "cvlbm3d_apply_boundary",
     "cvlbm3d_refresh",
@@ -181,6 +183,8 @@ def load(require_cuda: bool = True):
         "cvlbm2d_refresh": (i32, [P2, F2, pI]),
         "cvlbm2d_stress": (i32, [P2, F2, pI]),
         "cvlbm2d_kinetic_filter": (i32, [P2, F2, pI]),
+        "cvlbm2d_init_populations": (i32, [P2, pI, i32, pI, pI, pI, pI]),
+        "cvlbm2d_init_work_bytes": (i64, [i32, i32]),
         "cvlbm3d_run": (i32, [P3, F3, f64, i64, i32, i32, pI]),
         "cvlbm3d_apply_boundary": (i32, [P3, F3, f64, i32, pI]),
         "cvlbm3d_refresh": (i32, [P3, F3, pI]),

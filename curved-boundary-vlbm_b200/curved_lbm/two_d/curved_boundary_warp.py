@@ -666,7 +666,11 @@ class WarpCurvedBoundaryLBM2D:
     def initialize_from_numpy(self, *, U: np.ndarray, displacement: np.ndarray | None = None,
                               init_order: int = 1, apply_initial_boundaries: bool = True,
                               initial_boundary_time: float = 0.0) -> None:
-        """Host initial populations, upload, in-place boundary pass (reference :3855-3954)."""
+        """Initial populations, u*, in-place boundary pass (reference :3855-3954).
+
+        The populations are formed on the device by the operations of the
+        reference's host NumPy code; where that code raises or retries (a
+        flux evaluation with J <= 0), it runs on the host instead."""
         import torch
 
         U = np.asarray(U, dtype=np.float64)
@@ -676,31 +680,24 @@ class WarpCurvedBoundaryLBM2D:
                 else np.asarray(displacement, dtype=np.float64))
         if disp.shape != (2, self.nx, self.ny):
             raise ValueError(f"displacement must have shape {(2, self.nx, self.ny)}")
-        if init_order == 1:
-            f = _equilibrium_np(U, self.material, self.lattice_speed)
-            src = _source_np(U, self.source_mode, self.source_params)
-            f -= (0.5 * self.dt / float(Q)) * src[None, ...]
-        elif init_order == 2:
-            f = _second_order_populations_np(
-                U, self.material, self.lattice_speed, dx=self.dx, dy=self.dy, dt=self.dt,
-                periodic_x=False, periodic_y=False, source_mode=self.source_mode,
-                source_params=self.source_params)
-        elif init_order == 3:
-            f = _second_order_populations_masked_np(
-                U, self.active_np.astype(bool), self.material, self.lattice_speed, dx=self.dx,
-                dy=self.dy, dt=self.dt, periodic_x=False, periodic_y=False,
-                source_mode=self.source_mode, source_params=self.source_params)
-        else:
+        if init_order not in (1, 2, 3):
             raise ValueError("init_order must be 1, 2, or 3")
+        # formed in fpost (zeroed below) so that f0 is untouched if the host
+        # code raises
+        if self._device_initial_populations(U, init_order, self.fpost):
+            self.f0.copy_(self.fpost)
+        else:
+            # the host code raises FloatingPointError (or retries a flux
+            # tangent with a smaller step) where the device kernels flagged
+            f = self._host_initial_populations(U, init_order)
+            self.f0.copy_(torch.as_tensor(np.ascontiguousarray(f.reshape((FQ, self.nx, self.ny))),
+                                          device=self._tdev))
         inactive = self.active_np == 0
-        f[:, :, inactive] = 0.0
         dm = np.array(disp, dtype=np.float64, copy=True)
         dm[:, inactive] = 0.0
         us0 = dm - 0.5 * self.dt * U[:2]
         us0[:, inactive] = 0.0
         dev = self._tdev
-        self.f0.copy_(torch.as_tensor(np.ascontiguousarray(f.reshape((FQ, self.nx, self.ny))),
-                                      device=dev))
         self.f1.zero_()
         self.fpost.zero_()
         self.u_star.copy_(torch.as_tensor(np.ascontiguousarray(us0), device=dev))
@@ -715,6 +712,44 @@ class WarpCurvedBoundaryLBM2D:
                                                                self._stream()),
                               "cvlbm2d_kinetic_filter")
             self.refresh_current()
+
+    def _host_initial_populations(self, U: np.ndarray, init_order: int) -> np.ndarray:
+        """Initial populations [4, 6, nx, ny] by the reference's host NumPy
+        (:3875-3890), zero at inactive nodes."""
+        if init_order == 1:
+            f = _equilibrium_np(U, self.material, self.lattice_speed)
+            src = _source_np(U, self.source_mode, self.source_params)
+            f -= (0.5 * self.dt / float(Q)) * src[None, ...]
+        elif init_order == 2:
+            f = _second_order_populations_np(
+                U, self.material, self.lattice_speed, dx=self.dx, dy=self.dy, dt=self.dt,
+                periodic_x=False, periodic_y=False, source_mode=self.source_mode,
+                source_params=self.source_params)
+        else:
+            f = _second_order_populations_masked_np(
+                U, self.active_np.astype(bool), self.material, self.lattice_speed, dx=self.dx,
+                dy=self.dy, dt=self.dt, periodic_x=False, periodic_y=False,
+                source_mode=self.source_mode, source_params=self.source_params)
+        f[:, :, self.active_np == 0] = 0.0
+        return f
+
+    def _device_initial_populations(self, U: np.ndarray, init_order: int, out) -> bool:
+        """`out` ([24, nx, ny] device tensor) from U by the library's init
+        kernels (cvlbm2d_init_populations,
+        the host NumPy's operations on the device); False where the host code
+        has to run instead (a flux evaluation with J <= 0 or past the Gent
+        chain limit, where it raises or retries with a smaller step)."""
+        import torch
+
+        dev = self._tdev
+        Ud = torch.as_tensor(np.ascontiguousarray(U.reshape(NCOMP, -1)), device=dev)
+        nbytes = int(self._lib.cvlbm2d_init_work_bytes(self.nx, self.ny))
+        work = torch.empty(nbytes // 8 + 1, dtype=torch.float64, device=dev)
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        _native.check(self._lib.cvlbm2d_init_populations(
+            self._problem, _native.ptr(Ud), int(init_order), _native.ptr(out),
+            _native.ptr(work), _native.ptr(status), self._stream()), "cvlbm2d_init_populations")
+        return int(status.item()) == 0
 
     # -- boundary ----------------------------------------------------------
     def enable_dynamic_link_traction(self, enabled: bool = True) -> None:

@@ -186,6 +186,22 @@ int cvlbm2d_run_static_scratch(const cvlbm2d_problem *p, cvlbm2d_fields *f, doub
  * applies it after every step by itself. */
 int cvlbm2d_kinetic_filter(const cvlbm2d_problem *p, cvlbm2d_fields *f, void *stream);
 
+/* Initial populations of initialize_from_numpy, computed on the device
+ * instead of by the reference's host NumPy (two_d/curved_boundary_warp.py:
+ * 3855-3900 calling two_d/vector_nonlinear_elastic_warp.py:595-847): order 1
+ * feq(U) - (dt/8) B(U); order 2 the second-order start from centred
+ * differences of U; order 3 the same from active neighbours only.  U: device
+ * [6][nx*ny], full lattice; f0: device [24][nx*ny] out, zero at inactive
+ * nodes; work: device scratch of cvlbm2d_init_work_bytes(nx, ny) bytes.
+ * *status (device int32) is set to 1 where the reference's host code raises
+ * FloatingPointError (J <= 0 or the Gent chain limit in some flux
+ * evaluation; the host code then retries with a smaller difference step) or
+ * where the kernels' Jacobian floor would change a value: f0 is then not
+ * the reference's and the caller repeats the host computation. */
+int cvlbm2d_init_populations(const cvlbm2d_problem *p, const double *U, int32_t order,
+                             double *f0, void *work, int32_t *status, void *stream);
+int64_t cvlbm2d_init_work_bytes(int32_t nx, int32_t ny);
+
 /* Cut-link reconstruction at time t, fpost -> f1, or in place on f0 through a
  * frozen copy in fpost.  Replaces apply_boundary_reconstruction
  * (two_d/curved_boundary_warp.py:4020-4035). */

@@ -1,0 +1,106 @@
+"""Initial populations on the device against the reference's host NumPy.
+
+initialize_from_numpy forms the populations with cvlbm2d_init_populations
+(order 1: feq - (dt/8) B; order 2: the second-order start from centred
+differences; order 3: from active neighbours only).  The kernels keep the
+NumPy code's operation order, so for the neo-Hooke and SVK laws the
+populations equal the host's bit for bit; laws with log/exp differ by the
+two libm's rounding (FIELD_RTOL).  Where the host code raises (a flux
+evaluation with J <= 0) the device flags it and the host code runs, raising
+the reference's FloatingPointError.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+# log/exp laws: a few ulps of the largest population
+FIELD_RTOL = 1e-13
+
+
+def _solver(n=48, material="neo_hooke", source="damping"):
+    from curved_lbm import workloads
+    from curved_lbm.two_d import curved_boundary_warp as c2
+
+    geom, mat, spec, kw = workloads.annulus(n)
+    if material != "neo_hooke":
+        mat = c2.WarpHyperelasticMaterial(model=material, lam=1.0, mu=1.0, param0=0.6,
+                                          param1=0.3, param2=0.05)
+    kw = dict(kw)
+    if source == "constant":
+        kw.update(source_mode="constant", source_vector=(0.001, -0.002, 0.0005, 0.0, 0.0, -0.0005))
+        kw.pop("damping_gamma", None)
+    return c2.WarpCurvedBoundaryLBM2D(geom, material=mat, boundary=spec, device="cuda:0", **kw)
+
+
+def _perturbed_state(n, seed=0):
+    """A smooth deformed state with J > 0 everywhere (inactive nodes too)."""
+    rng = np.random.default_rng(seed)
+    x = (np.arange(n) + 0.5) / n
+    X, Y = np.meshgrid(x, x, indexing="ij")
+    U = np.zeros((6, n, n))
+    a = rng.uniform(0.02, 0.05, 6)
+    U[0] = a[0] * np.sin(2 * np.pi * X) * np.cos(np.pi * Y)
+    U[1] = a[1] * np.cos(3 * X + Y)
+    U[2] = 1.0 + a[2] * np.sin(5 * Y)
+    U[3] = a[3] * X * Y
+    U[4] = -a[4] * np.cos(2 * X)
+    U[5] = 1.0 + a[5] * X
+    return U
+
+
+def _device(s, U, order):
+    import torch
+
+    out = torch.empty_like(s.f0)
+    assert s._device_initial_populations(U, order, out)
+    return out.cpu().numpy().reshape(4, 6, s.nx, s.ny)
+
+
+@pytest.mark.parametrize("order", [1, 2, 3])
+@pytest.mark.parametrize("source", ["damping", "constant"])
+def test_device_init_equals_host_bitwise(order, source):
+    s = _solver(source=source)
+    U = _perturbed_state(s.nx)
+    np.testing.assert_array_equal(_device(s, U, order), s._host_initial_populations(U, order))
+
+
+@pytest.mark.parametrize("material", ["svk", "yeoh", "log_neo_hooke"])
+def test_device_init_other_laws(material):
+    s = _solver(material=material)
+    U = _perturbed_state(s.nx, seed=1)
+    for order in (1, 2, 3):
+        dev, host = _device(s, U, order), s._host_initial_populations(U, order)
+        if material == "svk":
+            np.testing.assert_array_equal(dev, host)
+        else:
+            assert np.max(np.abs(dev - host)) <= FIELD_RTOL * np.max(np.abs(host)), (material, order)
+
+
+def test_device_init_defers_to_host_where_it_raises():
+    s = _solver()
+    U = _perturbed_state(s.nx)
+    U[2, 0, 0] = -0.5  # J < 0 at an (inactive) corner node
+    import torch
+
+    out = torch.empty_like(s.f0)
+    assert not s._device_initial_populations(U, 1, out)
+    before = s.f0.clone()
+    with pytest.raises(FloatingPointError):
+        s.initialize_from_numpy(U=U, init_order=1)
+    assert torch.equal(s.f0, before)
+
+
+def test_initialize_from_numpy_uses_device_path():
+    """The populations after initialize_from_numpy (no boundary pass) are the
+    host NumPy's, for the bench's annulus start."""
+    from curved_lbm import workloads
+
+    s = _solver(n=64)
+    U, disp = workloads.annulus_initial_state(64)
+    s.initialize_from_numpy(U=U, displacement=disp, init_order=2, apply_initial_boundaries=False)
+    f = s.f0.cpu().numpy().reshape(4, 6, 64, 64)
+    np.testing.assert_array_equal(f, s._host_initial_populations(U, 2))
