@@ -20,7 +20,8 @@ INCLUDE = REPO_ROOT / "include"
 LIB_DIR = PKG_DIR / "_lib"
 LIB_PATH = LIB_DIR / "libcvlbm.so"
 
-SOURCES = ("cvlbm_api.cu", "cvlbm2d.cu", "cvlbm3d.cu", "cvlbm3d_geom.cu", "cvlbm_gemm.cu",
+SOURCES = ("cvlbm_api.cu", "cvlbm2d.cu", "cvlbm3d.cu", "cvlbm3d_geom.cu", "cvlbm_summary.cu",
+           "cvlbm_gemm.cu",
            "cvlbm_fno.cu")
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = [

@@ -121,6 +121,8 @@ EXPORTED = (
     "cvlbm2d_kinetic_filter",
     "cvlbm2d_init_populations",
     "cvlbm2d_init_work_bytes",
+    "cvlbm_field_summary",
+    "cvlbm_field_summary_work_bytes",
     "cvlbm3d_run",
     "cvlbm3d_apply_boundary",
     "cvlbm3d_refresh",
@@ -185,6 +187,8 @@ def load(require_cuda: bool = True):
         "cvlbm2d_kinetic_filter": (i32, [P2, F2, pI]),
         "cvlbm2d_init_populations": (i32, [P2, pI, i32, pI, pI, pI, pI]),
         "cvlbm2d_init_work_bytes": (i64, [i32, i32]),
+        "cvlbm_field_summary": (i32, [i32, i64, pI, pI, pI, pI, C.POINTER(f64), pI]),
+        "cvlbm_field_summary_work_bytes": (i64, []),
         "cvlbm3d_run": (i32, [P3, F3, f64, i64, i32, i32, pI]),
         "cvlbm3d_apply_boundary": (i32, [P3, F3, f64, i32, pI]),
         "cvlbm3d_refresh": (i32, [P3, F3, pI]),
@@ -306,3 +310,17 @@ class KernelTimer:
 
 def launch_count() -> int:
     return int(load().cvlbm_launch_count())
+
+
+def field_summary(lib, dim: int, n: int, U, u, active, device) -> dict:
+    """Device reductions of summary(): max |u|, max |v|, min J, max J, finite."""
+    import torch
+
+    work = torch.empty(int(lib.cvlbm_field_summary_work_bytes()) // 8 + 1, dtype=torch.float64,
+                       device=device)
+    out = (f64 * 6)()
+    check(lib.cvlbm_field_summary(int(dim), int(n), ptr(U), ptr(u), ptr(active), ptr(work), out,
+                                  stream_ptr(device)), "cvlbm_field_summary")
+    return {"max_abs_u": out[0], "max_abs_v": out[1], "min_J": out[2], "max_J": out[3],
+            "finite": bool(out[4] != 0.0), "count": int(out[5])}
+

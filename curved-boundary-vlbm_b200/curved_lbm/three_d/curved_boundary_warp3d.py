@@ -866,10 +866,11 @@ class WarpSparseCurvedBoundaryLBM3D:
                 or not np.all(_det3_np(F) > 0))
 
     def summary(self):
+        """The field reductions (max |u|, max |v|, min / max J, finite) run on
+        the device (cvlbm_field_summary)."""
         self.refresh_current()
-        U = self._host(self.U)
-        u = self._host(self.u)
-        J = _det3_np(U[3:12].reshape(3, 3, self.n_active))
+        red = _native.field_summary(self._lib, 3, self.n_active, self.U, self.u, None,
+                                    self._tdev)
         mem = self.memory_estimate_bytes()
         drad = int(self.local_displacement_sweeps) if self.local_displacement_interval > 0 else 0
         crad = drad + 2 if self.local_compatibility_interval > 0 else drad
@@ -911,12 +912,11 @@ class WarpSparseCurvedBoundaryLBM3D:
                 "composed_compatibility_radius": crad,
             },
             "memory_estimate_MiB": {k: float(v / 1024**2) for k, v in mem.items()},
-            "max_abs_u": float(np.max(np.sqrt(np.sum(u * u, axis=0)))) if self.n_active else 0.0,
-            "max_abs_v": float(np.max(np.sqrt(U[0] * U[0] + U[1] * U[1] + U[2] * U[2])))
-            if self.n_active else 0.0,
-            "min_J": float(np.min(J)) if self.n_active else 0.0,
-            "max_J": float(np.max(J)) if self.n_active else 0.0,
-            "finite": bool(np.isfinite(U).all() and np.all(J > 0)) if self.n_active else False,
+            "max_abs_u": float(red["max_abs_u"]) if self.n_active else 0.0,
+            "max_abs_v": float(red["max_abs_v"]) if self.n_active else 0.0,
+            "min_J": float(red["min_J"]) if self.n_active else 0.0,
+            "max_J": float(red["max_J"]) if self.n_active else 0.0,
+            "finite": red["finite"] if self.n_active else False,
         }
 
     # -- exact checkpoint / restart (no counterpart in the reference) --------

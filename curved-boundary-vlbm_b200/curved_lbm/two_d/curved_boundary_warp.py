@@ -915,21 +915,20 @@ class WarpCurvedBoundaryLBM2D:
         return self.active_np.astype(bool)
 
     def summary(self) -> dict:
-        """Reference :4343-4415."""
+        """Reference :4343-4415.  The field reductions (max |u|, max |v|,
+        min / max J, finite) run on the device (cvlbm_field_summary)."""
         self.refresh_current()
-        u = self.displacement()
-        U = self.system_state()
-        J = self.deformation_jacobian()
-        mask = self.active_mask()
+        red = _native.field_summary(self._lib, 2, self.nx * self.ny, self.U, self.u,
+                                    self._tables["active"], self._tdev)
+        anym = red["count"] > 0
         drad = self.local_displacement_sweeps if self.local_displacement_interval > 0 else 0
         crad = drad + 2 if self.local_compatibility_interval > 0 else drad
-        anym = bool(np.any(mask))
         return {
             "device": self.device, "geometry": self.geometry.label,
             "boundary_label": self.boundary.label, "boundary_kind": self.boundary.kind,
             "boundary_mode": int(self.boundary.value_mode), "model": self.material.model,
             "lambda": float(self.material.lam), "mu": float(self.material.mu), "nx": self.nx,
-            "ny": self.ny, "n_active": int(np.count_nonzero(mask)),
+            "ny": self.ny, "n_active": int(red["count"]),
             "n_cut_links": self.geometry.n_links, "steps": self.steps, "time": float(self.time),
             "dx": float(self.dx), "dt": float(self.dt), "lattice_speed": float(self.lattice_speed),
             "collision_omega": float(self.collision_omega), "collision_model": self.collision_model,
@@ -953,14 +952,11 @@ class WarpCurvedBoundaryLBM2D:
             "local_composed_compatibility_radius": crad,
             "linearized_stability_ratio": float(
                 self.material.linearized_stability_ratio(self.lattice_speed)),
-            "max_abs_u": float(np.max(np.sqrt(np.sum(u[:, mask] * u[:, mask], axis=0))))
-            if anym else 0.0,
-            "max_abs_v": float(np.max(np.sqrt(U[0, mask] * U[0, mask] + U[1, mask] * U[1, mask])))
-            if anym else 0.0,
-            "min_J": float(np.min(J[mask])) if anym else 0.0,
-            "max_J": float(np.max(J[mask])) if anym else 0.0,
-            "finite": bool(np.isfinite(u[:, mask]).all() and np.isfinite(U[:, mask]).all()
-                           and np.all(J[mask] > 0.0)) if anym else False,
+            "max_abs_u": float(red["max_abs_u"]) if anym else 0.0,
+            "max_abs_v": float(red["max_abs_v"]) if anym else 0.0,
+            "min_J": float(red["min_J"]) if anym else 0.0,
+            "max_J": float(red["max_J"]) if anym else 0.0,
+            "finite": red["finite"] if anym else False,
         }
 
     # -- exact checkpoint / restart (no counterpart in the reference) --------

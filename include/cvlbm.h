@@ -202,6 +202,19 @@ int cvlbm2d_init_populations(const cvlbm2d_problem *p, const double *U, int32_t 
                              double *f0, void *work, int32_t *status, void *stream);
 int64_t cvlbm2d_init_work_bytes(int32_t nx, int32_t ny);
 
+/* Field reductions of summary() (two_d/curved_boundary_warp.py:4343-4415 and
+ * the 3-D class's summary) over the active nodes, from the refreshed fields:
+ * out (host, 6 doubles) = max |u|, max |v|, min J, max J, finite (1/0: every
+ * value finite - u and U in 2-D, U in 3-D - and J > 0), node count.  dim 2:
+ * U [6][n], u [2][n], active [n] (0/1; null = all); dim 3: U [12][n], u [3][n]
+ * (sparse active order, active null).  Each node's |u|, |v| and J are formed
+ * with the reference's NumPy expressions; NaN propagates like NumPy's
+ * max/min.  work: device scratch of cvlbm_field_summary_work_bytes() bytes.
+ * Synchronises `stream`. */
+int cvlbm_field_summary(int32_t dim, int64_t n, const double *U, const double *u,
+                        const int32_t *active, void *work, double *out, void *stream);
+int64_t cvlbm_field_summary_work_bytes(void);
+
 /* Cut-link reconstruction at time t, fpost -> f1, or in place on f0 through a
  * frozen copy in fpost.  Replaces apply_boundary_reconstruction
  * (two_d/curved_boundary_warp.py:4020-4035). */
