@@ -112,7 +112,8 @@ def warmstart_bench(args, dev):
 
     rep = warmstart.train_and_compare(nxy=args.tube_nxy, n_train=args.train, n_test=args.test,
                                       epochs=args.epochs, tol=args.tol, seed=7,
-                                      device=str(dev), gen_batch=args.gen_batch)
+                                      device=str(dev), gen_batch=args.gen_batch,
+                                      consecutive=args.consecutive)
     if args.rank != 0:
         return 0
     line = {"metric": "time-to-residual 1e-8, cold plain / warm batched",
@@ -456,6 +457,8 @@ def main():
     ap.add_argument("--epochs", type=int, default=300, help="tube_warmstart: training epochs")
     ap.add_argument("--gen-batch", type=int, default=32,
                     help="tube_warmstart: training solves run side by side")
+    ap.add_argument("--consecutive", type=int, default=1,
+                    help="tube_warmstart: residual checks in a row below the tolerance")
     ap.add_argument("--instances", type=int, default=256, help="batch256: instance count")
     ap.add_argument("--tol", type=float, default=1e-8, help="batch256: residual tolerance")
     ap.add_argument("--max-replays", type=int, default=100000, help="batch256: replay cap")

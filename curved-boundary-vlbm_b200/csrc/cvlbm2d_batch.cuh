@@ -78,19 +78,27 @@ __global__ void __launch_bounds__(kTX * TY, MINB)
   }
 }
 
-__global__ void __launch_bounds__(kLinkThreads2, 4)
+template <int MAT>
+__global__ void __launch_bounds__(kLinkThreads2, 3)
     k_batch_links2(const Inst2* __restrict__ inst, const InstState2* __restrict__ st,
                    const int2* __restrict__ work, int n_work) {
   __shared__ LinkShared2 sh[kLinksPerBlock2];
+  __shared__ LinkBC2 bc;
+  const int lane = threadIdx.x & (kLG - 1);
+  const int grp = threadIdx.x / kLG;
   for (int w = blockIdx.x; w < n_work; w += gridDim.x) {
     const int2 wk = work[w];
     // uniform over the block (one work item per iteration): the barriers
-    // inside link2_block are reached by every thread or by none
+    // below are reached by every thread or by none
     if (!st[wk.x].active) continue;
     const Inst2& I = inst[wk.x];
+    __syncthreads();  // the previous item's readers of bc are done
+    stage_bc2(I.c.p, bc);
+    __syncthreads();
     double* f1 = I.f[parity_of(st[wk.x]) ^ 1];
-    link2_block(I.c, sh, wk.y, f1, f1, I.U, I.u, &st[wk.x].clock, 0.0, 0.5 * I.c.p.dt, 1,
-                I.scratch, I.partner);
+    const Mat m = link_mat2<MAT>(I.c);
+    link2_group(I.c, m, bc, sh[grp], lane, wk.y + grp, f1, f1, I.U, I.u, &st[wk.x].clock, 0.0,
+                0.5 * I.c.p.dt, 1, I.scratch, I.partner);
   }
 }
 
@@ -206,6 +214,7 @@ struct cvlbm2d_batch {
   // two instance groups on two streams (see batch_run_grouped)
   int groups = 1;
   int inst_split = 0, work_split = 0, lwork_split = 0;
+  int all_neo_hooke = 0;  // every instance neo-Hooke: the link kernel compiled for it
   cudaStream_t side = nullptr;
   cudaEvent_t ev_a = nullptr, ev_b = nullptr;
 };
@@ -240,7 +249,12 @@ void batch_nodes(cvlbm2d_batch* b, int w0, int w1, int store_all, cudaStream_t s
 void batch_links_tick(cvlbm2d_batch* b, int l0, int l1, int i0, int i1, cudaStream_t s) {
   if (l1 > l0) {
     const int grid = b->link_grid < l1 - l0 ? b->link_grid : l1 - l0;
-    k_batch_links2<<<grid, kLinkThreads2, 0, s>>>(b->d_inst, b->d_state, b->d_lwork + l0, l1 - l0);
+    if (b->all_neo_hooke)
+      k_batch_links2<kMatNeoHooke><<<grid, kLinkThreads2, 0, s>>>(b->d_inst, b->d_state,
+                                                                  b->d_lwork + l0, l1 - l0);
+    else
+      k_batch_links2<-1><<<grid, kLinkThreads2, 0, s>>>(b->d_inst, b->d_state, b->d_lwork + l0,
+                                                        l1 - l0);
     cv::count_launches(1);
   }
   if (i1 > i0) {
@@ -383,7 +397,14 @@ extern "C" int cvlbm2d_batch_create(int32_t n_inst, const cvlbm2d_problem* probl
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.nodes, v.threads, v.smem);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_l, k_batch_links2, kLinkThreads2, 0);
+  b->all_neo_hooke = 1;
+  for (int i = 0; i < n_inst; ++i)
+    if (problems[i].mat.model != kMatNeoHooke) b->all_neo_hooke = 0;
+  if (b->all_neo_hooke)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_l, k_batch_links2<kMatNeoHooke>,
+                                                  kLinkThreads2, 0);
+  else
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_l, k_batch_links2<-1>, kLinkThreads2, 0);
   const int full = sms * (per_sm > 0 ? per_sm : 1);
   b->node_grid = grid_blocks > 0 ? grid_blocks : full;
   if (b->node_grid > b->n_work) b->node_grid = b->n_work > 0 ? b->n_work : 1;

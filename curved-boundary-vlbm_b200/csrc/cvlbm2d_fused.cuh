@@ -486,29 +486,51 @@ __global__ void __launch_bounds__(kTX * TY)
 }
 
 // ---------------------------------------------------------------------------
-// Cut-link kernel: 8 links per 64-thread block, in two stages.
-//   gather  8 lanes per link, 16 gathered quantities: q < 6 sums d/dx of
-//           component q over the link's 24-node stencil, 6 <= q < 12 d/dy of
-//           component q - 6, 12 <= q < 16 the F predictor component q - 12;
-//           lane l takes q = l and l + 8 (one code path for every lane on
-//           characteristic links); lanes 0/1 then the tangential image of u
-//           (compatible predictors on a traction wall).
-//   finish  one thread per link: predictor, normal-image solve,
-//           characteristic state and flux tangents, the six population rows.
-//           In one thread the independent chains (the two flux tangents, the
-//           six rows, the BFL population loads) overlap instead of running
-//           lane after lane, and a warp carries 8 links, not 2.
-// Links are visited in `order` (traction links first) so neighbouring links
-// take the same branches.
+// Cut-link kernel: 16 lanes per link, 8 links per 128-thread block.
+// The kernel is a chain of dependent steps per link, so its length is set by
+// the number of dependent global-load levels and by the serial math.  Loads
+// are therefore issued as early as their addresses are known:
+//   level 1  the link row, the stencil node ids and this lane's stencil
+//            weights (all indexed by the processing slot alone); the
+//            boundary tables are staged in shared memory per block
+//   level 2  the stencil values U[node] of this lane's quantity, U at the
+//            node, the dynamic traction and the BFL populations of the row
+//            this lane writes
+// then: lane q < 6 sums d/dx of component q, 6 <= q < 12 d/dy of component
+// q - 6, 12 <= q < 16 the F predictor component q - 12 (one code path for
+// every lane on characteristic links), lanes 0/1 the tangential image of u;
+// lane 0 the predictor and the normal-image solve; lanes 0/1 the two flux
+// tangents (the same code path, the lane picks the direction) while lane 2
+// evaluates P at the characteristic state; lanes 0-5 one population row each.
+// Links are visited in `order` (traction links first) so a warp's two links
+// take the same branches.  MAT >= 0 compiles the kernel for that material
+// law only (smaller code: fewer instruction-cache misses on the chain).
 // ---------------------------------------------------------------------------
-constexpr int kLG = 8;
+constexpr int kLG = 16;
 constexpr int kLinksPerBlock2 = 8;
 constexpr int kLinkThreads2 = kLG * kLinksPerBlock2;
 
 struct LinkShared2 {
   double g[16];  // ux[6], uy[6], Fg[4]
   double dut[2], wt_abs;
+  double Fb[4], cv[6], cw[6], Ax[6], Ay[6], eqx[6], eqy[6], Pb[4], Pc[4];
 };
+
+// boundary tables of one problem, staged per block
+struct LinkBC2 {
+  int32_t kind[kMaxIds2], mode[kMaxIds2];
+  double params[kMaxIds2 * 8];
+};
+
+__device__ __forceinline__ void stage_bc2(const cvlbm2d_problem& p, LinkBC2& B) {
+  for (int t = threadIdx.x; t < kMaxIds2 * 8; t += blockDim.x) {
+    B.params[t] = p.bc_params[t];
+    if (t < kMaxIds2) {
+      B.kind[t] = p.bc_kind[t];
+      B.mode[t] = p.bc_mode[t];
+    }
+  }
+}
 
 // Per-link inputs: the link row when the host built rows, else the link tables.
 struct LinkIn2 {
@@ -518,12 +540,12 @@ struct LinkIn2 {
   bool live, rowed, up_ok, lsq_ok;
 };
 
-__device__ __forceinline__ LinkIn2 link2_in(const Ctx2& c, int slot) {
+__device__ __forceinline__ LinkIn2 link2_in(const Ctx2& c, const LinkBC2& B, int slot) {
   const cvlbm2d_problem& p = c.p;
   LinkIn2 L;
   L.live = slot < p.n_links;
   L.rowed = p.link_rows != nullptr;
-  L.pp = p.bc_params;
+  L.pp = B.params;
   L.eta = 0.5;
   L.xb = L.yb = L.nyb = 0.0;
   L.nxb = 1.0;
@@ -534,8 +556,6 @@ __device__ __forceinline__ LinkIn2 link2_in(const Ctx2& c, int slot) {
   if (!L.live) return L;
   int bid;
   if (L.rowed) {
-    // every per-link input is one load away from the slot (no link_order /
-    // link-table / stencil-id indirection)
     const cvlbm2d_link_row* row = p.link_rows + slot;
     L.ell = row->ell;
     L.i = row->i;
@@ -570,84 +590,12 @@ __device__ __forceinline__ LinkIn2 link2_in(const Ctx2& c, int slot) {
     L.lsq_ok = p.lsq_valid[ell] != 0;
   }
   if (bid < 0 || bid >= kMaxIds2) bid = 0;
-  L.kind = p.bc_kind[bid];
-  L.mode = p.bc_mode[bid];
-  L.pp = p.bc_params + bid * 8;
+  L.kind = B.kind[bid];
+  L.mode = B.mode[bid];
+  L.pp = B.params + bid * 8;
   L.qi = L.qo + 2;
   if (L.qi >= 4) L.qi -= 4;
   return L;
-}
-
-// sum_m w[m] * Uc[node[m]] over the 24 stencil slots in slot order (as
-// _lsq_U_at_boundary, two_d/curved_boundary_warp.py:1213-1221), with all
-// loads issued before the sequential sum.
-__device__ __forceinline__ double lsq_sum(const int* __restrict__ node, const double* __restrict__ w,
-                                          const double* __restrict__ Uc) {
-  int nd[kMaxLsq2];
-  double wv[kMaxLsq2], uv[kMaxLsq2];
-#pragma unroll
-  for (int m = 0; m < kMaxLsq2; ++m) {
-    nd[m] = node[m];
-    wv[m] = w[m];
-  }
-#pragma unroll
-  for (int m = 0; m < kMaxLsq2; ++m) uv[m] = nd[m] >= 0 ? Uc[nd[m]] : 0.0;
-  double out = 0.0;
-#pragma unroll
-  for (int m = 0; m < kMaxLsq2; ++m)
-    if (nd[m] >= 0) out += wv[m] * uv[m];
-  return out;
-}
-
-// Gather stage of one link (slot `slot`) on lane `lane` of its 8-lane group.
-__device__ __forceinline__ void link2_gather(const Ctx2& c, LinkShared2& S, int lane, int slot,
-                                             const double* __restrict__ U,
-                                             const double* __restrict__ u) {
-  const cvlbm2d_problem& p = c.p;
-  const LinkIn2 L = link2_in(c, slot);
-  if (!L.live) return;
-  const int N = c.N, recon = p.recon;
-  // stencil ids and weights of this link (slot order when rows are given)
-  const size_t sl = (size_t)(L.rowed ? slot : L.ell) * kMaxLsq2;
-  const int* lnode = (L.rowed ? p.lsq_node_slot : p.lsq_node) + sl;
-  const bool lsq_recon = (recon == 11 || recon == 12) && L.lsq_ok;
-  const bool use_char = lsq_recon && L.kind == kNeumann;
-  const bool compat = (recon == 9 || recon == 11) && L.lsq_ok;
-#pragma unroll
-  for (int q = lane; q < 16; q += kLG) {
-    if (q < 12 ? use_char : lsq_recon) {
-      const double* w = q < 6 ? (L.rowed ? p.lsq_wx_slot : p.lsq_wx)
-                      : q < 12 ? (L.rowed ? p.lsq_wy_slot : p.lsq_wy)
-                               : (L.rowed ? p.lsq_wb_slot : p.lsq_wb);
-      const int comp = q < 6 ? q : q < 12 ? q - 6 : q - 10;
-      S.g[q] = lsq_sum(lnode, w + sl, U + (size_t)comp * N);
-    } else if (q >= 12) {
-      const double* Uk = U + (size_t)(q - 10) * N;
-      double fg;
-      if (recon == 0 || recon == 2 || recon == 13) {
-        fg = L.up_ok ? Uk[L.n] + L.eta * (Uk[L.n] - Uk[L.nu]) : Uk[L.n];
-        if (recon == 2 && L.lsq_ok)
-          fg = lsq_sum(lnode, (L.rowed ? p.lsq_wb_slot : p.lsq_wb) + sl, Uk);
-      } else {
-        fg = interp_link(Uk, p.active, L.i, L.j, L.qo, L.eta, p.nx, p.ny);
-      }
-      S.g[q] = fg;
-    }
-  }
-  if (compat && L.kind == kNeumann && lane < 2) {
-    // tangential image of u along the wall, component `lane`
-    const double* wt = (L.rowed ? p.lsq_wt_slot : p.lsq_wt) + sl;
-    double d = 0.0, wa = 0.0;
-    for (int mm = 0; mm < kMaxLsq2; ++mm) {
-      const int nd = lnode[mm];
-      if (nd >= 0) {
-        d += wt[mm] * u[(size_t)lane * N + nd];
-        wa += fabs(wt[mm]);
-      }
-    }
-    S.dut[lane] = d;
-    if (lane == 0) S.wt_abs = wa;
-  }
 }
 
 // BFL inputs of population row a of a link: the outgoing post-collision value
@@ -669,121 +617,220 @@ __device__ __forceinline__ void link2_bfl_in(const LinkIn2& L, int a, int N,
   }
 }
 
-// Finish stage of one link, on one thread.
-__device__ __forceinline__ void link2_finish(
-    const Ctx2& c, const LinkShared2& S, int slot, const double* __restrict__ fpost,
-    double* __restrict__ fout, const double* __restrict__ U, const double* clock, double t_host,
-    double offset, int fused, const double* __restrict__ scratch,
-    const int32_t* __restrict__ partner) {
+// One cut link (processing slot `slot`) on the 16 lanes of a group; every
+// lane of the group calls it (only __syncwarp inside).
+__device__ __forceinline__ void link2_group(
+    const Ctx2& c, const Mat& m, const LinkBC2& B, LinkShared2& S, int lane, int slot,
+    const double* __restrict__ fpost, double* __restrict__ fout, const double* __restrict__ U,
+    const double* __restrict__ u, const double* clock, double t_host, double offset, int fused,
+    const double* __restrict__ scratch, const int32_t* __restrict__ partner) {
   const cvlbm2d_problem& p = c.p;
-  const Mat& m = c.m;
-  const LinkIn2 L = link2_in(c, slot);
-  if (!L.live) return;
-  const int N = c.N, recon = p.recon, kind = L.kind, mode = L.mode, n = L.n, qi = L.qi;
+  const int N = c.N, recon = p.recon;
+  const bool live = slot < p.n_links;
+  const bool rowed = p.link_rows != nullptr;
+  // this lane's quantity: d/dx (q < 6), d/dy (6 <= q < 12) of component
+  // comp, or the predictor of F component q - 12
+  const int q = lane;
+  const int comp = q < 6 ? q : q < 12 ? q - 6 : q - 10;
+  const bool lsq_tables = recon == 2 || recon == 9 || recon == 11 || recon == 12;
+  // -- level 1: slot-indexed stencil tables (slot order) and the link row ----
+  int nd[kMaxLsq2];
+  double wv[kMaxLsq2];
+  const bool early = live && rowed && lsq_tables;
+  if (early) {
+    const size_t sl = (size_t)slot * kMaxLsq2;
+    const double* w = q < 6 ? p.lsq_wx_slot : q < 12 ? p.lsq_wy_slot : p.lsq_wb_slot;
+#pragma unroll
+    for (int k = 0; k < kMaxLsq2; ++k) {
+      nd[k] = p.lsq_node_slot[sl + k];
+      wv[k] = w[sl + k];
+    }
+  }
+  const LinkIn2 L = link2_in(c, B, slot);
+  const size_t sl = (size_t)(L.rowed ? slot : L.ell) * kMaxLsq2;
+  if (live && !early && lsq_tables) {
+    const int* lnode = (L.rowed ? p.lsq_node_slot : p.lsq_node) + sl;
+    const double* w = q < 6 ? (L.rowed ? p.lsq_wx_slot : p.lsq_wx)
+                    : q < 12 ? (L.rowed ? p.lsq_wy_slot : p.lsq_wy)
+                             : (L.rowed ? p.lsq_wb_slot : p.lsq_wb);
+#pragma unroll
+    for (int k = 0; k < kMaxLsq2; ++k) {
+      nd[k] = lnode[k];
+      wv[k] = w[sl + k];
+    }
+  }
+  const bool lsq_recon = (recon == 11 || recon == 12) && L.lsq_ok;
+  const bool use_char = lsq_recon && L.kind == kNeumann;
+  const bool compat = (recon == 9 || recon == 11) && L.lsq_ok;
+  const bool tang = compat && L.kind == kNeumann && lane < 2;
+  // -- level 2: stencil values, node values, traction, BFL populations -------
+  const bool mine = live && (q < 12 ? use_char : (lsq_recon || (recon == 2 && L.lsq_ok)));
+  double uv[kMaxLsq2];
+  if (mine) {
+    const double* Uq = U + (size_t)comp * N;
+#pragma unroll
+    for (int k = 0; k < kMaxLsq2; ++k) uv[k] = nd[k] >= 0 ? Uq[nd[k]] : 0.0;
+  }
+  double Un0 = 0.0, Un1 = 0.0, trx = 0.0, try_ = 0.0;
+  if (live && lane == 0) {
+    Un0 = U[L.n];
+    Un1 = U[(size_t)N + L.n];
+    if (L.kind == kNeumann && p.use_dynamic_traction != 0) {
+      trx = p.traction_x[L.ell];
+      try_ = p.traction_y[L.ell];
+    }
+  }
+  double fo = 0.0, fi = 0.0, upv = 0.0;
+  if (live && lane < 6 && !use_char) link2_bfl_in(L, lane, N, fpost, fused, scratch, partner, fo, fi, upv);
+
+  // -- gathered quantities ----------------------------------------------------
+  if (live) {
+    if (mine) {
+      double acc = 0.0;
+#pragma unroll
+      for (int k = 0; k < kMaxLsq2; ++k)
+        if (nd[k] >= 0) acc += wv[k] * uv[k];
+      S.g[q] = acc;
+    } else if (q >= 12) {
+      const double* Uk = U + (size_t)comp * N;
+      double fg;
+      if (recon == 0 || recon == 2 || recon == 13) {
+        fg = L.up_ok ? Uk[L.n] + L.eta * (Uk[L.n] - Uk[L.nu]) : Uk[L.n];
+      } else {
+        fg = interp_link(Uk, p.active, L.i, L.j, L.qo, L.eta, p.nx, p.ny);
+      }
+      S.g[q] = fg;
+    }
+    if (tang) {
+      // tangential image of u along the wall, component `lane`
+      const double* wt = (L.rowed ? p.lsq_wt_slot : p.lsq_wt) + sl;
+      const double* uc = u + (size_t)lane * N;
+      double d = 0.0, wa = 0.0;
+#pragma unroll
+      for (int k = 0; k < kMaxLsq2; ++k) {
+        if (nd[k] >= 0) {
+          d += wt[k] * uc[nd[k]];
+          wa += fabs(wt[k]);
+        }
+      }
+      S.dut[lane] = d;
+      if (lane == 0) S.wt_abs = wa;
+    }
+  }
+  __syncwarp();
+
+  const int qi = L.qi, kind = L.kind, mode = L.mode;
   const double* pp = L.pp;
   const double nxb = L.nxb, nyb = L.nyb, eta = L.eta;
-  const bool lsq_recon = (recon == 11 || recon == 12) && L.lsq_ok;
-  const bool use_char = lsq_recon && kind == kNeumann;
-  const bool compat = (recon == 9 || recon == 11) && L.lsq_ok;
-  // loads that do not depend on the chain below go first
-  const double Un0 = U[n], Un1 = U[(size_t)N + n];
-  double fo[6], fi[6], upv[6];
-  if (!use_char) {
-#pragma unroll
-    for (int a = 0; a < 6; ++a) link2_bfl_in(L, a, N, fpost, fused, scratch, partner, fo[a],
-                                             fi[a], upv[a]);
-  }
-  const double tmid = time_of(clock, t_host, offset);
-  double bv0 = value2(0, mode, pp, L.xb, L.yb, nxb, nyb, tmid);
-  double bv1 = value2(1, mode, pp, L.xb, L.yb, nxb, nyb, tmid);
-  if (kind == kNeumann && p.use_dynamic_traction != 0) {
-    bv0 = p.traction_x[L.ell];
-    bv1 = p.traction_y[L.ell];
-  }
   const double dt = p.dt, cc = p.c, om = p.omega;
   const double dxin = (double)cx2(qi), dyin = (double)cy2(qi);
+  const double tmid = time_of(clock, t_host, offset);
+  // lane 0 of the group loaded the dynamic traction; every lane needs bv for
+  // its row (all 32 lanes of the warp take part in the shuffles)
+  const int lane0 = (threadIdx.x & 31) & ~(kLG - 1);
+  const double trx_g = __shfl_sync(0xffffffffu, trx, lane0);
+  const double try_g = __shfl_sync(0xffffffffu, try_, lane0);
+  double bv0 = 0.0, bv1 = 0.0;
+  if (live) {
+    bv0 = value2(0, mode, pp, L.xb, L.yb, nxb, nyb, tmid);
+    bv1 = value2(1, mode, pp, L.xb, L.yb, nxb, nyb, tmid);
+    if (kind == kNeumann && p.use_dynamic_traction != 0) {
+      bv0 = trx_g;
+      bv1 = try_g;
+    }
+  }
 
-  // -- predictor finalisation and the normal-image solve ---------------------
-  double Fg[4] = {S.g[12], S.g[13], S.g[14], S.g[15]};
-  if (compat) {
-    const double tanx = -nyb, tany = nxb;
-    double dut0 = 0.0, dut1 = 0.0, wt_abs = 0.0;
-    if (kind == kNeumann) {
-      dut0 = S.dut[0];
-      dut1 = S.dut[1];
-      wt_abs = S.wt_abs;
-    } else {
-      if (mode == 6) {
-        double at = tmid;
-        if (pp[6] > 0.0 && at > pp[6]) at = pp[6];
-        dut0 = at * (pp[0] * tanx + pp[1] * tany);
-        dut1 = at * (pp[3] * tanx + pp[4] * tany);
+  // -- predictor finalisation, normal-image solve, characteristic state -------
+  if (live && lane == 0) {
+    double Fg[4] = {S.g[12], S.g[13], S.g[14], S.g[15]};
+    if (compat) {
+      const double tanx = -nyb, tany = nxb;
+      double dut0 = 0.0, dut1 = 0.0, wt_abs = 0.0;
+      if (kind == kNeumann) {
+        dut0 = S.dut[0];
+        dut1 = S.dut[1];
+        wt_abs = S.wt_abs;
+      } else {
+        if (mode == 6) {
+          double at = tmid;
+          if (pp[6] > 0.0 && at > pp[6]) at = pp[6];
+          dut0 = at * (pp[0] * tanx + pp[1] * tany);
+          dut1 = at * (pp[3] * tanx + pp[4] * tany);
+        }
+        wt_abs = 1.0;
       }
-      wt_abs = 1.0;
+      if (wt_abs > 0.0) {
+        const double hn0 = Fg[0] * nxb + Fg[1] * nyb, hn1 = Fg[2] * nxb + Fg[3] * nyb;
+        const double gt0 = tanx + dut0, gt1 = tany + dut1;
+        Fg[0] = hn0 * nxb + gt0 * tanx;
+        Fg[1] = hn0 * nyb + gt0 * tany;
+        Fg[2] = hn1 * nxb + gt1 * tanx;
+        Fg[3] = hn1 * nyb + gt1 * tany;
+      }
     }
-    if (wt_abs > 0.0) {
-      const double hn0 = Fg[0] * nxb + Fg[1] * nyb, hn1 = Fg[2] * nxb + Fg[3] * nyb;
-      const double gt0 = tanx + dut0, gt1 = tany + dut1;
-      Fg[0] = hn0 * nxb + gt0 * tanx;
-      Fg[1] = hn0 * nyb + gt0 * tany;
-      Fg[2] = hn1 * nxb + gt1 * tanx;
-      Fg[3] = hn1 * nyb + gt1 * tany;
+    double Fb[4] = {Fg[0], Fg[1], Fg[2], Fg[3]};
+    if (kind == kNeumann) solve_normal_image2(Fg, nxb, nyb, bv0, bv1, m, p.normal_solver, Fb);
+    const P2 Pb = piola2(Fb[0], Fb[1], Fb[2], Fb[3], m);
+    S.Pb[0] = Pb.a;
+    S.Pb[1] = Pb.b;
+    S.Pb[2] = Pb.c;
+    S.Pb[3] = Pb.d;
+    for (int k = 0; k < 4; ++k) S.Fb[k] = Fb[k];
+    double cv[6] = {Un0, Un1, Fb[0], Fb[1], Fb[2], Fb[3]};
+    if (kind == kDirichlet) {
+      cv[0] = bv0;
+      cv[1] = bv1;
     }
+    if (use_char) {
+      const double sx = -eta * dt * cc * (double)cx2(L.qo);
+      const double sy = -eta * dt * cc * (double)cy2(L.qo);
+      double dv[6];
+      for (int a = 0; a < 6; ++a) dv[a] = sx * S.g[a] + sy * S.g[6 + a];
+      double sc = 1.0;
+      for (int g = 0; g < 10; ++g) {
+        const double t11 = cv[2] + sc * dv[2], t12 = cv[3] + sc * dv[3];
+        const double t21 = cv[4] + sc * dv[4], t22 = cv[5] + sc * dv[5];
+        if (t11 * t22 - t12 * t21 > 10.0 * m.jf) break;
+        sc = 0.5 * sc;
+      }
+      for (int a = 0; a < 6; ++a) cv[a] = cv[a] + sc * dv[a];
+    }
+    for (int a = 0; a < 6; ++a) S.cv[a] = cv[a];
   }
-  double Fb[4] = {Fg[0], Fg[1], Fg[2], Fg[3]};
-  if (kind == kNeumann) solve_normal_image2(Fg, nxb, nyb, bv0, bv1, m, p.normal_solver, Fb);
-  const P2 Pb = piola2(Fb[0], Fb[1], Fb[2], Fb[3], m);
+  __syncwarp();
 
-  // -- characteristic state, flux tangents and equilibrium flux --------------
-  double cv[6] = {Un0, Un1, Fb[0], Fb[1], Fb[2], Fb[3]};
-  if (kind == kDirichlet) {
-    cv[0] = bv0;
-    cv[1] = bv1;
-  }
-  double cw[6], eqx[6], eqy[6];
-  P2 Pc{0.0, 0.0, 0.0, 0.0};
-  bool char_ok = false;
-  if (use_char) {
-    double ux[6], uy[6];
+  // -- flux tangents (lanes 0/1, one code path) and P at the state (lane 2) ---
+  if (use_char && lane < 2) {
+    double ax[6], ay[6];
+    flux2_jvp(S.cv, S.g + 6 * lane, m, ax, ay);  // lane 0: A_x U_x, lane 1: A_y U_y
 #pragma unroll
     for (int a = 0; a < 6; ++a) {
-      ux[a] = S.g[a];
-      uy[a] = S.g[6 + a];
+      if (lane == 0)
+        S.Ax[a] = ax[a];
+      else
+        S.Ay[a] = ay[a];
     }
-    const double sx = -eta * dt * cc * (double)cx2(L.qo);
-    const double sy = -eta * dt * cc * (double)cy2(L.qo);
-    double dv[6];
-    for (int a = 0; a < 6; ++a) dv[a] = sx * ux[a] + sy * uy[a];
-    double sc = 1.0;
-    for (int g = 0; g < 10; ++g) {
-      const double t11 = cv[2] + sc * dv[2], t12 = cv[3] + sc * dv[3];
-      const double t21 = cv[4] + sc * dv[4], t22 = cv[5] + sc * dv[5];
-      if (t11 * t22 - t12 * t21 > 10.0 * m.jf) break;
-      sc = 0.5 * sc;
-    }
-    for (int a = 0; a < 6; ++a) cv[a] = cv[a] + sc * dv[a];
-    double Ax[6], Ay[6], unused[6];
-    flux2_jvp(cv, ux, m, Ax, unused);  // A_x U_x
-    flux2_jvp(cv, uy, m, unused, Ay);  // A_y U_y
-#pragma unroll
-    for (int a = 0; a < 6; ++a) {
-      const double b = source_comp(a, p.source_mode, p.source, cv);
-      cw[a] = b - Ax[a] - Ay[a] + cc * (dxin * ux[a] + dyin * uy[a]);
-    }
-    char_ok = cv[2] * cv[5] - cv[3] * cv[4] > m.jf;
-    if (char_ok) {
-      flux2_jvp(cv, cw, m, eqx, eqy);
-      Pc = piola2(cv[2], cv[3], cv[4], cv[5], m);
-    } else {
-#pragma unroll
-      for (int a = 0; a < 6; ++a) link2_bfl_in(L, a, N, fpost, fused, scratch, partner, fo[a],
-                                               fi[a], upv[a]);
-    }
+  } else if (use_char && lane == 2) {
+    const P2 Pc = piola2(S.cv[2], S.cv[3], S.cv[4], S.cv[5], m);
+    S.Pc[0] = Pc.a;
+    S.Pc[1] = Pc.b;
+    S.Pc[2] = Pc.c;
+    S.Pc[3] = Pc.d;
   }
+  __syncwarp();
+  if (use_char && lane < 6) {
+    const int a = lane;
+    const double b = source_comp(a, p.source_mode, p.source, S.cv);
+    S.cw[a] = b - S.Ax[a] - S.Ay[a] + cc * (dxin * S.g[a] + dyin * S.g[6 + a]);
+  }
+  __syncwarp();
+  const bool char_ok = use_char && S.cv[2] * S.cv[5] - S.cv[3] * S.cv[4] > m.jf;
+  if (char_ok && lane == 0) flux2_jvp(S.cv, S.cw, m, S.eqx, S.eqy);
+  __syncwarp();
 
-  // -- the six population rows ----------------------------------------------
-#pragma unroll
-  for (int a = 0; a < 6; ++a) {
+  // -- one population row per lane -----------------------------------------
+  if (live && lane < 6) {
+    const int a = lane;
     double D = 1.0, Sv = 0.0;
     if (kind == kDirichlet) {
       switch (a) {
@@ -796,53 +843,56 @@ __device__ __forceinline__ void link2_finish(
       }
     } else {
       switch (a) {
-        case 0: Sv = -(dxin * Pb.a + dyin * Pb.b) / cc; break;
-        case 1: Sv = -(dxin * Pb.c + dyin * Pb.d) / cc; break;
-        default: D = -1.0; Sv = 0.5 * Fb[a - 2]; break;
+        case 0: Sv = -(dxin * S.Pb[0] + dyin * S.Pb[1]) / cc; break;
+        case 1: Sv = -(dxin * S.Pb[2] + dyin * S.Pb[3]) / cc; break;
+        default: D = -1.0; Sv = 0.5 * S.Fb[a - 2]; break;
       }
     }
     double val;
     if (char_ok) {
-      const double jv = 0.25 * (cw[a] + (2.0 / cc) * (dxin * eqx[a] + dyin * eqy[a]));
-      const double ge = feq2(qi, a, cv, Pc, 2.0 / cc);
-      const double sa = source_comp(a, p.source_mode, p.source, cv);
+      const P2 Pc{S.Pc[0], S.Pc[1], S.Pc[2], S.Pc[3]};
+      const double jv = 0.25 * (S.cw[a] + (2.0 / cc) * (dxin * S.eqx[a] + dyin * S.eqy[a]));
+      const double ge = feq2(qi, a, S.cv, Pc, 2.0 / cc);
+      const double sa = source_comp(a, p.source_mode, p.source, S.cv);
       val = ge - dt / om * jv + dt * (1.0 / om - 0.5) * 0.25 * sa;
-    } else if (eta >= 0.5) {
-      const double al = 1.0 / (2.0 * eta);
-      val = al * (D * fo[a] + Sv) + (1.0 - al) * fi[a];
     } else {
-      val = D * (2.0 * eta * fo[a] + (1.0 - 2.0 * eta) * upv[a]) + Sv;
+      if (use_char) link2_bfl_in(L, a, N, fpost, fused, scratch, partner, fo, fi, upv);
+      if (eta >= 0.5) {
+        const double al = 1.0 / (2.0 * eta);
+        val = al * (D * fo + Sv) + (1.0 - al) * fi;
+      } else {
+        val = D * (2.0 * eta * fo + (1.0 - 2.0 * eta) * upv) + Sv;
+      }
     }
-    fout[(size_t)(qi * 6 + a) * N + n] = val;
+    fout[(size_t)(qi * 6 + a) * N + L.n] = val;
   }
 }
 
-// Links [slot0, slot0 + 8) on the 64 threads of a block (every thread calls
-// it; contains block barriers).
-__device__ __forceinline__ void link2_block(
-    const Ctx2& c, LinkShared2* sh, int slot0, const double* __restrict__ fpost,
-    double* __restrict__ fout, const double* __restrict__ U, const double* __restrict__ u,
-    const double* clock, double t_host, double offset, int fused,
-    const double* __restrict__ scratch, const int32_t* __restrict__ partner) {
-  const int lane = threadIdx.x & (kLG - 1);
-  const int grp = threadIdx.x / kLG;
-  link2_gather(c, sh[grp], lane, slot0 + grp, U, u);
-  __syncthreads();
-  if (threadIdx.x < kLinksPerBlock2)
-    link2_finish(c, sh[threadIdx.x], slot0 + threadIdx.x, fpost, fout, U, clock, t_host, offset,
-                 fused, scratch, partner);
-  __syncthreads();
+// The material of the kernel: the problem's, or MAT when it is compiled for one.
+template <int MAT>
+__device__ __forceinline__ Mat link_mat2(const Ctx2& c) {
+  Mat m = c.m;
+  if (MAT >= 0) m.model = MAT;
+  return m;
 }
 
-__global__ void __launch_bounds__(kLinkThreads2, 4)
+template <int MAT>
+__global__ void __launch_bounds__(kLinkThreads2, 3)
     k_links2g(Ctx2 c, const double* __restrict__ fpost, double* __restrict__ fout,
               const double* __restrict__ U, const double* __restrict__ u, const double* clock,
               double t_host, double offset, int fused, const double* __restrict__ scratch,
               const int32_t* __restrict__ partner, double* clock_next) {
   __shared__ LinkShared2 sh[kLinksPerBlock2];
+  __shared__ LinkBC2 bc;
+  stage_bc2(c.p, bc);
+  __syncthreads();
+  const int lane = threadIdx.x & (kLG - 1);
+  const int grp = threadIdx.x / kLG;
+  const int slot = blockIdx.x * kLinksPerBlock2 + grp;
   if (clock_next && blockIdx.x == 0 && threadIdx.x == 0) *clock_next = clock[0] + c.p.dt;
-  link2_block(c, sh, blockIdx.x * kLinksPerBlock2, fpost, fout, U, u, clock, t_host, offset,
-              fused, scratch, partner);
+  const Mat m = link_mat2<MAT>(c);
+  link2_group(c, m, bc, sh[grp], lane, slot, fpost, fout, U, u, clock, t_host, offset, fused,
+              scratch, partner);
 }
 
 }  // namespace

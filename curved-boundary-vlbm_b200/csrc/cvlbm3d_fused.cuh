@@ -719,17 +719,31 @@ constexpr int kGatherLinks = 128 / kGatherLanes;
 __global__ void __launch_bounds__(128)
     k3_link_gather(Ctx3 c, Fused3 fz, double* __restrict__ char_state) {
   __shared__ int s_slot[kGatherLinks][kChar];
-  __shared__ double s_w[4][kChar][kGatherLinks];
+  __shared__ double s_w[kGatherLinks][4][kChar];
   const cvlbm3d_problem& p = c.p;
   const int L = p.n_links;
   const int ell0 = blockIdx.x * kGatherLinks;
-  for (int t = threadIdx.x; t < kChar * kGatherLinks; t += blockDim.x) {
-    const int mm = t / kGatherLinks, g = t % kGatherLinks;
-    const int ell = ell0 + g;
-    s_slot[g][mm] = ell < L ? fz.char_slot[(size_t)mm * L + ell] : -1;
+  if (p.char_slot_lm && p.char_w_lm) {
+    // link-major copies: the block's 8 links are one contiguous run of slots
+    // and one of weights (16 KB), read with 16-byte loads
+    const int nl = L - ell0 < kGatherLinks ? L - ell0 : kGatherLinks;
+    const int4* src_s = reinterpret_cast<const int4*>(p.char_slot_lm + (size_t)ell0 * kChar);
+    int4* dst_s = reinterpret_cast<int4*>(&s_slot[0][0]);
+    for (int t = threadIdx.x; t < kGatherLinks * kChar / 4; t += blockDim.x)
+      dst_s[t] = t < nl * kChar / 4 ? src_s[t] : make_int4(-1, -1, -1, -1);
+    const double2* src_w = reinterpret_cast<const double2*>(p.char_w_lm + (size_t)ell0 * 4 * kChar);
+    double2* dst_w = reinterpret_cast<double2*>(&s_w[0][0][0]);
+    for (int t = threadIdx.x; t < kGatherLinks * 4 * kChar / 2; t += blockDim.x)
+      dst_w[t] = t < nl * 4 * kChar / 2 ? src_w[t] : make_double2(0.0, 0.0);
+  } else {
+    for (int t = threadIdx.x; t < kChar * kGatherLinks; t += blockDim.x) {
+      const int mm = t / kGatherLinks, g = t % kGatherLinks;
+      const int ell = ell0 + g;
+      s_slot[g][mm] = ell < L ? fz.char_slot[(size_t)mm * L + ell] : -1;
 #pragma unroll
-    for (int k = 0; k < 4; ++k)
-      s_w[k][mm][g] = ell < L ? p.char_w[((size_t)k * kChar + mm) * L + ell] : 0.0;
+      for (int k = 0; k < 4; ++k)
+        s_w[g][k][mm] = ell < L ? p.char_w[((size_t)k * kChar + mm) * L + ell] : 0.0;
+    }
   }
   __syncthreads();
   const int a = threadIdx.x % kGatherLanes;
@@ -750,10 +764,10 @@ __global__ void __launch_bounds__(128)
     for (int k = 0; k < kChunk; ++k) {
       const int mm = m0 + k;
       if (s_slot[g][mm] >= 0) {
-        v0 += s_w[0][mm][g] * uv[k];
-        gx += s_w[1][mm][g] * uv[k];
-        gy += s_w[2][mm][g] * uv[k];
-        gz += s_w[3][mm][g] * uv[k];
+        v0 += s_w[g][0][mm] * uv[k];
+        gx += s_w[g][1][mm] * uv[k];
+        gy += s_w[g][2][mm] * uv[k];
+        gz += s_w[g][3][mm] * uv[k];
       }
     }
   }

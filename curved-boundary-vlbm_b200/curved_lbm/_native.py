@@ -96,6 +96,7 @@ class Problem3D(C.Structure):
         ("link_partner", pI), ("link_order", pI), ("link_nodes", pI), ("n_link_nodes", i32),
         ("overlap", i32),
         ("wave_items", pI), ("n_wave_items", i32), ("n_planes", i32), ("wave_plane_chunks", pI),
+        ("char_slot_lm", pI), ("char_w_lm", pI),
     ]
 
 

@@ -319,9 +319,11 @@ def make_tube_solver(prm: dict, nxy: int, *, ramp_time: float, device="cuda:0"):
 
 
 def run_to_residual(solver, tol: float, *, check: int = 100, t_min: float = 0.0,
-                    max_steps: int = 400_000, graph=None) -> dict:
+                    max_steps: int = 400_000, graph=None, consecutive: int = 1) -> dict:
     """Step until |u - u_prev|_2 / (check |u|_2) < tol (relative displacement
-    change per step over a check interval), after t >= t_min."""
+    change per step over a check interval) at `consecutive` checks in a row,
+    after t >= t_min.  (More than one check keeps a lightly damped
+    oscillation from passing the test at a turning point.)"""
     import torch
 
     g = graph if graph is not None else solver.capture_graph(check)
@@ -330,13 +332,15 @@ def run_to_residual(solver, tol: float, *, check: int = 100, t_min: float = 0.0,
     t0 = _time.perf_counter()
     steps0 = solver.steps
     r = float("inf")
+    run = 0
     while solver.steps - steps0 < max_steps:
         g.launch()
         du = torch.linalg.vector_norm(solver.u - prev).item()
         nu = torch.linalg.vector_norm(solver.u).item()
         r = du / (check * nu) if nu > 0 else float("inf")
         prev.copy_(solver.u)
-        if solver.time >= t_min and r < tol:
+        run = run + 1 if (solver.time >= t_min and r < tol) else 0
+        if run >= consecutive:
             break
     torch.cuda.synchronize()
     return {"wall_s": _time.perf_counter() - t0, "steps": solver.steps - steps0, "residual": r,
@@ -344,7 +348,7 @@ def run_to_residual(solver, tol: float, *, check: int = 100, t_min: float = 0.0,
 
 
 def run_batch_to_residual(solvers: list, tol: float, *, check: int = 100, t_min=0.0,
-                          max_steps: int = 400_000) -> dict:
+                          max_steps: int = 400_000, consecutive: int = 1) -> dict:
     """`run_to_residual` for several independent solvers at once.
 
     Each solver replays its own captured `check`-step graph on its own CUDA
@@ -373,6 +377,7 @@ def run_batch_to_residual(solvers: list, tol: float, *, check: int = 100, t_min=
     norms = torch.zeros((n, 2), dtype=torch.float64, device=dev)
     steps0 = [s.steps for s in solvers]
     res = [float("inf")] * n
+    runs = [0] * n
     active = list(range(n))
     torch.cuda.synchronize(dev)
     main = torch.cuda.current_stream(dev)
@@ -395,8 +400,8 @@ def run_batch_to_residual(solvers: list, tol: float, *, check: int = 100, t_min=
             s = solvers[i]
             du, nu = float(h[i, 0]), float(h[i, 1])
             res[i] = du / (check * nu) if nu > 0 else float("inf")
-            done = s.time >= t_mins[i] and res[i] < tol
-            if not done and s.steps - steps0[i] < max_steps:
+            runs[i] = runs[i] + 1 if (s.time >= t_mins[i] and res[i] < tol) else 0
+            if runs[i] < consecutive and s.steps - steps0[i] < max_steps:
                 still.append(i)
         active = still
         for i in active:
@@ -572,7 +577,7 @@ def _solver_state(s) -> np.ndarray:
 
 def train_and_compare(*, nxy: int = 32, n_train: int = 64, n_test: int = 4, epochs: int = 200,
                       tol: float = 1e-8, seed: int = 7, device="cuda:0", modes=(4, 4, 8),
-                      lr: float = 2e-3, gen_batch: int = 32) -> dict:
+                      lr: float = 2e-3, gen_batch: int = 32, consecutive: int = 1) -> dict:
     """Generate solver equilibria, train the surrogate, then compare warm and
     cold starts on held-out cases.
 
@@ -624,13 +629,13 @@ def train_and_compare(*, nxy: int = 32, n_train: int = 64, n_test: int = 4, epoc
     cases = []
     for prm, pred, (x, mask) in zip(test, preds, feats):
         cold = make_tube_solver(prm, nxy, ramp_time=ramp, device=device)
-        ci = run_to_residual(cold, tol, t_min=ramp)
+        ci = run_to_residual(cold, tol, t_min=ramp, consecutive=consecutive)
         u_cold = solver_targets(cold)
         st_cold = _solver_state(cold)
         run_to_residual(cold, tol / 100.0)
         ref = solver_targets(cold)
         warm, ok, t_min = warm_solver(prm, pred)
-        wi = run_to_residual(warm, tol, t_min=t_min)
+        wi = run_to_residual(warm, tol, t_min=t_min, consecutive=consecutive)
         u_warm = solver_targets(warm)
         cases.append({"params": prm, "warm_ok": ok, "cold_steps": ci["steps"],
                       "warm_steps": wi["steps"], "cold_wall_s": ci["wall_s"],
@@ -643,13 +648,14 @@ def train_and_compare(*, nxy: int = 32, n_train: int = 64, n_test: int = 4, epoc
         del cold, warm
     # the same solves again, every case side by side
     colds = [make_tube_solver(prm, nxy, ramp_time=ramp, device=device) for prm in test]
-    cb = run_batch_to_residual(colds, tol, t_min=ramp)
+    cb = run_batch_to_residual(colds, tol, t_min=ramp, consecutive=consecutive)
     cold_same = all(c["cold_steps"] == b["steps"] and np.array_equal(c["_cold_state"],
                                                                       _solver_state(s))
                     for c, b, s in zip(cases, cb["solvers"], colds))
     del colds
     built = [warm_solver(prm, pred) for prm, pred in zip(test, preds)]
-    wb = run_batch_to_residual([s for s, _, _ in built], tol, t_min=[t for _, _, t in built])
+    wb = run_batch_to_residual([s for s, _, _ in built], tol, t_min=[t for _, _, t in built],
+                               consecutive=consecutive)
     warm_same = all(c["warm_steps"] == b["steps"] and np.array_equal(c["_warm_state"],
                                                                       _solver_state(s))
                     for c, b, (s, _, _) in zip(cases, wb["solvers"], built))
@@ -659,7 +665,8 @@ def train_and_compare(*, nxy: int = 32, n_train: int = 64, n_test: int = 4, epoc
     cold_w = sum(c["cold_wall_s"] for c in cases)
     warm_w = sum(c["warm_wall_s"] for c in cases)
     return {"nxy": nxy, "dx": dx, "min_wall": 4.0 * dx, "n_train": n_train, "n_test": n_test,
-            "epochs": epochs, "tol": tol, "modes": list(modes), "generate_s": gen_s,
+            "epochs": epochs, "tol": tol, "consecutive_checks": consecutive,
+            "modes": list(modes), "generate_s": gen_s,
             "fit_s": fit_s, "train_loss_first": hist[0], "train_loss_last": hist[-1],
             "train_steps_mean": steps_sum / max(n_done, 1), "ranks": world,
             "cases": cases, "cold_wall_s": cold_w, "warm_wall_s": warm_w,

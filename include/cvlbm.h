@@ -354,6 +354,11 @@ typedef struct cvlbm3d_problem {
   int32_t n_wave_items;
   int32_t n_planes;                               /* x-planes (nx) */
   const int32_t *wave_plane_chunks;               /* [n_planes] items of one stage per plane */
+  /* link-major copies of the characteristic tables for the fused gather
+     (optional; both set: each block of 8 links reads its slots and weights
+     as one contiguous run instead of 64-byte pieces n_links apart) */
+  const int32_t *char_slot_lm;                    /* [n_links][64] = char_slot transposed */
+  const double *char_w_lm;                        /* [n_links][4][64] = char_w transposed */
 } cvlbm3d_problem;
 
 typedef struct cvlbm3d_fields {
