@@ -127,6 +127,8 @@ def warmstart_bench(args, dev):
                                       "held-out comparison on rank 0",
                        "epochs": args.epochs, "tol": args.tol},
             "warm_plain_speedup": rep["speedup_wall"], "steps_ratio": rep["speedup_steps"],
+            "equal_error_speedup": rep["speedup_batched_equal_error"],
+            "equal_error_steps_ratio": rep["speedup_steps_equal_error"],
             "report": rep}
     print(json.dumps(line, default=float), flush=True)
     return 0

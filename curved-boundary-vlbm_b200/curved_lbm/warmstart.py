@@ -348,7 +348,7 @@ def run_to_residual(solver, tol: float, *, check: int = 100, t_min: float = 0.0,
 
 
 def run_batch_to_residual(solvers: list, tol: float, *, check: int = 100, t_min=0.0,
-                          max_steps: int = 400_000, consecutive: int = 1) -> dict:
+                          max_steps=400_000, consecutive: int = 1) -> dict:
     """`run_to_residual` for several independent solvers at once.
 
     Each solver replays its own captured `check`-step graph on its own CUDA
@@ -357,8 +357,8 @@ def run_batch_to_residual(solvers: list, tol: float, *, check: int = 100, t_min=
     read back with a single copy per round.  A solver stops at the first
     round its residual criterion holds, exactly as it would alone (same
     graph, same steps), so each solver's steps and final state equal those of
-    a solo `run_to_residual`.  `t_min` is one time for all or one per
-    solver.  Returns per-solver steps / residual / invalid and the wall time
+    a solo `run_to_residual`.  `t_min` and `max_steps` are one value for
+    all or one per solver.  Returns per-solver steps / residual / invalid and the wall time
     of the whole batch."""
     import torch
 
@@ -369,8 +369,9 @@ def run_batch_to_residual(solvers: list, tol: float, *, check: int = 100, t_min=
         raise ValueError("run_batch_to_residual: every solver must live on the same device")
     n = len(solvers)
     t_mins = [float(t) for t in t_min] if isinstance(t_min, (list, tuple)) else [float(t_min)] * n
-    if len(t_mins) != n:
-        raise ValueError("run_batch_to_residual: one t_min per solver")
+    caps = [int(v) for v in max_steps] if isinstance(max_steps, (list, tuple)) else [int(max_steps)] * n
+    if len(t_mins) != n or len(caps) != n:
+        raise ValueError("run_batch_to_residual: one t_min / max_steps per solver")
     graphs = [s.capture_graph(check) for s in solvers]
     streams = [torch.cuda.Stream(device=dev) for _ in range(n)]
     prev = [s.u.clone() for s in solvers]
@@ -401,7 +402,7 @@ def run_batch_to_residual(solvers: list, tol: float, *, check: int = 100, t_min=
             du, nu = float(h[i, 0]), float(h[i, 1])
             res[i] = du / (check * nu) if nu > 0 else float("inf")
             runs[i] = runs[i] + 1 if (s.time >= t_mins[i] and res[i] < tol) else 0
-            if runs[i] < consecutive and s.steps - steps0[i] < max_steps:
+            if runs[i] < consecutive and s.steps - steps0[i] < caps[i]:
                 still.append(i)
         active = still
         for i in active:
@@ -589,7 +590,10 @@ def train_and_compare(*, nxy: int = 32, n_train: int = 64, n_test: int = 4, epoc
     Wall times: cold and warm plain (one solve after another, the way the
     reference runs its cases) and batched (every held-out case side by side,
     `run_batch_to_residual`).  The batched runs are checked to reach the
-    plain runs' step counts and states bit for bit.
+    plain runs' step counts and states bit for bit.  At equal final error:
+    the warm solves stopped at the first check where their error against the
+    converged field is at or below the cold run's final error, timed batched
+    (`speedup_batched_equal_error`).
     """
     from . import replicas, workloads
 
@@ -644,7 +648,7 @@ def train_and_compare(*, nxy: int = 32, n_train: int = 64, n_test: int = 4, epoc
                       "prediction_err": _rel_err(pred, ref, mask),
                       "guess_err": _rel_err(kinematic_guess(prm, nxy) * mask[None, :], ref, mask),
                       "warm_invalid": wi["invalid"], "cold_invalid": ci["invalid"],
-                      "_cold_state": st_cold, "_warm_state": _solver_state(warm)})
+                      "_cold_state": st_cold, "_warm_state": _solver_state(warm), "_ref": ref})
         del cold, warm
     # the same solves again, every case side by side
     colds = [make_tube_solver(prm, nxy, ramp_time=ramp, device=device) for prm in test]
@@ -660,8 +664,33 @@ def train_and_compare(*, nxy: int = 32, n_train: int = 64, n_test: int = 4, epoc
                                                                       _solver_state(s))
                     for c, b, (s, _, _) in zip(cases, wb["solvers"], built))
     del built
+    # equal final error: the first check (every `check` steps) at which the
+    # warm run's error against the converged field is at or below the cold
+    # run's final error (calibration pass, untimed), then the warm solves
+    # timed side by side to exactly those step counts
+    check = 100
+    eq_steps = []
+    for prm, pred, (x, mask), c in zip(test, preds, feats, cases):
+        warm, ok, t_min = warm_solver(prm, pred)
+        g = warm.capture_graph(check)
+        steps = None
+        while warm.steps < 50 * max(c["cold_steps"], check):
+            g.launch()
+            if _rel_err(solver_targets(warm), c["_ref"], mask) <= c["cold_err"]:
+                steps = warm.steps
+                break
+        c["warm_steps_equal_error"] = steps
+        eq_steps.append(steps if steps is not None else warm.steps)
+        del g, warm
+    built = [warm_solver(prm, pred) for prm, pred in zip(test, preds)]
+    we = run_batch_to_residual([s for s, _, _ in built], 0.0, check=check, max_steps=eq_steps)
+    eq_errs = [_rel_err(solver_targets(s), c["_ref"], m) for (s, _, _), c, (_, m)
+               in zip(built, cases, feats)]
+    for c, e in zip(cases, eq_errs):
+        c["warm_err_equal_error"] = e
+    del built
     for c in cases:
-        del c["_cold_state"], c["_warm_state"]
+        del c["_cold_state"], c["_warm_state"], c["_ref"]
     cold_w = sum(c["cold_wall_s"] for c in cases)
     warm_w = sum(c["warm_wall_s"] for c in cases)
     return {"nxy": nxy, "dx": dx, "min_wall": 4.0 * dx, "n_train": n_train, "n_test": n_test,
@@ -672,6 +701,11 @@ def train_and_compare(*, nxy: int = 32, n_train: int = 64, n_test: int = 4, epoc
             "cases": cases, "cold_wall_s": cold_w, "warm_wall_s": warm_w,
             "cold_batched_wall_s": cb["wall_s"], "warm_batched_wall_s": wb["wall_s"],
             "batched_equals_plain": bool(cold_same and warm_same),
+            "warm_batched_equal_error_wall_s": we["wall_s"],
+            "equal_error_reached": all(c["warm_steps_equal_error"] is not None for c in cases),
+            "speedup_batched_equal_error": cold_w / max(we["wall_s"], 1e-12),
+            "speedup_steps_equal_error": sum(c["cold_steps"] for c in cases)
+            / max(sum(eq_steps), 1),
             "speedup_wall": cold_w / max(warm_w, 1e-12),
             "speedup_batched": cold_w / max(wb["wall_s"], 1e-12),
             "speedup_steps": sum(c["cold_steps"] for c in cases)

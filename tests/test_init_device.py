@@ -17,8 +17,12 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-# log/exp laws: a few ulps of the largest population
-FIELD_RTOL = 1e-13
+# log/exp laws: the two libm's roundings of P differ by an ulp or so, and the
+# second-order start's flux tangents are centred differences with a step
+# eps = 1e-6 / max(1, max|W|), which divide that difference by 2 eps: 1e-11
+# of the largest population (measured on a B200: order 1 and 2 below 1e-13,
+# order 3 of log_neo_hooke above it)
+FIELD_RTOL = 1e-11
 
 
 def _solver(n=48, material="neo_hooke", source="damping"):
