@@ -58,10 +58,13 @@ HBM_FALLBACK_GBS = 6650.0
 # ---------------------------------------------------------------------------
 # workloads
 # ---------------------------------------------------------------------------
-def build_annulus(device=None, n=512, oracle=False, threads=1):
+def build_annulus(device=None, n=512, oracle=False, threads=1, intervals=None):
     from curved_lbm import workloads
 
     geom, mat, spec, kw = workloads.annulus(n)
+    if intervals is not None:  # profiler captures of the node kernel's parts
+        kw = dict(kw, local_displacement_interval=intervals[0],
+                  local_compatibility_interval=intervals[1])
     if oracle:
         from oracle.oracle import Oracle2D
 
@@ -465,6 +468,10 @@ def main():
     ap.add_argument("--tol", type=float, default=1e-8, help="batch256: residual tolerance")
     ap.add_argument("--max-replays", type=int, default=100000, help="batch256: replay cap")
     ap.add_argument("--inner", type=int, default=100, help="lattice steps per bench step")
+    ap.add_argument("--local-intervals", default="",
+                    help="annulus: 'SWEEP,REPAIR' step intervals of the displacement sweep and "
+                         "the F repair (0 = off), for profiler captures of the node kernel's "
+                         "parts, not bench lines")
     ap.add_argument("--size", type=int, default=0,
                     help="lattice nodes per axis (0 = the workload's own size; smaller sizes "
                          "are for profiler captures, not bench lines)")
@@ -523,6 +530,10 @@ def main():
             dist.destroy_process_group()
         return rc
     size_kw = {"n": args.size} if args.size > 0 else {}
+    if args.local_intervals:
+        if args.workload != "annulus512":
+            raise SystemExit("--local-intervals applies to the annulus workload only")
+        size_kw["intervals"] = tuple(int(v) for v in args.local_intervals.split(","))
     solver, n_active = BUILDERS[args.workload](device=str(dev), **size_kw)
     if args.overlap != "default" and hasattr(solver, "overlap_links"):
         solver.overlap_links = args.overlap == "on"
