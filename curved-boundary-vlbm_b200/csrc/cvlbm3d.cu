@@ -711,7 +711,10 @@ extern "C" int cvlbm3d_run(const cvlbm3d_problem* p, cvlbm3d_fields* f, double t
       timer_end(tk, s);
       if (L > 0) {
         if (p->has_char) {
-          k3_link_gather<<<blocks(L, kGatherLinks), 128, 0, s>>>(c, fz, f->char_state);
+          if (p->char_slot_lm && p->char_w_lm)
+            k3_link_gather4<<<blocks(L, kGather4Links), 128, 0, s>>>(c, fz, f->char_state);
+          else
+            k3_link_gather<<<blocks(L, kGatherLinks), 128, 0, s>>>(c, fz, f->char_state);
           cv::count_launches(1);
         }
         k3_link_prepare<<<blocks(L, 128), 128, 0, s>>>(c, fz, f->u, *f, clock, t, 0.5 * p->dt);

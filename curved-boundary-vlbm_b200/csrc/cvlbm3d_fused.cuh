@@ -741,27 +741,13 @@ __global__ void __launch_bounds__(128)
   const cvlbm3d_problem& p = c.p;
   const int L = p.n_links;
   const int ell0 = blockIdx.x * kGatherLinks;
-  if (p.char_slot_lm && p.char_w_lm) {
-    // link-major copies: the block's 8 links are one contiguous run of slots
-    // and one of weights (16 KB), read with 16-byte loads
-    const int nl = L - ell0 < kGatherLinks ? L - ell0 : kGatherLinks;
-    const int4* src_s = reinterpret_cast<const int4*>(p.char_slot_lm + (size_t)ell0 * kChar);
-    int4* dst_s = reinterpret_cast<int4*>(&s_slot[0][0]);
-    for (int t = threadIdx.x; t < kGatherLinks * kChar / 4; t += blockDim.x)
-      dst_s[t] = t < nl * kChar / 4 ? src_s[t] : make_int4(-1, -1, -1, -1);
-    const double2* src_w = reinterpret_cast<const double2*>(p.char_w_lm + (size_t)ell0 * 4 * kChar);
-    double2* dst_w = reinterpret_cast<double2*>(&s_w[0][0][0]);
-    for (int t = threadIdx.x; t < kGatherLinks * 4 * kChar / 2; t += blockDim.x)
-      dst_w[t] = t < nl * 4 * kChar / 2 ? src_w[t] : make_double2(0.0, 0.0);
-  } else {
-    for (int t = threadIdx.x; t < kChar * kGatherLinks; t += blockDim.x) {
-      const int mm = t / kGatherLinks, g = t % kGatherLinks;
-      const int ell = ell0 + g;
-      s_slot[g][mm] = ell < L ? fz.char_slot[(size_t)mm * L + ell] : -1;
+  for (int t = threadIdx.x; t < kChar * kGatherLinks; t += blockDim.x) {
+    const int mm = t / kGatherLinks, g = t % kGatherLinks;
+    const int ell = ell0 + g;
+    s_slot[g][mm] = ell < L ? fz.char_slot[(size_t)mm * L + ell] : -1;
 #pragma unroll
-      for (int k = 0; k < 4; ++k)
-        s_w[g][k][mm] = ell < L ? p.char_w[((size_t)k * kChar + mm) * L + ell] : 0.0;
-    }
+    for (int k = 0; k < 4; ++k)
+      s_w[g][k][mm] = ell < L ? p.char_w[((size_t)k * kChar + mm) * L + ell] : 0.0;
   }
   __syncthreads();
   const int a = threadIdx.x % kGatherLanes;
@@ -793,6 +779,68 @@ __global__ void __launch_bounds__(128)
   char_state[((size_t)1 * 12 + a) * L + ell] = gx;
   char_state[((size_t)2 * 12 + a) * L + ell] = gy;
   char_state[((size_t)3 * 12 + a) * L + ell] = gz;
+}
+
+// The same gather with 4 lanes per link, 3 components per lane and 32 links
+// per block, from the link-major copies of the tables (char_slot_lm
+// [n_links][64], char_w_lm [n_links][64][4]): a sample's slot and four
+// weights are one 4-byte and two 16-byte loads shared by the link's lanes,
+// every lane does useful work (the 16-lane form leaves 4 of 16 idle), and
+// each lane runs 12 independent accumulations.  Each of the 48 sums runs
+// over the samples in slot order, as in k3_link_gather (the same doubles).
+constexpr int kGather4Lanes = 4;
+constexpr int kGather4Links = 128 / kGather4Lanes;
+
+__global__ void __launch_bounds__(128)
+    k3_link_gather4(Ctx3 c, Fused3 fz, double* __restrict__ char_state) {
+  const cvlbm3d_problem& p = c.p;
+  const int L = p.n_links;
+  const int lane = threadIdx.x % kGather4Lanes;
+  const int ell = blockIdx.x * kGather4Links + threadIdx.x / kGather4Lanes;
+  if (ell >= L || p.char_idx[ell] < 0) return;
+  const int a0 = 3 * lane;
+  const int* slot = p.char_slot_lm + (size_t)ell * kChar;
+  const double2* w2 = reinterpret_cast<const double2*>(p.char_w_lm + (size_t)ell * kChar * 4);
+  double acc[3][4];
+#pragma unroll
+  for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) acc[cc][k] = 0.0;
+  constexpr int kChunk = 8;
+#pragma unroll 1
+  for (int m0 = 0; m0 < kChar; m0 += kChunk) {
+    int q[kChunk];
+    double2 wa[kChunk], wb[kChunk];
+    double uv[kChunk][3];
+#pragma unroll
+    for (int k = 0; k < kChunk; ++k) {
+      q[k] = slot[m0 + k];
+      wa[k] = w2[2 * (m0 + k)];
+      wb[k] = w2[2 * (m0 + k) + 1];
+    }
+#pragma unroll
+    for (int k = 0; k < kChunk; ++k) {
+      const double* row = fz.Uneed + (size_t)(q[k] >= 0 ? q[k] : 0) * kC3 + a0;
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) uv[k][cc] = q[k] >= 0 ? row[cc] : 0.0;
+    }
+#pragma unroll
+    for (int k = 0; k < kChunk; ++k) {
+      if (q[k] >= 0) {
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) {
+          acc[cc][0] += wa[k].x * uv[k][cc];
+          acc[cc][1] += wa[k].y * uv[k][cc];
+          acc[cc][2] += wb[k].x * uv[k][cc];
+          acc[cc][3] += wb[k].y * uv[k][cc];
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) char_state[((size_t)k * 12 + a0 + cc) * L + ell] = acc[cc][k];
 }
 
 // Boundary value, F predictor, Newton normal solve and P(F_b) of one link;

@@ -418,10 +418,10 @@ class WarpSparseCurvedBoundaryLBM3D:
             t["need_slot"] = dev_i(need_slot)
             if char_slot is not None:
                 t["char_slot"] = dev_i(char_slot)
-                # link-major copies for the fused gather (one contiguous run
-                # of slots and weights per block of links)
+                # link-major copies for the fused gather: a link's slots and,
+                # per sample, its four weights side by side
                 t["char_slot_lm"] = t["char_slot"].view(-1, nl).t().contiguous()
-                t["char_w_lm"] = t["char_w"].view(4, -1, nl).permute(2, 0, 1).contiguous()
+                t["char_w_lm"] = t["char_w"].view(4, -1, nl).permute(2, 1, 0).contiguous()
             t["link_partner"] = dev_i(partner)
             t["link_order"] = dev_i(order)
         link_nodes = np.unique(np.asarray(tables["link_p"], dtype=np.int64))

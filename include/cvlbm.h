@@ -358,11 +358,12 @@ typedef struct cvlbm3d_problem {
   int32_t n_wave_items;
   int32_t n_planes;                               /* x-planes (nx) */
   const int32_t *wave_plane_chunks;               /* [n_planes] items of one stage per plane */
-  /* link-major copies of the characteristic tables for the fused gather
-     (optional; both set: each block of 8 links reads its slots and weights
-     as one contiguous run instead of 64-byte pieces n_links apart) */
+  /* link-major copies of the characteristic tables (optional; both set
+     select the 4-lanes-per-link gather, which reads a sample's slot and its
+     four weights as one 4-byte and two 16-byte loads) */
   const int32_t *char_slot_lm;                    /* [n_links][64] = char_slot transposed */
-  const double *char_w_lm;                        /* [n_links][4][64] = char_w transposed */
+  const double *char_w_lm;                        /* [n_links][64][4]: char_w[k][m][l] at
+                                                     [l][m][k] */
 } cvlbm3d_problem;
 
 typedef struct cvlbm3d_fields {

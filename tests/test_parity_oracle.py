@@ -175,6 +175,22 @@ def test_shell_200_steps_match_oracle(variant):
     close_rel("u", s.active_displacement(), ref["u"])
 
 
+def test_shell96_gather_forms_bitwise_equal():
+    """The 4-lanes-per-link characteristic gather (link-major tables) and the
+    16-lane form (the reference's table layout): one state after 20 steps."""
+    states = []
+    for lm in (True, False):
+        s = _gpu_shell(96, 0)
+        if not lm:
+            s._tables.pop("char_slot_lm")
+            s._tables.pop("char_w_lm")
+            s._problem = s._make_problem()
+        s.run(20)
+        states.append([s._host(t) for t in (s.f0, s.U, s.u, s.char_state)])
+    for a, b in zip(*states):
+        assert np.array_equal(a, b)
+
+
 def test_shell96_collide_variants_bitwise_equal():
     """Every collide kernel, with and without the next step's moments
     overlapping the link kernels, eager and replayed from a graph: one state."""
