@@ -685,15 +685,6 @@ extern "C" int cvlbm3d_run(const cvlbm3d_problem* p, cvlbm3d_fields* f, double t
         else if (p->node_variant == 2)
           k3_collide_node<3><<<blocks(N, 128), 128, 0, s>>>(c, fz, f->f0, f->f1, f->U, f->u,
                                                             repair, k == nsteps - 1);
-        else if (p->node_variant == 5)
-          k3_collide_node<4, 1><<<blocks(N, 128), 128, 0, s>>>(c, fz, f->f0, f->f1, f->U, f->u,
-                                                               repair, k == nsteps - 1);
-        else if (p->node_variant == 6)
-          k3_collide_node<3, 1><<<blocks(N, 128), 128, 0, s>>>(c, fz, f->f0, f->f1, f->U, f->u,
-                                                               repair, k == nsteps - 1);
-        else if (p->node_variant == 7)
-          k3_collide_node<3, 2><<<blocks(N, 128), 128, 0, s>>>(c, fz, f->f0, f->f1, f->U, f->u,
-                                                               repair, k == nsteps - 1);
         else
           k3_collide_node<4><<<blocks(N, 128), 128, 0, s>>>(c, fz, f->f0, f->f1, f->U, f->u,
                                                             repair, k == nsteps - 1);

@@ -541,12 +541,11 @@ __device__ __forceinline__ void node_prologue3(const Ctx3& c, const Fused3& fz, 
   }
 }
 
-template <int Q, bool PRE = false>
+template <int Q>
 __device__ __forceinline__ void collide_dir3(const cvlbm3d_problem& p, const Fused3& fz,
                                              const NodeState3& st,
                                              const double* __restrict__ f0,
-                                             double* __restrict__ f1, int N, int n,
-                                             const double* pre = nullptr) {
+                                             double* __restrict__ f1, int N, int n) {
   constexpr int ax = Q % 3;
   constexpr double s = Q < 3 ? 1.0 : -1.0;
   const double k3c = 3.0 / p.c, sixth = 1.0 / 6.0, om = p.omega;
@@ -570,7 +569,7 @@ __device__ __forceinline__ void collide_dir3(const cvlbm3d_problem& p, const Fus
   }
   double old[kC3];
 #pragma unroll
-  for (int a = 0; a < kC3; ++a) old[a] = PRE ? pre[a] : f0[(size_t)(Q * kC3 + a) * N + n];
+  for (int a = 0; a < kC3; ++a) old[a] = f0[(size_t)(Q * kC3 + a) * N + n];
 #pragma unroll
   for (int a = 0; a < kC3; ++a) {
     double fe;
@@ -593,10 +592,8 @@ __device__ __forceinline__ void collide_dir3(const cvlbm3d_problem& p, const Fus
 }
 
 // MINB resident blocks of 128 threads per SM bound the registers per thread
-// (4: 128 registers, 3: 168).  NPF directions' populations (0-2) are loaded
-// before the node's prologue, so that their memory latency overlaps its
-// FP64 work (Piola, repair) instead of following it.
-template <int MINB, int NPF = 0>
+// (4: 128 registers, 3: 168).
+template <int MINB>
 __global__ void __launch_bounds__(128, MINB)
     k3_collide_node(Ctx3 c, Fused3 fz, const double* __restrict__ f0, double* __restrict__ f1,
                     double* __restrict__ U, const double* __restrict__ u, int do_repair,
@@ -604,26 +601,11 @@ __global__ void __launch_bounds__(128, MINB)
   const int N = c.N;
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= N) return;
-  double pre0[kC3], pre1[kC3];
-  if (NPF >= 1) {
-#pragma unroll
-    for (int a = 0; a < kC3; ++a) pre0[a] = f0[(size_t)(0 * kC3 + a) * N + n];
-  }
-  if (NPF >= 2) {
-#pragma unroll
-    for (int a = 0; a < kC3; ++a) pre1[a] = f0[(size_t)(1 * kC3 + a) * N + n];
-  }
   NodeState3 st;
   node_prologue3(c, fz, U, u, do_repair, store_all, n, st);
   const cvlbm3d_problem& p = c.p;
-  if (NPF >= 1)
-    collide_dir3<0, true>(p, fz, st, f0, f1, N, n, pre0);
-  else
-    collide_dir3<0>(p, fz, st, f0, f1, N, n);
-  if (NPF >= 2)
-    collide_dir3<1, true>(p, fz, st, f0, f1, N, n, pre1);
-  else
-    collide_dir3<1>(p, fz, st, f0, f1, N, n);
+  collide_dir3<0>(p, fz, st, f0, f1, N, n);
+  collide_dir3<1>(p, fz, st, f0, f1, N, n);
   collide_dir3<2>(p, fz, st, f0, f1, N, n);
   collide_dir3<3>(p, fz, st, f0, f1, N, n);
   collide_dir3<4>(p, fz, st, f0, f1, N, n);

@@ -710,7 +710,7 @@ class WarpSparseCurvedBoundaryLBM3D:
 
     # fused collide kernel: 0 one thread per node (128 registers), 1 six warps
     # per 32 nodes (shared memory), 2 one thread per node (168 registers)
-    NODE_VARIANTS = (0, 1, 2, 3, 4, 5, 6, 7)
+    NODE_VARIANTS = (0, 1, 2, 3, 4)
 
     @property
     def overlap_links(self) -> bool:

@@ -328,12 +328,8 @@ typedef struct cvlbm3d_problem {
                                                      per 32 nodes (shared memory), 2 one
                                                      thread per node within 168 registers,
                                                      3 / 4 the wavefront form (wave_*
-                                                     tables) within 128 / 168 registers,
-                                                     5 / 6 / 7 one thread per node with the
-                                                     first one / one / two directions'
-                                                     populations loaded before the node's
-                                                     Piola and repair work (128 / 168 / 168
-                                                     registers); results are identical */
+                                                     tables) within 128 / 168 registers;
+                                                     results are identical */
   const int32_t *char_slot;                       /* [64*n_links] char_idx mapped to
                                                      U_need rows (-1 unused) */
   const int32_t *link_partner;                    /* [n_links] link at the same node in the

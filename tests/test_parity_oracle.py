@@ -163,7 +163,7 @@ def test_shell64_1000_steps_match_oracle():
     _cache.pop(("shell", 64, 1000), None)
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
 def test_shell_200_steps_match_oracle(variant):
     s = _gpu_shell(40, variant)
     ref = _oracle_shell(40, 200, s.characteristic_stencil)
@@ -199,8 +199,7 @@ def test_shell96_collide_variants_bitwise_equal():
     want = None
     for v, overlap, graph in ((1, False, False), (0, False, False), (2, False, False),
                               (0, True, False), (0, True, True), (3, False, False),
-                              (4, False, False), (3, False, True), (5, False, False),
-                              (6, False, False), (7, False, False), (7, False, True)):
+                              (4, False, False), (3, False, True)):
         s = _gpu_shell(96, v)
         s.overlap_links = overlap
         if graph:
