@@ -161,10 +161,24 @@ __device__ __forceinline__ void fused2_tile(
       ucol1 = ustar[N + n] + c.hdt * S[1];
     }
   }
-  for (int r = threadIdx.x; r < kRN; r += blockDim.x) {
-    const int ri = r / kRX, rj = r - ri * kRX;
-    const bool interior = ri >= kH && ri < kH + kTY && rj >= kH && rj < kH + kTX;
-    if (interior) continue;
+  // the halo ring only (3 rows above and below the tile, 3 columns either
+  // side of its rows), enumerated so that every lane of a warp takes a halo
+  // node (a loop over the whole region would leave the lanes over interior
+  // nodes idle in most warps)
+  constexpr int kHalo = 2 * kH * kRX + 2 * kH * kTY;
+  for (int h = threadIdx.x; h < kHalo; h += blockDim.x) {
+    int ri, rj;
+    if (h < 2 * kH * kRX) {
+      const int hr = h / kRX;  // 0..5: rows 0..2 and TY+3..TY+5
+      rj = h - hr * kRX;
+      ri = hr < kH ? hr : kTY + hr;
+    } else {
+      const int h3 = h - 2 * kH * kRX;
+      const int row = h3 / (2 * kH), col = h3 - row * (2 * kH);
+      ri = kH + row;
+      rj = col < kH ? col : kTX + col;
+    }
+    const int r = ri * kRX + rj;
     const int gi = i0 - kH + ri, gj = j0 - kH + rj;
     const bool inb = gi >= 0 && gi < nx && gj >= 0 && gj < ny;
     const int m = gi * ny + gj;
