@@ -551,13 +551,19 @@ def main():
     # timed afterwards on a graph of the same steps without the overlap.
     overlap = bool(getattr(solver, "overlap_links", False))
     timer = _native.KernelTimer(args.inner)
+    # the 2-D cut-link kernel's own event pairs (timed where the node kernel is)
+    ltimer = _native.KernelTimer(args.inner, "links") if args.workload == "annulus512" else None
     if not overlap:
         timer.attach()
+        if ltimer:
+            ltimer.attach()
     n0 = _native.launch_count()
     graph = solver.capture_graph(args.inner)
     launches_per_graph = _native.launch_count() - n0
     if not overlap:
         timer.detach()
+        if ltimer:
+            ltimer.detach()
 
     for _ in range(args.warmup):
         graph.launch()
@@ -568,6 +574,7 @@ def main():
         dist.barrier()
 
     step_ms, kern_ms, kern_n = [], 0.0, 0
+    link_ms, link_n = 0.0, 0
     with ClockSampler(local) as clocks:
         torch.cuda.synchronize(dev)
         if world > 1:
@@ -584,6 +591,10 @@ def main():
                 ms, cnt = timer.elapsed()
                 kern_ms += ms
                 kern_n += cnt
+                if ltimer:
+                    ms, cnt = ltimer.elapsed()
+                    link_ms += ms
+                    link_n += cnt
         torch.cuda.synchronize(dev)
         if world > 1:
             dist.barrier()
@@ -591,12 +602,18 @@ def main():
     if overlap:
         solver.overlap_links = False
         timer.attach()
+        if ltimer:
+            ltimer.attach()
         kgraph = solver.capture_graph(args.inner)
         timer.detach()
+        if ltimer:
+            ltimer.detach()
         solver.overlap_links = True
         for _ in range(2):
             kgraph.launch()
         timer.elapsed()
+        if ltimer:
+            ltimer.elapsed()
         kern_total_ms = 0.0
         for _ in range(args.steps):
             flush.zero_()
@@ -609,6 +626,10 @@ def main():
             ms, cnt = timer.elapsed()
             kern_ms += ms
             kern_n += cnt
+            if ltimer:
+                ms, cnt = ltimer.elapsed()
+                link_ms += ms
+                link_n += cnt
         del kgraph
     total_ms = float(sum(step_ms))
     from curved_lbm import replicas
@@ -710,6 +731,11 @@ def main():
         "clocks": clocks.summary(),
         "gpu_launches": int(launches_per_graph * args.steps),
     }
+    if link_n:
+        line["link_kernel"] = {
+            "avg_us": link_ms * 1e3 / link_n, "launches": link_n,
+            "timed": "CUDA events around each cut-link kernel launch, in the graph without "
+                     "the link overlap (L2 flushed between bench steps)"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     del graph

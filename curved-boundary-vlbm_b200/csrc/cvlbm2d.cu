@@ -610,12 +610,14 @@ void launch_links(const Ctx2& c, const double* src, double* dst, const double* U
   attr[0].val.priority = link_priority();
   cfg.attrs = attr;
   cfg.numAttrs = 1;
+  const int tk = link_timer_begin(s);
   if (c.m.model == kMatNeoHooke)
     cudaLaunchKernelEx(&cfg, k_links2g<kMatNeoHooke>, c, src, dst, U, u, clock, t, offset, fused,
                        scratch, partner, clock_next);
   else
     cudaLaunchKernelEx(&cfg, k_links2g<-1>, c, src, dst, U, u, clock, t, offset, fused, scratch,
                        partner, clock_next);
+  link_timer_end(tk, s);
   cv::count_launches(1);
 }
 

@@ -11,11 +11,13 @@ namespace cv {
 namespace {
 thread_local std::string g_last_error;
 thread_local cvlbm_timer* g_timer = nullptr;
+thread_local cvlbm_timer* g_link_timer = nullptr;
 std::atomic<long long> g_launches{0};
 }  // namespace
 void set_error(const char* msg) { g_last_error = msg ? msg : ""; }
 void count_launches(int n) { g_launches += n; }
 cvlbm_timer* attached_timer() { return g_timer; }
+cvlbm_timer* attached_link_timer() { return g_link_timer; }
 int attach_timer(cvlbm_timer* t) {
   g_timer = t;
   return CVLBM_OK;
@@ -38,6 +40,7 @@ extern "C" int cvlbm_timer_create(int32_t capacity, cvlbm_timer** out) {
 extern "C" void cvlbm_timer_destroy(cvlbm_timer* t) {
   if (!t) return;
   if (cv::g_timer == t) cv::g_timer = nullptr;
+  if (cv::g_link_timer == t) cv::g_link_timer = nullptr;
   for (int k = 0; k < t->capacity; ++k) {
     cudaEventDestroy(t->begin[k]);
     cudaEventDestroy(t->end[k]);
@@ -70,6 +73,11 @@ extern "C" int cvlbm_timer_elapsed(cvlbm_timer* t, double* total_ms, int32_t* co
 }
 
 extern "C" int cvlbm_timer_attach(cvlbm_timer* t) { return cv::attach_timer(t); }
+
+extern "C" int cvlbm_timer_attach_links(cvlbm_timer* t) {
+  cv::g_link_timer = t;
+  return CVLBM_OK;
+}
 
 extern "C" int cvlbm_version(void) { return 10000; }
 

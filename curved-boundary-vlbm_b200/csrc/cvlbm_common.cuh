@@ -44,6 +44,19 @@ inline void timer_end(int k, cudaStream_t s) {
   if (k >= 0) cudaEventRecordWithFlags(attached_timer()->end[k], s, cudaEventRecordExternal);
 }
 
+// The same for the cut-link kernel (a second per-thread timer).
+cvlbm_timer* attached_link_timer();
+inline int link_timer_begin(cudaStream_t s) {
+  cvlbm_timer* t = attached_link_timer();
+  if (!t || t->used >= t->capacity) return -1;
+  int k = t->used++;
+  cudaEventRecordWithFlags(t->begin[k], s, cudaEventRecordExternal);
+  return k;
+}
+inline void link_timer_end(int k, cudaStream_t s) {
+  if (k >= 0) cudaEventRecordWithFlags(attached_link_timer()->end[k], s, cudaEventRecordExternal);
+}
+
 inline int fail(int code, const char* msg) {
   set_error(msg);
   return code;

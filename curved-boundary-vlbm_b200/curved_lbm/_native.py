@@ -141,6 +141,7 @@ EXPORTED = (
     "cvlbm_timer_reset",
     "cvlbm_timer_elapsed",
     "cvlbm_timer_attach",
+    "cvlbm_timer_attach_links",
     "cvlbm_launch_count",
     "cvlbm2d_tile_variant",
     "cvlbm2d_run_static_scratch",
@@ -206,6 +207,7 @@ def load(require_cuda: bool = True):
         "cvlbm_timer_reset": (i32, [pI]),
         "cvlbm_timer_elapsed": (i32, [pI, C.POINTER(f64), C.POINTER(i32)]),
         "cvlbm_timer_attach": (i32, [pI]),
+        "cvlbm_timer_attach_links": (i32, [pI]),
         "cvlbm_launch_count": (i64, []),
         "cvlbm2d_tile_variant": (i32, [i32]),
         "cvlbm2d_run_static_scratch": (i32, [P2, F2, f64, i64, i32, pI]),
@@ -283,16 +285,19 @@ def ptr(t) -> int:
 class KernelTimer:
     """CUDA-event pairs around the dominant kernel of every step (see cvlbm.h)."""
 
-    def __init__(self, capacity: int) -> None:
+    def __init__(self, capacity: int, kernel: str = "node") -> None:
+        """kernel: "node" (the bulk node kernel) or "links" (the 2-D cut-link kernel)."""
         self.lib = load()
         self.handle = C.c_void_p()
+        self._attach = (self.lib.cvlbm_timer_attach_links if kernel == "links"
+                        else self.lib.cvlbm_timer_attach)
         check(self.lib.cvlbm_timer_create(int(capacity), C.byref(self.handle)), "cvlbm_timer_create")
 
     def attach(self) -> None:
-        check(self.lib.cvlbm_timer_attach(self.handle), "cvlbm_timer_attach")
+        check(self._attach(self.handle), "cvlbm_timer_attach")
 
     def detach(self) -> None:
-        check(self.lib.cvlbm_timer_attach(None), "cvlbm_timer_attach")
+        check(self._attach(None), "cvlbm_timer_attach")
 
     def reset(self) -> None:
         check(self.lib.cvlbm_timer_reset(self.handle), "cvlbm_timer_reset")

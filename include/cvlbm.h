@@ -450,6 +450,9 @@ int cvlbm_timer_elapsed(cvlbm_timer *t, double *total_ms, int32_t *count);
 /* Attach (or detach with NULL) the timer used by subsequent runs/captures
  * on this thread. */
 int cvlbm_timer_attach(cvlbm_timer *t);
+/* Attach (or with NULL detach) a timer to the cut-link kernel of the 2-D
+ * step, the same way: one event pair per launch of the link kernel. */
+int cvlbm_timer_attach_links(cvlbm_timer *t);
 
 /* Number of kernel launches this library has issued (host-side counter;
  * launches replayed from a CUDA graph are counted once, at capture). */
