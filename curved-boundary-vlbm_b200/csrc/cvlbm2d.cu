@@ -693,7 +693,9 @@ bool fused_ok(const cvlbm2d_problem* p, const cvlbm2d_fields* f) {
   const FusedLaunch2 fl = fused_variant(p->tile_variant);
   return p->tiles && p->need_fields && p->link_partner && f->link_scratch && p->lsq_node &&
          p->disp_sweeps <= 1 && fl.tile_i == p->tile_i && (!fl.mom || f->fpost) &&
-         p->collision_model == 0 && !(p->kinetic_filter > 0.0);
+         p->collision_model == 0 && !(p->kinetic_filter > 0.0) &&
+         // the fused node kernel indexes populations with 32-bit offsets
+         24LL * p->nx * p->ny < 2147483647LL;
 }
 
 }  // namespace

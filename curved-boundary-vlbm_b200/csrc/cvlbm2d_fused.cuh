@@ -65,7 +65,7 @@ __device__ __forceinline__ void moments2c(const Ctx2& c, const double* __restric
 #pragma unroll
   for (int q = 0; q < 4; ++q)
 #pragma unroll
-    for (int a = 0; a < 6; ++a) S[a] += f0[(size_t)(q * 6 + a) * N + n];
+    for (int a = 0; a < 6; ++a) S[a] += f0[(q * 6 + a) * N + n];
   if (c.p.source_mode == kSrcConstant) {
 #pragma unroll
     for (int a = 0; a < 6; ++a) S[a] += c.hdt * c.p.source[a];
@@ -142,7 +142,7 @@ __device__ __forceinline__ void fused2_tile(
       for (int q = 0; q < 4; ++q)
 #pragma unroll
         for (int a = 0; a < 6; ++a) {
-          const double v = f0[(size_t)(q * 6 + a) * N + n];
+          const double v = f0[(q * 6 + a) * N + n];
           sfo[(q * 6 + a) * kTN + threadIdx.x] = v;
           S[a] += v;
         }
@@ -426,7 +426,7 @@ __device__ __forceinline__ void fused2_tile(
       if constexpr (STAGE)
         old = sfo[(q * 6 + a) * kTN + threadIdx.x];
       else
-        old = f0[(size_t)(q * 6 + a) * N + n];
+        old = f0[(q * 6 + a) * N + n];
       const double fe = 0.25 * (has_g ? (neg ? Ua - g : Ua + g) : Ua);
       double v = old + om * (fe - old);
       if (add_src && (a < 2 || add_src_f)) v = v + swB;
@@ -440,7 +440,7 @@ __device__ __forceinline__ void fused2_tile(
       }
       const int d = dst[q];
       if (d >= 0)
-        f1[(size_t)(q * 6 + a) * N + d] = v;
+        f1[(q * 6 + a) * N + d] = v;
       else if (d <= -2)
         fz.scratch[(size_t)(-2 - d) * 6 + a] = v;
     }
@@ -452,11 +452,11 @@ __device__ __forceinline__ void fused2_tile(
   ustar_out[N + n] = (ucol1 + 0.5 * dt * S[1]) + (un1 - ucol1);
   if (own_need) {
     Ug[n] = S[0];
-    Ug[(size_t)N + n] = S[1];
-    Ug[2 * (size_t)N + n] = Fn[0];
-    Ug[3 * (size_t)N + n] = Fn[1];
-    Ug[4 * (size_t)N + n] = Fn[2];
-    Ug[5 * (size_t)N + n] = Fn[3];
+    Ug[N + n] = S[1];
+    Ug[2 * N + n] = Fn[0];
+    Ug[3 * N + n] = Fn[1];
+    Ug[4 * N + n] = Fn[2];
+    Ug[5 * N + n] = Fn[3];
     ug[n] = un0;
     ug[N + n] = un1;
   }
