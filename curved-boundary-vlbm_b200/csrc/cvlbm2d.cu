@@ -610,13 +610,22 @@ void launch_links(const Ctx2& c, const double* src, double* dst, const double* U
   attr[0].val.priority = link_priority();
   cfg.attrs = attr;
   cfg.numAttrs = 1;
+  // builds for the neo-Hooke law with the local_f closure and each Neumann
+  // solver hold only that path's code (fewer instruction-cache misses along
+  // the link's chain); other problems take the generic builds
+  auto kern = k_links2g<-1>;
+  if (c.m.model == kMatNeoHooke) {
+    kern = k_links2g<kMatNeoHooke>;
+    if (c.p.recon == 12 && c.p.normal_solver == kSolverFD)
+      kern = k_links2g<kMatNeoHooke, 12, kSolverFD>;
+    else if (c.p.recon == 12 && c.p.normal_solver == kSolverAcoustic)
+      kern = k_links2g<kMatNeoHooke, 12, kSolverAcoustic>;
+    else if (c.p.recon == 12 && c.p.normal_solver == kSolverEnergy)
+      kern = k_links2g<kMatNeoHooke, 12, kSolverEnergy>;
+  }
   const int tk = link_timer_begin(s);
-  if (c.m.model == kMatNeoHooke)
-    cudaLaunchKernelEx(&cfg, k_links2g<kMatNeoHooke>, c, src, dst, U, u, clock, t, offset, fused,
-                       scratch, partner, clock_next);
-  else
-    cudaLaunchKernelEx(&cfg, k_links2g<-1>, c, src, dst, U, u, clock, t, offset, fused, scratch,
-                       partner, clock_next);
+  cudaLaunchKernelEx(&cfg, kern, c, src, dst, U, u, clock, t, offset, fused, scratch, partner,
+                     clock_next);
   link_timer_end(tk, s);
   cv::count_launches(1);
 }

@@ -632,14 +632,18 @@ __device__ __forceinline__ void link2_bfl_in(const LinkIn2& L, int a, int N,
 }
 
 // One cut link (processing slot `slot`) on the 16 lanes of a group; every
-// lane of the group calls it (only __syncwarp inside).
+// lane of the group calls it (only __syncwarp inside).  RECON / SOLVER >= 0
+// fix the reconstruction and the Neumann solver at compile time (they must
+// equal the problem's), so that the kernel holds only that path's code.
+template <int RECON = -1, int SOLVER = -1>
 __device__ __forceinline__ void link2_group(
     const Ctx2& c, const Mat& m, const LinkBC2& B, LinkShared2& S, int lane, int slot,
     const double* __restrict__ fpost, double* __restrict__ fout, const double* __restrict__ U,
     const double* __restrict__ u, const double* clock, double t_host, double offset, int fused,
     const double* __restrict__ scratch, const int32_t* __restrict__ partner) {
   const cvlbm2d_problem& p = c.p;
-  const int N = c.N, recon = p.recon;
+  const int N = c.N, recon = RECON >= 0 ? RECON : p.recon;
+  const int solver = SOLVER >= 0 ? SOLVER : p.normal_solver;
   const bool live = slot < p.n_links;
   const bool rowed = p.link_rows != nullptr;
   // this lane's quantity: d/dx (q < 6), d/dy (6 <= q < 12) of component
@@ -783,7 +787,7 @@ __device__ __forceinline__ void link2_group(
       }
     }
     double Fb[4] = {Fg[0], Fg[1], Fg[2], Fg[3]};
-    if (kind == kNeumann) solve_normal_image2(Fg, nxb, nyb, bv0, bv1, m, p.normal_solver, Fb);
+    if (kind == kNeumann) solve_normal_image2(Fg, nxb, nyb, bv0, bv1, m, solver, Fb);
     const P2 Pb = piola2(Fb[0], Fb[1], Fb[2], Fb[3], m);
     S.Pb[0] = Pb.a;
     S.Pb[1] = Pb.b;
@@ -890,7 +894,7 @@ __device__ __forceinline__ Mat link_mat2(const Ctx2& c) {
   return m;
 }
 
-template <int MAT>
+template <int MAT, int RECON = -1, int SOLVER = -1>
 __global__ void __launch_bounds__(kLinkThreads2, 3)
     k_links2g(Ctx2 c, const double* __restrict__ fpost, double* __restrict__ fout,
               const double* __restrict__ U, const double* __restrict__ u, const double* clock,
@@ -905,8 +909,8 @@ __global__ void __launch_bounds__(kLinkThreads2, 3)
   const int slot = blockIdx.x * kLinksPerBlock2 + grp;
   if (clock_next && blockIdx.x == 0 && threadIdx.x == 0) *clock_next = clock[0] + c.p.dt;
   const Mat m = link_mat2<MAT>(c);
-  link2_group(c, m, bc, sh[grp], lane, slot, fpost, fout, U, u, clock, t_host, offset, fused,
-              scratch, partner);
+  link2_group<RECON, SOLVER>(c, m, bc, sh[grp], lane, slot, fpost, fout, U, u, clock, t_host,
+                             offset, fused, scratch, partner);
 }
 
 }  // namespace
