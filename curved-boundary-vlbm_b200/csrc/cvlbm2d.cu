@@ -44,6 +44,8 @@ struct Ctx2 {
   double ff;    // 0.5 / c
   double hdt;   // 0.5 dt
   double den;   // damping: 1 + 0.5 dt gamma (else 1)
+  double dt_om; // dt / omega
+  double src_w; // dt (1/omega - 0.5) * 0.25, the source weight of a characteristic row
 };
 
 // Boundary time: the step's start time (host value, or the device clock in
@@ -578,6 +580,8 @@ Ctx2 make_ctx(const cvlbm2d_problem* p) {
   c.ff = 0.5 / p->c;
   c.hdt = 0.5 * p->dt;
   c.den = p->source_mode == kSrcDamping ? 1.0 + c.hdt * p->source[0] : 1.0;
+  c.dt_om = p->dt / p->omega;
+  c.src_w = p->dt * (1.0 / p->omega - 0.5) * 0.25;
   return c;
 }
 

@@ -869,10 +869,12 @@ __device__ __forceinline__ void link2_group(
     double val;
     if (char_ok) {
       const P2 Pc{S.Pc[0], S.Pc[1], S.Pc[2], S.Pc[3]};
-      const double jv = 0.25 * (S.cw[a] + (2.0 / cc) * (dxin * S.eqx[a] + dyin * S.eqy[a]));
-      const double ge = feq2(qi, a, S.cv, Pc, 2.0 / cc);
+      // 2/c, dt/omega and dt (1/omega - 1/2) / 4 are per-problem constants
+      // formed once on the host with the same IEEE operations (Ctx2)
+      const double jv = 0.25 * (S.cw[a] + c.k2c * (dxin * S.eqx[a] + dyin * S.eqy[a]));
+      const double ge = feq2(qi, a, S.cv, Pc, c.k2c);
       const double sa = source_comp(a, p.source_mode, p.source, S.cv);
-      val = ge - dt / om * jv + dt * (1.0 / om - 0.5) * 0.25 * sa;
+      val = ge - c.dt_om * jv + c.src_w * sa;
     } else {
       if (use_char) link2_bfl_in(L, a, N, fpost, fused, scratch, partner, fo, fi, upv);
       if (eta >= 0.5) {
