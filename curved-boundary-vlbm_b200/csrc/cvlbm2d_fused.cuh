@@ -740,7 +740,7 @@ __device__ __forceinline__ void link2_group(
   const int qi = L.qi, kind = L.kind, mode = L.mode;
   const double* pp = L.pp;
   const double nxb = L.nxb, nyb = L.nyb, eta = L.eta;
-  const double dt = p.dt, cc = p.c, om = p.omega;
+  const double dt = p.dt, cc = p.c;
   const double dxin = (double)cx2(qi), dyin = (double)cy2(qi);
   const double tmid = time_of(clock, t_host, offset);
   // lane 0 of the group loaded the dynamic traction; every lane needs bv for
