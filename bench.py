@@ -732,10 +732,30 @@ def main():
         "gpu_launches": int(launches_per_graph * args.steps),
     }
     if link_n:
+        # the same kernel launched eagerly (no graph): event pairs around each
+        # launch on the stream, without the graph's event-node transitions
+        eager_ms, eager_n = 0.0, 0
+        if hasattr(solver, "use_graphs"):
+            use_graphs, ov = solver.use_graphs, solver.overlap_links
+            solver.use_graphs, solver.overlap_links = False, False
+            ltimer.reset()
+            ltimer.attach()
+            for _ in range(args.steps):
+                flush.zero_()
+                solver.run(args.inner)
+                ms, cnt = ltimer.elapsed()
+                ltimer.reset()
+                eager_ms += ms
+                eager_n += cnt
+            ltimer.detach()
+            solver.use_graphs, solver.overlap_links = use_graphs, ov
         line["link_kernel"] = {
             "avg_us": link_ms * 1e3 / link_n, "launches": link_n,
             "timed": "CUDA events around each cut-link kernel launch, in the graph without "
-                     "the link overlap (L2 flushed between bench steps)"}
+                     "the link overlap (L2 flushed between bench steps)",
+            "eager_avg_us": eager_ms * 1e3 / eager_n if eager_n else None,
+            "eager_timed": "the same, launched without a graph (one native call per bench "
+                           "step)"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     del graph
