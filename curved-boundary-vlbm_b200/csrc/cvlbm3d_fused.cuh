@@ -775,13 +775,24 @@ constexpr int kGather4Links = 128 / kGather4Lanes;
 
 __global__ void __launch_bounds__(128)
     k3_link_gather4(Ctx3 c, Fused3 fz, double* __restrict__ char_state) {
+  // the block's 32 x 64 sample slots, staged with coalesced 16-byte loads so
+  // that each chunk of samples waits for one load level (weights and U rows
+  // together) instead of two (the slot, then its U row)
+  __shared__ int4 s_slot4[kGather4Links * kChar / 4];
   const cvlbm3d_problem& p = c.p;
   const int L = p.n_links;
+  const int ell0 = blockIdx.x * kGather4Links;
+  const int nl = L - ell0 < kGather4Links ? L - ell0 : kGather4Links;
+  const int4* src = reinterpret_cast<const int4*>(p.char_slot_lm + (size_t)ell0 * kChar);
+  for (int t = threadIdx.x; t < kGather4Links * kChar / 4; t += blockDim.x)
+    s_slot4[t] = t < nl * (kChar / 4) ? src[t] : make_int4(-1, -1, -1, -1);
+  __syncthreads();
   const int lane = threadIdx.x % kGather4Lanes;
-  const int ell = blockIdx.x * kGather4Links + threadIdx.x / kGather4Lanes;
+  const int g = threadIdx.x / kGather4Lanes;
+  const int ell = ell0 + g;
   if (ell >= L || p.char_idx[ell] < 0) return;
   const int a0 = 3 * lane;
-  const int* slot = p.char_slot_lm + (size_t)ell * kChar;
+  const int* slot = reinterpret_cast<const int*>(s_slot4) + g * kChar;
   const double2* w2 = reinterpret_cast<const double2*>(p.char_w_lm + (size_t)ell * kChar * 4);
   double acc[3][4];
 #pragma unroll
