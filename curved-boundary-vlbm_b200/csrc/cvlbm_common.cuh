@@ -31,17 +31,27 @@ void set_error(const char* msg);
 void count_launches(int n);
 cvlbm_timer* attached_timer();
 
+// Records a timer event on `s`: as an external event node when `s` is being
+// captured into a graph (so that every replay records it), else plainly.
+inline void record_timer_event(cudaEvent_t e, cudaStream_t s) {
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &st) == cudaSuccess && st == cudaStreamCaptureStatusActive)
+    cudaEventRecordWithFlags(e, s, cudaEventRecordExternal);
+  else
+    cudaEventRecord(e, s);
+}
+
 // Records the begin event of the next timer pair (if a timer is attached and
 // has room) and returns its index, else -1.
 inline int timer_begin(cudaStream_t s) {
   cvlbm_timer* t = attached_timer();
   if (!t || t->used >= t->capacity) return -1;
   int k = t->used++;
-  cudaEventRecordWithFlags(t->begin[k], s, cudaEventRecordExternal);
+  record_timer_event(t->begin[k], s);
   return k;
 }
 inline void timer_end(int k, cudaStream_t s) {
-  if (k >= 0) cudaEventRecordWithFlags(attached_timer()->end[k], s, cudaEventRecordExternal);
+  if (k >= 0) record_timer_event(attached_timer()->end[k], s);
 }
 
 // The same for the cut-link kernel (a second per-thread timer).
@@ -50,11 +60,11 @@ inline int link_timer_begin(cudaStream_t s) {
   cvlbm_timer* t = attached_link_timer();
   if (!t || t->used >= t->capacity) return -1;
   int k = t->used++;
-  cudaEventRecordWithFlags(t->begin[k], s, cudaEventRecordExternal);
+  record_timer_event(t->begin[k], s);
   return k;
 }
 inline void link_timer_end(int k, cudaStream_t s) {
-  if (k >= 0) cudaEventRecordWithFlags(attached_link_timer()->end[k], s, cudaEventRecordExternal);
+  if (k >= 0) record_timer_event(attached_link_timer()->end[k], s);
 }
 
 inline int fail(int code, const char* msg) {
