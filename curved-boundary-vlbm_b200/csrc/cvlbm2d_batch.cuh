@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(kTX * TY, MINB)
   }
 }
 
-template <int MAT>
+template <int MAT, int RECON = -1, int SOLVER = -1>
 __global__ void __launch_bounds__(kLinkThreads2, 3)
     k_batch_links2(const Inst2* __restrict__ inst, const InstState2* __restrict__ st,
                    const int2* __restrict__ work, int n_work) {
@@ -97,7 +97,8 @@ __global__ void __launch_bounds__(kLinkThreads2, 3)
     __syncthreads();
     double* f1 = I.f[parity_of(st[wk.x]) ^ 1];
     const Mat m = link_mat2<MAT>(I.c);
-    link2_group(I.c, m, bc, sh[grp], lane, wk.y + grp, f1, f1, I.U, I.u, &st[wk.x].clock, 0.0,
+    link2_group<RECON, SOLVER>(I.c, m, bc, sh[grp], lane, wk.y + grp, f1, f1, I.U, I.u,
+                               &st[wk.x].clock, 0.0,
                 0.5 * I.c.p.dt, 1, I.scratch, I.partner);
   }
 }
@@ -215,6 +216,7 @@ struct cvlbm2d_batch {
   int groups = 1;
   int inst_split = 0, work_split = 0, lwork_split = 0;
   int all_neo_hooke = 0;  // every instance neo-Hooke: the link kernel compiled for it
+  int local_f_solver = -1;  // ... and every one local_f with this Neumann solver
   cudaStream_t side = nullptr;
   cudaEvent_t ev_a = nullptr, ev_b = nullptr;
 };
@@ -246,15 +248,24 @@ void batch_nodes(cvlbm2d_batch* b, int w0, int w1, int store_all, cudaStream_t s
   cv::count_launches(1);
 }
 
+// The link kernel build for the batch: fixed at compile time to the law, the
+// closure and the Neumann solver when every instance shares them.
+using BatchLinkFn = void (*)(const Inst2*, const InstState2*, const int2*, int);
+BatchLinkFn batch_link_kernel(const cvlbm2d_batch* b) {
+  if (!b->all_neo_hooke) return k_batch_links2<-1>;
+  switch (b->local_f_solver) {
+    case kSolverFD: return k_batch_links2<kMatNeoHooke, 12, kSolverFD>;
+    case kSolverAcoustic: return k_batch_links2<kMatNeoHooke, 12, kSolverAcoustic>;
+    case kSolverEnergy: return k_batch_links2<kMatNeoHooke, 12, kSolverEnergy>;
+    default: return k_batch_links2<kMatNeoHooke>;
+  }
+}
+
 void batch_links_tick(cvlbm2d_batch* b, int l0, int l1, int i0, int i1, cudaStream_t s) {
   if (l1 > l0) {
     const int grid = b->link_grid < l1 - l0 ? b->link_grid : l1 - l0;
-    if (b->all_neo_hooke)
-      k_batch_links2<kMatNeoHooke><<<grid, kLinkThreads2, 0, s>>>(b->d_inst, b->d_state,
-                                                                  b->d_lwork + l0, l1 - l0);
-    else
-      k_batch_links2<-1><<<grid, kLinkThreads2, 0, s>>>(b->d_inst, b->d_state, b->d_lwork + l0,
-                                                        l1 - l0);
+    batch_link_kernel(b)<<<grid, kLinkThreads2, 0, s>>>(b->d_inst, b->d_state,
+                                                       b->d_lwork + l0, l1 - l0);
     cv::count_launches(1);
   }
   if (i1 > i0) {
@@ -398,13 +409,14 @@ extern "C" int cvlbm2d_batch_create(int32_t n_inst, const cvlbm2d_problem* probl
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.nodes, v.threads, v.smem);
   b->all_neo_hooke = 1;
-  for (int i = 0; i < n_inst; ++i)
+  b->local_f_solver = problems[0].recon == 12 ? problems[0].normal_solver : -1;
+  for (int i = 0; i < n_inst; ++i) {
     if (problems[i].mat.model != kMatNeoHooke) b->all_neo_hooke = 0;
-  if (b->all_neo_hooke)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_l, k_batch_links2<kMatNeoHooke>,
-                                                  kLinkThreads2, 0);
-  else
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_l, k_batch_links2<-1>, kLinkThreads2, 0);
+    if (problems[i].recon != 12 || problems[i].normal_solver != b->local_f_solver)
+      b->local_f_solver = -1;
+  }
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_l, batch_link_kernel(b), kLinkThreads2,
+                                                0);
   const int full = sms * (per_sm > 0 ? per_sm : 1);
   b->node_grid = grid_blocks > 0 ? grid_blocks : full;
   if (b->node_grid > b->n_work) b->node_grid = b->n_work > 0 ? b->n_work : 1;
