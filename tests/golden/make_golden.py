@@ -357,6 +357,35 @@ CASES_3D = {
     ),
 }
 
+
+def _recon_case_3d(recon: str, *, poisson=0.25, steps=5):
+    """Clamped inner sphere and a sin^2-ramped normal traction on the outer
+    one, with the given boundary reconstruction (3-D)."""
+    return dict(
+        geometry=dict(kind="spherical_shell", nx=16, ny=16, nz=16, length_x=2.2, length_y=2.2,
+                      length_z=2.2, center=[1.1, 1.1, 1.1], inner_radius=0.5, outer_radius=1.0),
+        material=dict(model="neo_hooke", poisson=poisson, mu=1.0),
+        boundary=dict(kind="neumann", value_mode=203, params=[0.04, 0.02, 0.0],
+                      id_kinds={"1": "neumann", "2": "dirichlet"},
+                      id_value_modes={"1": 203, "2": 0},
+                      id_params={"1": [0.04, 0.02, 0.0], "2": []}),
+        solver=dict(lattice_speed=10.0, collision_omega=1.8, boundary_reconstruction=recon,
+                    source_mode="damping", damping_gamma=5.0, local_displacement_interval=1,
+                    local_displacement_sweeps=1, local_displacement_relax=0.85,
+                    local_displacement_boundary_weight=100.0, local_compatibility_interval=1,
+                    local_compatibility_blend=0.5),
+        init=dict(kind="identity", init_order=1),
+        steps=steps,
+    )
+
+
+# The two 3-D reconstructions without a fixture above: half-way bounce-back
+# (eta fixed at 1/2) and the single-history BFL form of local_f.
+CASES_3D.update({
+    "g3_shell_halfway": _recon_case_3d("halfway"),
+    "g3_shell_localf_bfl": _recon_case_3d("local_f_bfl", poisson=0.3),
+})
+
 # Geometry-only pins (tables are compared bit for bit).
 # One small case per material law other than neo-Hooke: the 2-D traction
 # annulus (local_f closure, sweep, repair) from a perturbed state, and a 3-D

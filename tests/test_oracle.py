@@ -21,6 +21,7 @@ GOLD2 += [f"g2_mat_{m}" for m in ("svk", "log_neo_hooke", "mooney_rivlin", "yeoh
 GOLD2 += ["g2_mrt_ghost", "g2_kinetic_filter", "g2_mrt_filter"]
 GOLD2 += ["g2_lsq_bfl", "g2_compat_bfl_traction", "g2_local_char2", "g2_local_f_bfl"]
 GOLD3 += ["g3_mixed_localf", "g3_mixed_fd", "g3_mixed_energy"]
+GOLD3 += ["g3_shell_halfway", "g3_shell_localf_bfl"]
 GOLD3 += [f"g3_mat_{m}" for m in ("svk", "log_neo_hooke", "mooney_rivlin", "yeoh", "gent",
                                    "sph_neo_hooke")]
 
