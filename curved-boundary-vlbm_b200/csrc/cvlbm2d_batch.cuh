@@ -6,7 +6,7 @@
 // Per lattice step three launches cover every instance:
 //   k_batch_nodes2   persistent: a grid of (SMs x resident blocks) walks the
 //                    work list of (instance, tile) pairs
-//   k_batch_links2   persistent: walks (instance, 8-link group) pairs
+//   k_batch_links2   persistent: walks (instance, 16-link group) pairs
 //   k_batch_tick2    advances each active instance's clock and step counter
 // Every `check_every` steps the node kernel also stores U and u of every
 // active node, k_batch_partial2 reduces |u - u_prev|^2 and |u|^2 per
@@ -78,14 +78,20 @@ __global__ void __launch_bounds__(kTX * TY, MINB)
   }
 }
 
+// The batched link kernel runs 8 lanes per link (16 links per block): in the
+// batch the link work is throughput-bound, so twice the links in flight per
+// SM pay for each link's longer gather.
+constexpr int kBatchLG = 8;
+constexpr int kBatchLinksPerBlock = kLinkThreads2 / kBatchLG;
+
 template <int MAT, int RECON = -1, int SOLVER = -1>
 __global__ void __launch_bounds__(kLinkThreads2, 3)
     k_batch_links2(const Inst2* __restrict__ inst, const InstState2* __restrict__ st,
                    const int2* __restrict__ work, int n_work) {
-  __shared__ LinkShared2 sh[kLinksPerBlock2];
+  __shared__ LinkShared2 sh[kBatchLinksPerBlock];
   __shared__ LinkBC2 bc;
-  const int lane = threadIdx.x & (kLG - 1);
-  const int grp = threadIdx.x / kLG;
+  const int lane = threadIdx.x & (kBatchLG - 1);
+  const int grp = threadIdx.x / kBatchLG;
   for (int w = blockIdx.x; w < n_work; w += gridDim.x) {
     const int2 wk = work[w];
     // uniform over the block (one work item per iteration): the barriers
@@ -97,7 +103,7 @@ __global__ void __launch_bounds__(kLinkThreads2, 3)
     __syncthreads();
     double* f1 = I.f[parity_of(st[wk.x]) ^ 1];
     const Mat m = link_mat2<MAT>(I.c);
-    link2_group<RECON, SOLVER>(I.c, m, bc, sh[grp], lane, wk.y + grp, f1, f1, I.U, I.u,
+    link2_group<RECON, SOLVER, kBatchLG>(I.c, m, bc, sh[grp], lane, wk.y + grp, f1, f1, I.U, I.u,
                                &st[wk.x].clock, 0.0,
                 0.5 * I.c.p.dt, 1, I.scratch, I.partner);
   }
@@ -380,7 +386,7 @@ extern "C" int cvlbm2d_batch_create(int32_t n_inst, const cvlbm2d_problem* probl
     // raster order (a solver's list may hold its inner tiles first)
     std::sort(tiles.begin(), tiles.end());
     for (int t : tiles) work.push_back(make_int2(i, t));
-    for (int l = 0; l < p->n_links; l += kLinksPerBlock2) lwork.push_back(make_int2(i, l));
+    for (int l = 0; l < p->n_links; l += kBatchLinksPerBlock) lwork.push_back(make_int2(i, l));
   }
   work_start[n_inst] = (int)work.size();
   cvlbm2d_batch* b = new cvlbm2d_batch();

@@ -635,7 +635,10 @@ __device__ __forceinline__ void link2_bfl_in(const LinkIn2& L, int a, int N,
 // lane of the group calls it (only __syncwarp inside).  RECON / SOLVER >= 0
 // fix the reconstruction and the Neumann solver at compile time (they must
 // equal the problem's), so that the kernel holds only that path's code.
-template <int RECON = -1, int SOLVER = -1>
+// LG (16 or 8) lanes per link: with 8, lane l gathers quantities l and l + 8
+// one after the other (twice the links in flight per SM for the same
+// registers, a longer gather per link: the batched solve's throughput form).
+template <int RECON = -1, int SOLVER = -1, int LG = kLG>
 __device__ __forceinline__ void link2_group(
     const Ctx2& c, const Mat& m, const LinkBC2& B, LinkShared2& S, int lane, int slot,
     const double* __restrict__ fpost, double* __restrict__ fout, const double* __restrict__ U,
@@ -734,6 +737,32 @@ __device__ __forceinline__ void link2_group(
       S.dut[lane] = d;
       if (lane == 0) S.wt_abs = wa;
     }
+    if constexpr (LG == 8) {
+      // the second quantity of this lane: d/dy of components 2-5 or a
+      // predictor component
+      const int q2 = lane + 8;
+      const int comp2 = q2 < 12 ? q2 - 6 : q2 - 10;
+      const bool mine2 = q2 < 12 ? use_char : (lsq_recon || (recon == 2 && L.lsq_ok));
+      if (mine2) {
+        const double* w = (q2 < 12 ? (L.rowed ? p.lsq_wy_slot : p.lsq_wy)
+                                   : (L.rowed ? p.lsq_wb_slot : p.lsq_wb)) + sl;
+        const double* Uq = U + (size_t)comp2 * N;
+        double acc = 0.0;
+#pragma unroll
+        for (int k = 0; k < kMaxLsq2; ++k)
+          if (nd[k] >= 0) acc += w[k] * Uq[nd[k]];
+        S.g[q2] = acc;
+      } else if (q2 >= 12) {
+        const double* Uk = U + (size_t)comp2 * N;
+        double fg;
+        if (recon == 0 || recon == 2 || recon == 13) {
+          fg = L.up_ok ? Uk[L.n] + L.eta * (Uk[L.n] - Uk[L.nu]) : Uk[L.n];
+        } else {
+          fg = interp_link(Uk, p.active, L.i, L.j, L.qo, L.eta, p.nx, p.ny);
+        }
+        S.g[q2] = fg;
+      }
+    }
   }
   __syncwarp();
 
@@ -745,7 +774,7 @@ __device__ __forceinline__ void link2_group(
   const double tmid = time_of(clock, t_host, offset);
   // lane 0 of the group loaded the dynamic traction; every lane needs bv for
   // its row (all 32 lanes of the warp take part in the shuffles)
-  const int lane0 = (threadIdx.x & 31) & ~(kLG - 1);
+  const int lane0 = (threadIdx.x & 31) & ~(LG - 1);
   const double trx_g = __shfl_sync(0xffffffffu, trx, lane0);
   const double try_g = __shfl_sync(0xffffffffu, try_, lane0);
   double bv0 = 0.0, bv1 = 0.0;
