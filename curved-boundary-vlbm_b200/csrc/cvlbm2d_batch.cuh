@@ -98,9 +98,7 @@ __global__ void __launch_bounds__(kLinkThreads2, 3)
     // below are reached by every thread or by none
     if (!st[wk.x].active) continue;
     const Inst2& I = inst[wk.x];
-    __syncthreads();  // the previous item's readers of bc are done
-    stage_bc2(I.c.p, bc);
-    __syncthreads();
+    __syncthreads();  // the previous item's readers of bc are done (link2_group restages it)
     double* f1 = I.f[parity_of(st[wk.x]) ^ 1];
     const Mat m = link_mat2<MAT>(I.c);
     link2_group<RECON, SOLVER, kBatchLG>(I.c, m, bc, sh[grp], lane, wk.y + grp, f1, f1, I.U, I.u,

@@ -554,12 +554,15 @@ struct LinkIn2 {
   bool live, rowed, up_ok, lsq_ok;
 };
 
-__device__ __forceinline__ LinkIn2 link2_in(const Ctx2& c, const LinkBC2& B, int slot) {
+// The row part (no boundary tables needed: these loads can be issued before
+// the block's boundary tables are staged), then link2_in_bc.
+__device__ __forceinline__ LinkIn2 link2_in_row(const Ctx2& c, int slot, int& bid) {
   const cvlbm2d_problem& p = c.p;
   LinkIn2 L;
   L.live = slot < p.n_links;
   L.rowed = p.link_rows != nullptr;
-  L.pp = B.params;
+  L.pp = nullptr;
+  bid = 0;
   L.eta = 0.5;
   L.xb = L.yb = L.nyb = 0.0;
   L.nxb = 1.0;
@@ -568,7 +571,6 @@ __device__ __forceinline__ LinkIn2 link2_in(const Ctx2& c, const LinkBC2& B, int
   L.kind = kDirichlet;
   L.up_ok = L.lsq_ok = false;
   if (!L.live) return L;
-  int bid;
   if (L.rowed) {
     const cvlbm2d_link_row* row = p.link_rows + slot;
     L.ell = row->ell;
@@ -604,12 +606,17 @@ __device__ __forceinline__ LinkIn2 link2_in(const Ctx2& c, const LinkBC2& B, int
     L.lsq_ok = p.lsq_valid[ell] != 0;
   }
   if (bid < 0 || bid >= kMaxIds2) bid = 0;
-  L.kind = B.kind[bid];
-  L.mode = B.mode[bid];
-  L.pp = B.params + bid * 8;
   L.qi = L.qo + 2;
   if (L.qi >= 4) L.qi -= 4;
   return L;
+}
+
+// The boundary-table part of a link's inputs (after the tables are staged).
+__device__ __forceinline__ void link2_in_bc(LinkIn2& L, const LinkBC2& B, int bid) {
+  L.pp = B.params + bid * 8;
+  if (!L.live) return;
+  L.kind = B.kind[bid];
+  L.mode = B.mode[bid];
 }
 
 // BFL inputs of population row a of a link: the outgoing post-collision value
@@ -640,7 +647,7 @@ __device__ __forceinline__ void link2_bfl_in(const LinkIn2& L, int a, int N,
 // registers, a longer gather per link: the batched solve's throughput form).
 template <int RECON = -1, int SOLVER = -1, int LG = kLG>
 __device__ __forceinline__ void link2_group(
-    const Ctx2& c, const Mat& m, const LinkBC2& B, LinkShared2& S, int lane, int slot,
+    const Ctx2& c, const Mat& m, LinkBC2& B, LinkShared2& S, int lane, int slot,
     const double* __restrict__ fpost, double* __restrict__ fout, const double* __restrict__ U,
     const double* __restrict__ u, const double* clock, double t_host, double offset, int fused,
     const double* __restrict__ scratch, const int32_t* __restrict__ partner) {
@@ -667,7 +674,13 @@ __device__ __forceinline__ void link2_group(
       wv[k] = w[sl + k];
     }
   }
-  const LinkIn2 L = link2_in(c, B, slot);
+  int bid;
+  LinkIn2 L = link2_in_row(c, slot, bid);
+  // the block's boundary tables, staged while the loads above are in flight
+  // (every thread of the block reaches this barrier)
+  stage_bc2(p, B);
+  __syncthreads();
+  link2_in_bc(L, B, bid);
   const size_t sl = (size_t)(L.rowed ? slot : L.ell) * kMaxLsq2;
   if (live && !early && lsq_tables) {
     const int* lnode = (L.rowed ? p.lsq_node_slot : p.lsq_node) + sl;
@@ -932,9 +945,7 @@ __global__ void __launch_bounds__(kLinkThreads2, 3)
               double t_host, double offset, int fused, const double* __restrict__ scratch,
               const int32_t* __restrict__ partner, double* clock_next) {
   __shared__ LinkShared2 sh[kLinksPerBlock2];
-  __shared__ LinkBC2 bc;
-  stage_bc2(c.p, bc);
-  __syncthreads();
+  __shared__ LinkBC2 bc;  // staged inside link2_group
   const int lane = threadIdx.x & (kLG - 1);
   const int grp = threadIdx.x / kLG;
   const int slot = blockIdx.x * kLinksPerBlock2 + grp;
